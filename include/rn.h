@@ -1,0 +1,159 @@
+/* rn.h -- C-ABI of librn.so, the B200 time-step library for the rocket
+ * nozzle solver.
+ *
+ * Each entry point replaces one method of the reference's WebGL2 solver
+ * (source/solver.js, source/spray.js); the comment on each names the line it
+ * stands in for. Conventions:
+ *   - every call returns int: RN_OK (0), RN_NOT_READY (1) for a poll whose
+ *     data is not there yet, RN_BUSY (2) when an asynchronous read is already
+ *     in flight, or a negative error code; rn_last_error() gives the message
+ *     of the calling thread's last failure;
+ *   - host buffers belong to the caller and are copied in or out during the
+ *     call; device memory belongs to the handle;
+ *   - one handle is used by one host thread at a time; its work runs in order
+ *     on the handle's own CUDA stream. rn_step and rn_rescale_ambient return
+ *     once the work is queued; the read functions block until their data is
+ *     on the host.
+ * Layout: cell (i, j) of an Nx x Nr grid is element j*Nx + i; A = (rho, rho u,
+ * rho v, E) and B = (rho Z, rho F, G, rho O or inflow-speed average) are
+ * float4 per cell, exactly the reference's RGBA32F state textures.
+ */
+#ifndef RN_H
+#define RN_H
+#include <stddef.h>
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RN_OK 0
+#define RN_NOT_READY 1
+#define RN_BUSY 2
+#define RN_ERR_ARG (-1)
+#define RN_ERR_CUDA (-2)
+#define RN_ERR_STATE (-3)
+#define RN_ERR_NOMEM (-4)
+
+/* texture names for rn_read_rect / rn_request_async (the reference reads any
+ * texture it owns through _readRect, solver.js:1016) */
+#define RN_TEX_A 0          /* current state A, Nx x Nr */
+#define RN_TEX_B 1          /* current state B, Nx x Nr */
+#define RN_TEX_STEPINFO 2   /* (dt, t_old, t_new, w), 1 x 1 */
+#define RN_TEX_WALLROW 3    /* near-wall row (u, v, p, c), Nx x 1, after rn_draw_wall_row */
+#define RN_TEX_PARCEL_A 4   /* parcels (x, r, u, v), 256 x 256 */
+#define RN_TEX_PARCEL_B 5   /* parcels (d, m, type, x_imp), 256 x 256 */
+#define RN_TEX_PARCEL_C 6   /* parcels (dm, dp_x, dp_r, 0) given to the gas last step */
+
+typedef struct rn_solver* rn_handle;
+
+/* The normalised parameter block P of the reference (simsetup.js:274-310),
+ * reduced to the float32 uniforms the shaders receive. bar = (inlet[0],
+ * 1.6 uInlet0, max(ramp, 0)) is solver.js:935's uBar; fan is spray.js:271's
+ * 25 degrees in radians. Flags are 0/1. */
+typedef struct {
+  float amb[4], ambCons[4], ambB[4];
+  float gamR[2];
+  float inlet[4];
+  float bar[3];
+  float res[3];
+  float gas[4];
+  float Rs[3];
+  float chemK[4];
+  float cap[2];
+  float chamberNu[2];
+  float Tw, cfl, dtMax, wFloor, vMax, hllBlend, ramp, pStart, RcCells;
+  int order2, inj, visc, chem;
+  float mhat, tScale;
+  float fuel[4], ox[4];
+  float eF, eO, Ge, fan;
+} rn_params;
+
+/* one rectangle of an asynchronous read (requestAsync's reqs, solver.js:1028) */
+typedef struct {
+  int tex, x, y, w, h;
+} rn_read_req;
+
+/* Inputs of the FP64 read-out integrals: the exit column and its jExit, the
+ * throat column, the chamber probe cell, and dx (simsetup.js:239-250, 314-348). */
+typedef struct {
+  int iExit, jExit, iThroat, iChamber;
+  double dx, pAmb;       /* pAmb = P.amb[3] (normalised ambient pressure) */
+  double Rs[3], RaN;     /* gas constants for the chamber-cell temperature */
+  int inj;
+} rn_integral_spec;
+
+/* FP64 read-outs, normalised units as the reference's JavaScript computes
+ * them before its SI scaling: thrust F, exhaust mass flow mdot, Mach-weighted
+ * flow Mw (exit Mach = Mw/mdot), pressure-area pw and area A of the exit
+ * plane; throat mass flow, oxidiser and fuel-vapour flows; chamber-cell
+ * pressure and temperature ratio p/(rho Rmix); step info; every sum is a
+ * Neumaier-compensated double sum. */
+typedef struct {
+  double F, mdot, Mw, pw, A;
+  double throat_mdot, throat_mO, throat_mF;
+  double chamber_p, chamber_T;
+  double dt, t;
+} rn_integrals_out;
+
+/* new GPUSolver(gl) + resize(Nx, Nr) (solver.js:678, 759) */
+int rn_create(int Nx, int Nr, rn_handle* out);
+/* GPUSolver._free (solver.js:752) and the handle itself */
+int rn_destroy(rn_handle h);
+/* resize(Nx, Nr) (solver.js:759-789): reallocates and clears every buffer */
+int rn_resize(rn_handle h, int Nx, int Nr);
+/* setMask(u8) (solver.js:791-799): nonzero = solid */
+int rn_set_mask(rn_handle h, const uint8_t* mask);
+/* setGeometry({mask, geoA, geoG, geoM, jWall}) (solver.js:801-814): geoA is
+ * (Nx+1) x (Nr+1) float4, geoG and geoM Nx x Nr float4, jWall Nx float4 or NULL */
+int rn_set_geometry(rn_handle h, const uint8_t* mask, const float* geoA, const float* geoG, const float* geoM,
+                    const float* jWall);
+/* setState(A, B) (solver.js:816-828): all three state slots, clears dt/t and
+ * the spray ring */
+int rn_set_state(rn_handle h, const float* A, const float* B);
+/* readAll() (solver.js:1075) */
+int rn_get_state(rn_handle h, float* A, float* B);
+/* step(n, P) (solver.js:849-891), including GPUSpray.step (spray.js:256-297)
+ * when P->inj is set: queued on the handle's stream */
+int rn_step(rn_handle h, int n, const rn_params* P);
+/* rescaleAmbient(fp, fT, du, P) (solver.js:998-1010) */
+int rn_rescale_ambient(rn_handle h, float fp, float fT, float du, const rn_params* P);
+/* drawWallRow() (solver.js:986-996): fills RN_TEX_WALLROW */
+int rn_draw_wall_row(rn_handle h);
+/* _readRect(tex, x, y, w, h) (solver.js:1016-1025): blocking, w*h*4 floats */
+int rn_read_rect(rn_handle h, int tex, int x, int y, int w, int hgt, float* out);
+/* readStepInfo() (solver.js:1072) */
+int rn_read_step_info(rn_handle h, float out[4]);
+/* requestAsync(reqs, tag) (solver.js:1028-1048): copies into pinned memory
+ * behind an event; RN_BUSY when a read is already in flight */
+int rn_request_async(rn_handle h, const rn_read_req* reqs, int nreq, int tag);
+/* pollAsync() (solver.js:1050-1065): RN_NOT_READY until the copies are done,
+ * then writes the concatenated floats (requests in order) and the tag;
+ * RN_ERR_STATE when nothing is in flight; RN_ERR_ARG if cap_floats is short */
+int rn_poll_async(rn_handle h, int* tag, float* out, size_t cap_floats);
+/* cancelAsync() (solver.js:1066-1070) */
+int rn_cancel_async(rn_handle h);
+/* GPUSpray.setInjector({tab}) (spray.js:236-241): 256 x 3 float4 */
+int rn_spray_set_injector(rn_handle h, const float* tab);
+/* GPUSpray.reset() (spray.js:242-254) */
+int rn_spray_reset(rn_handle h);
+/* GPUSpray.stats(P) (spray.js:312-320): out = (fuel mass, oxidiser mass,
+ * live parcels, mean diameter) */
+int rn_spray_stats(rn_handle h, double out[4]);
+/* The read-outs the reference computes in JavaScript from column read-backs
+ * (exitPerformance simsetup.js:314-337, chamberPerformance 239-250,
+ * cellPrimSI 338-348), evaluated on the device in FP64. */
+int rn_integrals(rn_handle h, const rn_integral_spec* spec, rn_integrals_out* out);
+/* waits for all queued work of the handle */
+int rn_sync(rn_handle h);
+/* Bounded wait: polls the handle's stream until its work is done or
+ * timeout_ms elapse; RN_NOT_READY on timeout (the work keeps running). */
+int rn_wait(rn_handle h, int timeout_ms);
+/* number of kernels this handle has launched (for launch accounting) */
+int rn_kernel_launches(rn_handle h, long long* out);
+/* message of the calling thread's last error ("" if none) */
+const char* rn_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,65 @@
+"""Synthetic, seeded workloads with the shapes of the benchmark configurations.
+
+Each function returns a ``cfg`` dict for :func:`build_sim_setup` (SI units,
+the keys of the reference's ``cfgFromS``, app.js:201-211) plus the step count
+the configuration is quoted on. No dataset is involved: every input is built
+by the setup pipeline from these parameters.
+"""
+import math
+
+from .physics import ENGINE_PRESETS, PROPELLANTS
+
+BASE = dict(base=False, bodyRatio=1.5, mach=0.0, startMode="ramp", rampMs=0.12, order2=True, wallModel="cut",
+            minCells=8, Tw=800, inletAbsorb=1.0, injMode=False, hllBlend=1.0)
+
+
+def plain_small(Nx=256, Nr=96):
+    """Cold-gas conical nozzle: gamma 1.4, R 287 (Mw 28.97), p0 20 bar, T0 300 K,
+    contraction 4, 15-degree cone, expansion 8, sea level; inviscid MUSCL-HLLC,
+    CFL 0.5, 2000 steps."""
+    cfg = dict(BASE, prop="coldgas", Dt=0.020, De=0.020 * math.sqrt(8.0), type="cone", bellPct=80, coneAngle=15,
+               CR=4, chamberLen=1.4, Pc=20e5, Tc=300.0, gamma=1.4, Mw=28.97, alt=0.0, domainL=0.6, Nx=Nx,
+               aspect=Nr / Nx, cfl=0.5, viscous=False, afterburn=False, qAb=0.0, sAir=1.0)
+    return cfg, 2000
+
+
+def viscous_plume(Nx=512, Nr=192, alt_km=0.0):
+    """Methalox products, gamma 1.2, T0 3500 K, p0 70 bar, 80 % bell with
+    expansion 20 (throat 30 mm); Sutherland + eddy viscosity, wall model at
+    800 K, afterburning scalars; 10k steps."""
+    Dt = 0.030
+    cfg = dict(BASE, prop="methalox", Dt=Dt, De=Dt * math.sqrt(20.0), type="bell", bellPct=80, coneAngle=15,
+               CR=5, chamberLen=1.5, Pc=70e5, Tc=3500.0, gamma=1.2, Mw=20.5, alt=alt_km * 1000.0, domainL=1.2,
+               Nx=Nx, aspect=Nr / Nx, cfl=0.6, viscous=True, afterburn=True, qAb=3.0, sAir=0.8)
+    return cfg, 10000
+
+
+def injector_spray(Nx=512, Nr=192):
+    """Coaxial methalox injector chamber (preset injCoax) at 70 bar with the
+    65,536-parcel spray ring; about 2 ms of simulated time."""
+    e = ENGINE_PRESETS["injCoax"]
+    p = PROPELLANTS[e["prop"]]
+    cfg = dict(BASE, prop=e["prop"], Dt=e["Dt"] / 1000, De=max(e["De"], e["Dt"] * 1.02) / 1000, type=e["type"],
+               bellPct=e["bellPct"], coneAngle=e["coneAngle"], CR=e["CR"], chamberLen=e["chamberLen"],
+               Pc=e["Pc"] * 1e5, Tc=p["Tc"], gamma=p["gamma"], Mw=p["Mw"], alt=e["alt"] * 1000.0,
+               domainL=e["domain"], Nx=Nx, aspect=Nr / Nx, cfl=0.6, viscous=True, afterburn=True, qAb=p["qAb"],
+               sAir=p["sAir"], OF=p["spray"]["OF"], injTMR=1, injAngle=30)
+    cfg.update(e["inj"])
+    return cfg, None
+
+
+def preset(key, Nx, aspect=0.28):
+    """Any of the reference's engine presets (physics.js:233-309) as applied by
+    app.js:1108-1122 with the app's default settings."""
+    e = ENGINE_PRESETS[key]
+    p = PROPELLANTS[e["prop"]]
+    cfg = dict(BASE, prop=e["prop"], Dt=e["Dt"] / 1000, De=max(e["De"], e["Dt"] * 1.02) / 1000, type=e["type"],
+               bellPct=e["bellPct"], coneAngle=e["coneAngle"], CR=e["CR"], chamberLen=e["chamberLen"],
+               Pc=e["Pc"] * 1e5, Tc=p["Tc"], gamma=p["gamma"], Mw=p["Mw"], alt=e["alt"] * 1000.0,
+               mach=e["mach"], base=e["base"], domainL=e["domain"], Nx=Nx, aspect=aspect, cfl=0.6, viscous=True,
+               afterburn=True, qAb=p["qAb"], sAir=p["sAir"], injTMR=1, injAngle=30)
+    if p.get("spray"):
+        cfg["OF"] = p["spray"]["OF"]
+    if "inj" in e:
+        cfg.update(e["inj"])
+    return cfg

@@ -1,0 +1,527 @@
+// rn_api.cu -- the C-ABI of librn.so (declared in include/rn.h).
+//
+// A handle owns all device memory of one solver instance and one CUDA stream.
+// The layout in HBM is the reference's texture layout as plain arrays: a
+// 3-slot ring of state planes A and B (float4 per cell, row-major), the
+// geometry planes geoA ((Nx+1) x (Nr+1) float4), geoG and geoM (float4 per
+// cell), the mask (1 byte per cell), two step-info float4s and two wave-speed
+// slots; the spray ring is 2 x 3 planes of 65,536 float4 plus the deposit
+// records. rn_step queues 2 kernels per step for the inviscid scheme (stage 1,
+// stage 2), 3 with the viscous/reaction split step and 3 more with sprays.
+#include <cuda_runtime.h>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+#include "rn.h"
+#include "rn_kernels.cuh"
+
+using namespace rn;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+int cuda_fail(cudaError_t e, const char* what) {
+  return fail(RN_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define CK(call)                                              \
+  do {                                                        \
+    cudaError_t e_ = (call);                                  \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);       \
+  } while (0)
+
+constexpr int SPRAY_N = 65536;
+
+}  // namespace
+
+struct rn_solver {
+  int Nx = 0, Nr = 0, device = 0;
+  cudaStream_t stream = nullptr;
+  float4* SA[3] = {nullptr, nullptr, nullptr};
+  float4* SB[3] = {nullptr, nullptr, nullptr};
+  int cur = 0;
+  float4 *geoA = nullptr, *geoG = nullptr, *geoM = nullptr, *jw = nullptr, *wallRow = nullptr;
+  uint8_t* mask = nullptr;
+  float4* stepTex = nullptr;      // [2]
+  unsigned* wmax = nullptr;       // [2]
+  int stepIdx = 0, wslot = 0;
+  bool wvalid = false;
+  long long stepCount = 0, launches = 0;
+  // spray
+  float4 *PA[2] = {nullptr, nullptr}, *PB[2] = {nullptr, nullptr}, *PC[2] = {nullptr, nullptr};
+  float4 *src = nullptr, *tab = nullptr, *dep = nullptr;
+  unsigned *key = nullptr, *val = nullptr, *keyS = nullptr, *valS = nullptr;
+  void* sortTemp = nullptr;
+  size_t sortTempBytes = 0;
+  int scur = 0;
+  uint32_t head = 0, seed = 1;
+  // asynchronous read-back
+  float* pinned = nullptr;
+  size_t pinnedCap = 0, asyncFloats = 0;
+  cudaEvent_t asyncEv = nullptr;
+  bool asyncBusy = false;
+  int asyncTag = 0;
+  double* dInt = nullptr;
+
+  Grid grid() const { return Grid{Nx, Nr, mask, geoA, geoG, geoM}; }
+};
+
+namespace {
+
+void free_buffers(rn_solver* h) {
+  cudaFree(h->SA[0]);   // base of the 6-plane state ring
+  for (int s = 0; s < 3; s++) h->SA[s] = h->SB[s] = nullptr;
+  cudaFree(h->geoA); cudaFree(h->geoG); cudaFree(h->geoM); cudaFree(h->jw); cudaFree(h->wallRow);
+  cudaFree(h->mask); cudaFree(h->stepTex); cudaFree(h->wmax); cudaFree(h->dInt);
+  cudaFree(h->PA[0]);   // base of the 6-plane parcel ring
+  for (int p = 0; p < 2; p++) h->PA[p] = h->PB[p] = h->PC[p] = nullptr;
+  cudaFree(h->src); cudaFree(h->tab); cudaFree(h->dep); cudaFree(h->key); cudaFree(h->sortTemp);
+  h->geoA = h->geoG = h->geoM = h->jw = h->wallRow = nullptr;
+  h->mask = nullptr; h->stepTex = nullptr; h->wmax = nullptr; h->dInt = nullptr;
+  h->src = h->tab = h->dep = nullptr;
+  h->key = h->val = h->keyS = h->valS = nullptr;
+  h->sortTemp = nullptr;
+}
+
+int spray_reset_dev(rn_solver* h) {
+  // PA = (-1, -1, 0, 0), PB = PC = 0 for both ring copies (spray.js:242-254)
+  std::vector<float4> dead(SPRAY_N, make_float4(-1.f, -1.f, 0.f, 0.f));
+  for (int p = 0; p < 2; p++) {
+    CK(cudaMemcpyAsync(h->PA[p], dead.data(), sizeof(float4) * SPRAY_N, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemsetAsync(h->PB[p], 0, sizeof(float4) * SPRAY_N, h->stream));
+    CK(cudaMemsetAsync(h->PC[p], 0, sizeof(float4) * SPRAY_N, h->stream));
+  }
+  CK(cudaStreamSynchronize(h->stream));
+  h->head = 0;
+  h->scur = 0;
+  return RN_OK;
+}
+
+int alloc_buffers(rn_solver* h, int Nx, int Nr) {
+  if (Nx < 1 || Nr < 1 || (long long)Nx * Nr > (1LL << 28)) return fail(RN_ERR_ARG, "grid size out of range");
+  free_buffers(h);
+  h->Nx = Nx; h->Nr = Nr;
+  const size_t N = size_t(Nx) * Nr, NF = size_t(Nx + 1) * (Nr + 1);
+  float4* ring = nullptr;
+  cudaError_t e = cudaMalloc(&ring, sizeof(float4) * N * 6);
+  if (e != cudaSuccess) return fail(RN_ERR_NOMEM, std::string("state allocation: ") + cudaGetErrorString(e));
+  for (int s = 0; s < 3; s++) { h->SA[s] = ring + N * (2 * s); h->SB[s] = ring + N * (2 * s + 1); }
+  CK(cudaMemsetAsync(ring, 0, sizeof(float4) * N * 6, h->stream));
+  CK(cudaMalloc(&h->geoA, sizeof(float4) * NF));
+  CK(cudaMalloc(&h->geoG, sizeof(float4) * N));
+  CK(cudaMalloc(&h->geoM, sizeof(float4) * N));
+  CK(cudaMalloc(&h->mask, N));
+  CK(cudaMalloc(&h->jw, sizeof(float4) * Nx));
+  CK(cudaMalloc(&h->wallRow, sizeof(float4) * Nx));
+  CK(cudaMalloc(&h->stepTex, sizeof(float4) * 2));
+  CK(cudaMalloc(&h->wmax, sizeof(unsigned) * 2));
+  CK(cudaMalloc(&h->dInt, sizeof(double) * 16));
+  CK(cudaMemsetAsync(h->geoA, 0, sizeof(float4) * NF, h->stream));
+  CK(cudaMemsetAsync(h->geoG, 0, sizeof(float4) * N, h->stream));
+  CK(cudaMemsetAsync(h->geoM, 0, sizeof(float4) * N, h->stream));
+  CK(cudaMemsetAsync(h->mask, 0, N, h->stream));
+  CK(cudaMemsetAsync(h->jw, 0, sizeof(float4) * Nx, h->stream));
+  CK(cudaMemsetAsync(h->wallRow, 0, sizeof(float4) * Nx, h->stream));
+  CK(cudaMemsetAsync(h->stepTex, 0, sizeof(float4) * 2, h->stream));
+  CK(cudaMemsetAsync(h->wmax, 0, sizeof(unsigned) * 2, h->stream));
+  // spray ring and deposit records
+  float4* pr = nullptr;
+  CK(cudaMalloc(&pr, sizeof(float4) * SPRAY_N * 6));
+  for (int p = 0; p < 2; p++) {
+    h->PA[p] = pr + SPRAY_N * (3 * p);
+    h->PB[p] = pr + SPRAY_N * (3 * p + 1);
+    h->PC[p] = pr + SPRAY_N * (3 * p + 2);
+  }
+  CK(cudaMalloc(&h->src, sizeof(float4) * N));
+  CK(cudaMemsetAsync(h->src, 0, sizeof(float4) * N, h->stream));
+  CK(cudaMalloc(&h->tab, sizeof(float4) * 768));
+  CK(cudaMemsetAsync(h->tab, 0, sizeof(float4) * 768, h->stream));
+  CK(cudaMalloc(&h->dep, sizeof(float4) * SPRAY_N));
+  CK(cudaMalloc(&h->key, sizeof(unsigned) * SPRAY_N * 4));
+  h->val = h->key + SPRAY_N;
+  h->keyS = h->key + 2 * SPRAY_N;
+  h->valS = h->key + 3 * SPRAY_N;
+  h->sortTempBytes = spray_sort_temp_bytes(int(N));
+  CK(cudaMalloc(&h->sortTemp, h->sortTempBytes > 0 ? h->sortTempBytes : 16));
+  h->cur = 0; h->stepIdx = 0; h->wslot = 0; h->wvalid = false; h->stepCount = 0;
+  h->seed = 1;
+  return spray_reset_dev(h);
+}
+
+bool valid(rn_solver* h) { return h != nullptr && h->SA[0] != nullptr; }
+
+void make_grid_copy(const rn_solver* h, Grid& g) { g = h->grid(); }
+
+}  // namespace
+
+extern "C" {
+
+const char* rn_last_error(void) { return g_err.c_str(); }
+
+int rn_create(int Nx, int Nr, rn_handle* out) {
+  if (!out) return fail(RN_ERR_ARG, "rn_create: out is NULL");
+  *out = nullptr;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) return fail(RN_ERR_CUDA, std::string("no CUDA device: ") + cudaGetErrorString(e));
+  rn_solver* h = new rn_solver();
+  cudaGetDevice(&h->device);
+  e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) { delete h; return cuda_fail(e, "cudaStreamCreate"); }
+  e = cudaEventCreateWithFlags(&h->asyncEv, cudaEventDisableTiming);
+  if (e != cudaSuccess) { cudaStreamDestroy(h->stream); delete h; return cuda_fail(e, "cudaEventCreate"); }
+  int rc = alloc_buffers(h, Nx, Nr);
+  if (rc != RN_OK) {
+    std::string msg = g_err;
+    free_buffers(h);
+    cudaEventDestroy(h->asyncEv);
+    cudaStreamDestroy(h->stream);
+    delete h;
+    return fail(rc, msg);
+  }
+  *out = h;
+  return RN_OK;
+}
+
+int rn_destroy(rn_handle h) {
+  if (!h) return RN_OK;
+  cudaStreamSynchronize(h->stream);
+  free_buffers(h);
+  if (h->pinned) cudaFreeHost(h->pinned);
+  cudaEventDestroy(h->asyncEv);
+  cudaStreamDestroy(h->stream);
+  delete h;
+  return RN_OK;
+}
+
+int rn_resize(rn_handle h, int Nx, int Nr) {
+  if (!h) return fail(RN_ERR_ARG, "rn_resize: NULL handle");
+  rn_cancel_async(h);
+  CK(cudaStreamSynchronize(h->stream));
+  return alloc_buffers(h, Nx, Nr);
+}
+
+int rn_set_mask(rn_handle h, const uint8_t* mask) {
+  if (!valid(h) || !mask) return fail(RN_ERR_ARG, "rn_set_mask: bad argument");
+  const size_t N = size_t(h->Nx) * h->Nr;
+  std::vector<uint8_t> m(N);
+  for (size_t k = 0; k < N; k++) m[k] = mask[k] ? 1 : 0;
+  CK(cudaMemcpyAsync(h->mask, m.data(), N, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->wvalid = false;
+  return RN_OK;
+}
+
+int rn_set_geometry(rn_handle h, const uint8_t* mask, const float* geoA, const float* geoG, const float* geoM,
+                    const float* jWall) {
+  if (!valid(h) || !mask || !geoA || !geoG || !geoM) return fail(RN_ERR_ARG, "rn_set_geometry: bad argument");
+  // topology sanity: host offsets are -1, 0, +1 along one axis and point inside the grid
+  const int Nx = h->Nx, Nr = h->Nr;
+  for (int k = 0; k < Nx * Nr; k++) {
+    if (mask[k]) continue;
+    float hx = geoM[4 * k], hy = geoM[4 * k + 1];
+    int i = k % Nx, j = k / Nx;
+    int ix = int(std::lrint(hx)), iy = int(std::lrint(hy));
+    if (std::fabs(hx - ix) > 1e-3f || std::fabs(hy - iy) > 1e-3f || std::abs(ix) + std::abs(iy) > 1 || i + ix < 0 ||
+        i + ix >= Nx || j + iy < 0 || j + iy >= Nr)
+      return fail(RN_ERR_ARG, "rn_set_geometry: geoM host offset of cell " + std::to_string(k) + " is not a neighbour");
+    int sm = int(std::lrint(geoM[4 * k + 2])) & 15;
+    if (((sm & 1) && i == 0) || ((sm & 2) && i == Nx - 1) || ((sm & 4) && j == 0) || ((sm & 8) && j == Nr - 1))
+      return fail(RN_ERR_ARG, "rn_set_geometry: slave bit of cell " + std::to_string(k) + " points outside the grid");
+  }
+  int rc = rn_set_mask(h, mask);
+  if (rc != RN_OK) return rc;
+  const size_t N = size_t(Nx) * Nr, NF = size_t(Nx + 1) * (Nr + 1);
+  CK(cudaMemcpyAsync(h->geoA, geoA, sizeof(float4) * NF, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->geoG, geoG, sizeof(float4) * N, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->geoM, geoM, sizeof(float4) * N, cudaMemcpyHostToDevice, h->stream));
+  if (jWall) CK(cudaMemcpyAsync(h->jw, jWall, sizeof(float4) * Nx, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return RN_OK;
+}
+
+int rn_set_state(rn_handle h, const float* A, const float* B) {
+  if (!valid(h) || !A || !B) return fail(RN_ERR_ARG, "rn_set_state: bad argument");
+  const size_t N = size_t(h->Nx) * h->Nr;
+  for (int s = 0; s < 3; s++) {
+    CK(cudaMemcpyAsync(h->SA[s], A, sizeof(float4) * N, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->SB[s], B, sizeof(float4) * N, cudaMemcpyHostToDevice, h->stream));
+  }
+  CK(cudaMemsetAsync(h->stepTex, 0, sizeof(float4) * 2, h->stream));
+  h->cur = 0; h->stepIdx = 0; h->stepCount = 0; h->wvalid = false;
+  return spray_reset_dev(h);
+}
+
+int rn_get_state(rn_handle h, float* A, float* B) {
+  if (!valid(h) || !A || !B) return fail(RN_ERR_ARG, "rn_get_state: bad argument");
+  const size_t N = size_t(h->Nx) * h->Nr;
+  CK(cudaMemcpyAsync(A, h->SA[h->cur], sizeof(float4) * N, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaMemcpyAsync(B, h->SB[h->cur], sizeof(float4) * N, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return RN_OK;
+}
+
+int rn_step(rn_handle h, int n, const rn_params* P) {
+  if (!valid(h) || !P || n < 0) return fail(RN_ERR_ARG, "rn_step: bad argument");
+  const Grid g = h->grid();
+  const bool phys = P->visc || P->chem, inj = P->inj != 0;
+  for (int k = 0; k < n; k++) {
+    const int s0 = h->cur, s1 = (h->cur + 1) % 3, s2 = (h->cur + 2) % 3;
+    unsigned* wIn = h->wmax + h->wslot;
+    unsigned* wOut = h->wmax + (1 - h->wslot);
+    if (!h->wvalid) {
+      CK(cudaMemsetAsync(wIn, 0, sizeof(unsigned), h->stream));
+      launch_reduce(g, h->SA[s0], h->SB[s0], wIn, h->stream);
+      h->launches++;
+    }
+    float4* stPrev = h->stepTex + h->stepIdx;
+    float4* stNew = h->stepTex + (1 - h->stepIdx);
+    StageArgs a;
+    a.g = g;
+    a.A = h->SA[s0]; a.B = h->SB[s0]; a.A0 = h->SA[s0]; a.B0 = h->SB[s0];
+    a.oA = h->SA[s1]; a.oB = h->SB[s1];
+    a.stPrev = stPrev; a.stNew = stNew; a.wIn = wIn; a.wOut = wOut;
+    a.finalCfl = 0;
+    launch_stage1(a, *P, h->stream);
+    h->launches++;
+    if (inj) {
+      SprayArgs sp;
+      sp.g = g;
+      sp.A1 = h->SA[s1]; sp.B1 = h->SB[s1];
+      sp.PA = h->PA[h->scur]; sp.PB = h->PB[h->scur];
+      sp.oPA = h->PA[1 - h->scur]; sp.oPB = h->PB[1 - h->scur]; sp.oPC = h->PC[1 - h->scur];
+      sp.tab = h->tab; sp.st = stNew;
+      sp.key = h->key; sp.val = h->val; sp.dep = h->dep;
+      sp.head = int(h->head); sp.seed = int(h->seed);
+      int launched = 0;
+      if (launch_spray(sp, *P, h->sortTemp, h->sortTempBytes, h->keyS, h->valS, h->src, h->stream, &launched) != 0)
+        return fail(RN_ERR_CUDA, "rn_step: deposit sort failed");
+      h->launches += launched;
+    }
+    StageArgs b = a;
+    b.A = h->SA[s1]; b.B = h->SB[s1]; b.A0 = h->SA[s0]; b.B0 = h->SB[s0];
+    b.oA = h->SA[s2]; b.oB = h->SB[s2];
+    b.finalCfl = (!phys && !inj) ? 1 : 0;
+    launch_stage2(b, *P, h->stream);
+    h->launches++;
+    h->cur = s2;
+    if (phys) {
+      PhysArgs p;
+      p.g = g;
+      p.A1 = h->SA[s1]; p.B1 = h->SB[s1]; p.A2 = h->SA[s2]; p.B2 = h->SB[s2];
+      p.oA = h->SA[s0]; p.oB = h->SB[s0];
+      p.st = stNew; p.wOut = wOut; p.finalCfl = inj ? 0 : 1;
+      launch_physics(p, *P, h->stream);
+      h->launches++;
+      h->cur = s0;
+    }
+    if (inj) {
+      const int out = (h->cur + 1) % 3;
+      ApplyArgs ap;
+      ap.g = g;
+      ap.A = h->SA[h->cur]; ap.B = h->SB[h->cur]; ap.src = h->src;
+      ap.oA = h->SA[out]; ap.oB = h->SB[out];
+      ap.wOut = wOut; ap.finalCfl = 1;
+      launch_apply(ap, *P, h->stream);
+      h->launches++;
+      h->cur = out;
+      h->scur = 1 - h->scur;
+      h->head = (h->head + 4) % SPRAY_N;
+      h->seed = h->seed + 1u;
+    }
+    h->stepIdx = 1 - h->stepIdx;
+    h->wslot = 1 - h->wslot;
+    h->wvalid = true;
+    h->stepCount++;
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e, "rn_step launch");
+  return RN_OK;
+}
+
+int rn_rescale_ambient(rn_handle h, float fp, float fT, float du, const rn_params* P) {
+  if (!valid(h) || !P) return fail(RN_ERR_ARG, "rn_rescale_ambient: bad argument");
+  const int s0 = h->cur, s1 = (h->cur + 1) % 3;
+  launch_rescale(h->grid(), h->SA[s0], h->SB[s0], h->SA[s1], h->SB[s1], fp, fT, du, *P, h->stream);
+  h->launches++;
+  h->cur = s1;
+  h->wvalid = false;
+  CK(cudaGetLastError());
+  return RN_OK;
+}
+
+int rn_draw_wall_row(rn_handle h) {
+  if (!valid(h)) return fail(RN_ERR_ARG, "rn_draw_wall_row: bad handle");
+  launch_wallrow(h->grid(), h->SA[h->cur], h->SB[h->cur], h->jw, h->wallRow, h->stream);
+  h->launches++;
+  CK(cudaGetLastError());
+  return RN_OK;
+}
+
+}  // extern "C"
+
+namespace {
+// device pointer, row pitch (float4) and extent of a named texture
+int tex_ptr(rn_solver* h, int tex, const float4** p, int* W, int* H) {
+  switch (tex) {
+    case RN_TEX_A: *p = h->SA[h->cur]; *W = h->Nx; *H = h->Nr; return RN_OK;
+    case RN_TEX_B: *p = h->SB[h->cur]; *W = h->Nx; *H = h->Nr; return RN_OK;
+    case RN_TEX_STEPINFO: *p = h->stepTex + h->stepIdx; *W = 1; *H = 1; return RN_OK;
+    case RN_TEX_WALLROW: *p = h->wallRow; *W = h->Nx; *H = 1; return RN_OK;
+    case RN_TEX_PARCEL_A: *p = h->PA[h->scur]; *W = 256; *H = 256; return RN_OK;
+    case RN_TEX_PARCEL_B: *p = h->PB[h->scur]; *W = 256; *H = 256; return RN_OK;
+    case RN_TEX_PARCEL_C: *p = h->PC[h->scur]; *W = 256; *H = 256; return RN_OK;
+    default: return fail(RN_ERR_ARG, "unknown texture " + std::to_string(tex));
+  }
+}
+int queue_rect(rn_solver* h, int tex, int x, int y, int w, int hgt, float* dst) {
+  const float4* p;
+  int W, H;
+  int rc = tex_ptr(h, tex, &p, &W, &H);
+  if (rc != RN_OK) return rc;
+  if (x < 0 || y < 0 || w < 0 || hgt < 0 || x + w > W || y + hgt > H) return fail(RN_ERR_ARG, "read rectangle out of range");
+  if (w == 0 || hgt == 0) return RN_OK;
+  CK(cudaMemcpy2DAsync(dst, sizeof(float4) * w, p + size_t(y) * W + x, sizeof(float4) * W, sizeof(float4) * w, hgt,
+                       cudaMemcpyDeviceToHost, h->stream));
+  return RN_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int rn_read_rect(rn_handle h, int tex, int x, int y, int w, int hgt, float* out) {
+  if (!valid(h) || !out) return fail(RN_ERR_ARG, "rn_read_rect: bad argument");
+  int rc = queue_rect(h, tex, x, y, w, hgt, out);
+  if (rc != RN_OK) return rc;
+  CK(cudaStreamSynchronize(h->stream));
+  return RN_OK;
+}
+
+int rn_read_step_info(rn_handle h, float out[4]) { return rn_read_rect(h, RN_TEX_STEPINFO, 0, 0, 1, 1, out); }
+
+int rn_request_async(rn_handle h, const rn_read_req* reqs, int nreq, int tag) {
+  if (!valid(h) || (nreq > 0 && !reqs) || nreq < 0) return fail(RN_ERR_ARG, "rn_request_async: bad argument");
+  if (h->asyncBusy) return RN_BUSY;
+  size_t total = 0;
+  for (int r = 0; r < nreq; r++) total += size_t(reqs[r].w) * reqs[r].h * 4;
+  if (total > h->pinnedCap) {
+    if (h->pinned) cudaFreeHost(h->pinned);
+    h->pinned = nullptr;
+    h->pinnedCap = 0;
+    CK(cudaHostAlloc(&h->pinned, sizeof(float) * (total > 0 ? total : 4), cudaHostAllocDefault));
+    h->pinnedCap = total;
+  }
+  size_t off = 0;
+  for (int r = 0; r < nreq; r++) {
+    int rc = queue_rect(h, reqs[r].tex, reqs[r].x, reqs[r].y, reqs[r].w, reqs[r].h, h->pinned + off);
+    if (rc != RN_OK) return rc;
+    off += size_t(reqs[r].w) * reqs[r].h * 4;
+  }
+  CK(cudaEventRecord(h->asyncEv, h->stream));
+  h->asyncBusy = true;
+  h->asyncTag = tag;
+  h->asyncFloats = total;
+  return RN_OK;
+}
+
+int rn_poll_async(rn_handle h, int* tag, float* out, size_t cap_floats) {
+  if (!valid(h)) return fail(RN_ERR_ARG, "rn_poll_async: bad handle");
+  if (!h->asyncBusy) return fail(RN_ERR_STATE, "rn_poll_async: no read in flight");
+  cudaError_t e = cudaEventQuery(h->asyncEv);
+  if (e == cudaErrorNotReady) return RN_NOT_READY;
+  if (e != cudaSuccess) return cuda_fail(e, "cudaEventQuery");
+  if (cap_floats < h->asyncFloats) return fail(RN_ERR_ARG, "rn_poll_async: output buffer too small");
+  if (out && h->asyncFloats) std::memcpy(out, h->pinned, sizeof(float) * h->asyncFloats);
+  if (tag) *tag = h->asyncTag;
+  h->asyncBusy = false;
+  return RN_OK;
+}
+
+int rn_cancel_async(rn_handle h) {
+  if (!h) return RN_OK;
+  if (h->asyncBusy) cudaEventSynchronize(h->asyncEv);
+  h->asyncBusy = false;
+  return RN_OK;
+}
+
+int rn_spray_set_injector(rn_handle h, const float* tab) {
+  if (!valid(h) || !tab) return fail(RN_ERR_ARG, "rn_spray_set_injector: bad argument");
+  CK(cudaMemcpyAsync(h->tab, tab, sizeof(float4) * 768, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return RN_OK;
+}
+
+int rn_spray_reset(rn_handle h) {
+  if (!valid(h)) return fail(RN_ERR_ARG, "rn_spray_reset: bad handle");
+  return spray_reset_dev(h);
+}
+
+int rn_spray_stats(rn_handle h, double out[4]) {
+  if (!valid(h) || !out) return fail(RN_ERR_ARG, "rn_spray_stats: bad argument");
+  std::vector<float4> b(SPRAY_N);
+  CK(cudaMemcpyAsync(b.data(), h->PB[h->scur], sizeof(float4) * SPRAY_N, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  double f = 0, o = 0, dS = 0;
+  long long n = 0;
+  for (int k = 0; k < SPRAY_N; k++) {
+    double m = b[k].y;
+    if (m > 0) {
+      n++;
+      dS += b[k].x;
+      if (b[k].z < 0.5f) f += m; else o += m;
+    }
+  }
+  out[0] = f; out[1] = o; out[2] = double(n); out[3] = n ? dS / double(n) : 0.0;
+  return RN_OK;
+}
+
+int rn_integrals(rn_handle h, const rn_integral_spec* spec, rn_integrals_out* out) {
+  if (!valid(h) || !spec || !out) return fail(RN_ERR_ARG, "rn_integrals: bad argument");
+  if (spec->iExit < 0 || spec->iExit + 1 > h->Nx || spec->jExit < 0 || spec->jExit > h->Nr || spec->iThroat < 0 ||
+      spec->iThroat >= h->Nx || spec->iChamber < 0 || spec->iChamber >= h->Nx)
+    return fail(RN_ERR_ARG, "rn_integrals: column index out of range");
+  launch_integrals(h->grid(), h->SA[h->cur], h->SB[h->cur], h->geoA, *spec, h->stepTex + h->stepIdx, h->dInt,
+                   h->stream);
+  h->launches++;
+  double r[12];
+  CK(cudaMemcpyAsync(r, h->dInt, sizeof(r), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  out->F = r[0]; out->mdot = r[1]; out->Mw = r[2]; out->pw = r[3]; out->A = r[4];
+  out->throat_mdot = r[5]; out->throat_mO = r[6]; out->throat_mF = r[7];
+  out->chamber_p = r[8]; out->chamber_T = r[9]; out->dt = r[10]; out->t = r[11];
+  return RN_OK;
+}
+
+int rn_sync(rn_handle h) {
+  if (!h) return fail(RN_ERR_ARG, "rn_sync: NULL handle");
+  CK(cudaStreamSynchronize(h->stream));
+  return RN_OK;
+}
+
+int rn_wait(rn_handle h, int timeout_ms) {
+  if (!h) return fail(RN_ERR_ARG, "rn_wait: NULL handle");
+  auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    cudaError_t e = cudaStreamQuery(h->stream);
+    if (e == cudaSuccess) return RN_OK;
+    if (e != cudaErrorNotReady) return cuda_fail(e, "cudaStreamQuery");
+    auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - t0).count();
+    if (ms >= timeout_ms) return RN_NOT_READY;
+    std::this_thread::sleep_for(std::chrono::microseconds(200));
+  }
+}
+
+int rn_kernel_launches(rn_handle h, long long* out) {
+  if (!h || !out) return fail(RN_ERR_ARG, "rn_kernel_launches: bad argument");
+  *out = h->launches;
+  return RN_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,69 @@
+// rn_kernels.cuh -- kernel argument blocks and launch helpers shared by the
+// step kernels (rn_step.cu), the spray kernels (rn_spray.cu) and the C-ABI
+// (rn_api.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include "rn_math.cuh"
+
+namespace rn {
+
+// Tile of one stage/physics block: TX x TY cells, one thread per cell.
+constexpr int TX = 32, TY = 8, NT = TX * TY;
+
+struct StageArgs {
+  Grid g;
+  const float4* A;  const float4* B;    // stage input state
+  const float4* A0; const float4* B0;   // state at t^n (stage 2)
+  float4* oA; float4* oB;               // stage output
+  const float4* stPrev;                 // stage 1: step info of the previous step
+  float4* stNew;                        // stage 1 writes it, later kernels read it
+  const unsigned* wIn;                  // stage 1: max wave speed of the step's input state
+  unsigned* wOut;                       // cleared by stage 1, accumulated by the step's last kernel
+  int finalCfl;                         // this kernel writes the step's final state
+};
+
+struct PhysArgs {
+  Grid g;
+  const float4* A1; const float4* B1;   // stage-1 result (its primitives feed the viscous terms)
+  const float4* A2; const float4* B2;   // stage-2 result (updated here)
+  float4* oA; float4* oB;
+  const float4* st;
+  unsigned* wOut;
+  int finalCfl;
+};
+
+struct SprayArgs {
+  Grid g;
+  const float4* A1; const float4* B1;   // stage-1 state: the gas the parcels see
+  const float4* PA; const float4* PB;   // parcels before the step
+  float4* oPA; float4* oPB; float4* oPC;
+  const float4* tab;                    // 256 x 3 injector table
+  const float4* st;
+  unsigned* key; unsigned* val; float4* dep;   // deposit records (cell key, parcel index, source)
+  int head, seed;
+};
+
+struct ApplyArgs {
+  Grid g;
+  const float4* A; const float4* B;
+  const float4* src;
+  float4* oA; float4* oB;
+  unsigned* wOut;
+  int finalCfl;
+};
+
+void launch_stage1(const StageArgs& a, const rn_params& P, cudaStream_t s);
+void launch_stage2(const StageArgs& a, const rn_params& P, cudaStream_t s);
+void launch_physics(const PhysArgs& a, const rn_params& P, cudaStream_t s);
+void launch_reduce(const Grid& g, const float4* A, const float4* B, unsigned* w, cudaStream_t s);
+void launch_rescale(const Grid& g, const float4* A, const float4* B, float4* oA, float4* oB, float fp, float fT,
+                    float du, const rn_params& P, cudaStream_t s);
+void launch_wallrow(const Grid& g, const float4* A, const float4* B, const float4* jw, float4* row, cudaStream_t s);
+void launch_integrals(const Grid& g, const float4* A, const float4* B, const float4* geoAx, const rn_integral_spec& spec,
+                      const float4* st, double* out, cudaStream_t s);
+int launch_spray(const SprayArgs& a, const rn_params& P, void* sortTemp, size_t sortTempBytes, unsigned* keyOut,
+                 unsigned* valOut, float4* src, cudaStream_t s, int* launches);
+void launch_apply(const ApplyArgs& a, const rn_params& P, cudaStream_t s);
+size_t spray_sort_temp_bytes(int Ncells);
+
+}  // namespace rn

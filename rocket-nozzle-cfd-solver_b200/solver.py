@@ -1,0 +1,377 @@
+"""GPUSolver / GPUSpray: the reference's JavaScript solver API over librn.so.
+
+Mirrors ``GPUSolver`` (source/solver.js:677-1076) and ``GPUSpray``
+(source/spray.js:211-321) method for method, with the CUDA library declared in
+``include/rn.h`` in place of the WebGL2 context. Textures are named by the
+``RN_TEX_*`` ids; ``state`` returns ``{"A": RN_TEX_A, "B": RN_TEX_B}`` so a
+caller can build ``requestAsync`` requests exactly as ``app.js`` does.
+
+There is no CPU fallback: constructing a solver without the library or
+without a CUDA device raises.
+"""
+import ctypes
+import math
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "librn.so")
+
+RN_OK, RN_NOT_READY, RN_BUSY = 0, 1, 2
+RN_TEX_A, RN_TEX_B, RN_TEX_STEPINFO, RN_TEX_WALLROW = 0, 1, 2, 3
+RN_TEX_PARCEL_A, RN_TEX_PARCEL_B, RN_TEX_PARCEL_C = 4, 5, 6
+SPRAY_W = SPRAY_H = 256
+SPRAY_N = SPRAY_W * SPRAY_H
+
+EXPORTS = ("rn_create", "rn_destroy", "rn_resize", "rn_set_mask", "rn_set_geometry", "rn_set_state",
+           "rn_get_state", "rn_step", "rn_rescale_ambient", "rn_draw_wall_row", "rn_read_rect",
+           "rn_read_step_info", "rn_request_async", "rn_poll_async", "rn_cancel_async", "rn_spray_set_injector",
+           "rn_spray_reset", "rn_spray_stats", "rn_integrals", "rn_sync", "rn_wait", "rn_kernel_launches",
+           "rn_last_error")
+
+
+class RnError(RuntimeError):
+    """A librn.so call returned an error code."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"librn error {code}: {msg}")
+        self.code = code
+
+
+class RnParams(ctypes.Structure):
+    """``rn_params`` (include/rn.h): the float32 uniforms of P."""
+    _fields_ = [
+        ("amb", ctypes.c_float * 4), ("ambCons", ctypes.c_float * 4), ("ambB", ctypes.c_float * 4),
+        ("gamR", ctypes.c_float * 2), ("inlet", ctypes.c_float * 4), ("bar", ctypes.c_float * 3),
+        ("res", ctypes.c_float * 3), ("gas", ctypes.c_float * 4), ("Rs", ctypes.c_float * 3),
+        ("chemK", ctypes.c_float * 4), ("cap", ctypes.c_float * 2), ("chamberNu", ctypes.c_float * 2),
+        ("Tw", ctypes.c_float), ("cfl", ctypes.c_float), ("dtMax", ctypes.c_float), ("wFloor", ctypes.c_float),
+        ("vMax", ctypes.c_float), ("hllBlend", ctypes.c_float), ("ramp", ctypes.c_float),
+        ("pStart", ctypes.c_float), ("RcCells", ctypes.c_float),
+        ("order2", ctypes.c_int), ("inj", ctypes.c_int), ("visc", ctypes.c_int), ("chem", ctypes.c_int),
+        ("mhat", ctypes.c_float), ("tScale", ctypes.c_float),
+        ("fuel", ctypes.c_float * 4), ("ox", ctypes.c_float * 4),
+        ("eF", ctypes.c_float), ("eO", ctypes.c_float), ("Ge", ctypes.c_float), ("fan", ctypes.c_float),
+    ]
+
+
+class RnReadReq(ctypes.Structure):
+    _fields_ = [("tex", ctypes.c_int), ("x", ctypes.c_int), ("y", ctypes.c_int), ("w", ctypes.c_int),
+                ("h", ctypes.c_int)]
+
+
+class RnIntegralSpec(ctypes.Structure):
+    _fields_ = [("iExit", ctypes.c_int), ("jExit", ctypes.c_int), ("iThroat", ctypes.c_int),
+                ("iChamber", ctypes.c_int), ("dx", ctypes.c_double), ("pAmb", ctypes.c_double),
+                ("Rs", ctypes.c_double * 3), ("RaN", ctypes.c_double), ("inj", ctypes.c_int)]
+
+
+class RnIntegralsOut(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in ("F", "mdot", "Mw", "pw", "A", "throat_mdot", "throat_mO",
+                                               "throat_mF", "chamber_p", "chamber_T", "dt", "t")]
+
+
+def params_from_P(P):
+    """Round the reference's parameter block ``P`` to the uniforms the shaders
+    receive (``gl.uniform*fv`` converts JavaScript doubles to float32)."""
+    p = RnParams()
+    for n in ("amb", "ambCons", "ambB", "gamR", "inlet", "res", "gas", "Rs", "chemK", "cap", "chamberNu"):
+        arr = getattr(p, n)
+        for k, v in enumerate(P[n]):
+            arr[k] = float(v)
+    # uBar = (inlet[0], 1.6 uInlet0, max(ramp, 0)) formed in doubles (solver.js:935)
+    p.bar[0] = float(P["inlet"][0])
+    p.bar[1] = 1.6 * float(P["uInlet0"])
+    p.bar[2] = max(float(P["ramp"]), 0.0)
+    for n in ("Tw", "cfl", "dtMax", "wFloor", "vMax", "hllBlend", "ramp", "pStart", "RcCells"):
+        setattr(p, n, float(P[n]))
+    p.order2 = 1 if P["order2"] else 0
+    p.inj = 1 if P["inj"] else 0
+    p.visc = 1 if P["visc"] else 0
+    p.chem = 1 if P["chem"] else 0
+    p.fan = 25 * math.pi / 180                   # spray.js:271
+    if P.get("inj"):
+        d = P["injData"]
+        p.mhat = P["spray"]["mhat"]
+        p.tScale = P["spray"]["tScale"]
+        for k in range(4):
+            p.fuel[k] = d["fuelVec"][k]
+            p.ox[k] = d["oxVec"][k]
+        p.eF, p.eO, p.Ge = d["eF"], d["eO"], d["Ge"]
+    return p
+
+
+_lib = None
+
+
+def lib():
+    """Load librn.so once; raise if it is missing (no CPU fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RnError(-100, f"{LIB_PATH} is not built; run __graft_entry__.build()")
+    L = ctypes.CDLL(LIB_PATH)
+    H = ctypes.c_void_p
+    i, f = ctypes.c_int, ctypes.c_float
+    fp = ctypes.POINTER(ctypes.c_float)
+    L.rn_create.argtypes = [i, i, ctypes.POINTER(H)]
+    L.rn_destroy.argtypes = [H]
+    L.rn_resize.argtypes = [H, i, i]
+    L.rn_set_mask.argtypes = [H, ctypes.c_void_p]
+    L.rn_set_geometry.argtypes = [H, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                  ctypes.c_void_p]
+    L.rn_set_state.argtypes = [H, ctypes.c_void_p, ctypes.c_void_p]
+    L.rn_get_state.argtypes = [H, ctypes.c_void_p, ctypes.c_void_p]
+    L.rn_step.argtypes = [H, i, ctypes.POINTER(RnParams)]
+    L.rn_rescale_ambient.argtypes = [H, f, f, f, ctypes.POINTER(RnParams)]
+    L.rn_draw_wall_row.argtypes = [H]
+    L.rn_read_rect.argtypes = [H, i, i, i, i, i, ctypes.c_void_p]
+    L.rn_read_step_info.argtypes = [H, fp]
+    L.rn_request_async.argtypes = [H, ctypes.POINTER(RnReadReq), i, i]
+    L.rn_poll_async.argtypes = [H, ctypes.POINTER(i), ctypes.c_void_p, ctypes.c_size_t]
+    L.rn_cancel_async.argtypes = [H]
+    L.rn_spray_set_injector.argtypes = [H, ctypes.c_void_p]
+    L.rn_spray_reset.argtypes = [H]
+    L.rn_spray_stats.argtypes = [H, ctypes.POINTER(ctypes.c_double)]
+    L.rn_integrals.argtypes = [H, ctypes.POINTER(RnIntegralSpec), ctypes.POINTER(RnIntegralsOut)]
+    L.rn_sync.argtypes = [H]
+    L.rn_wait.argtypes = [H, i]
+    L.rn_kernel_launches.argtypes = [H, ctypes.POINTER(ctypes.c_longlong)]
+    L.rn_last_error.restype = ctypes.c_char_p
+    for n in EXPORTS[:-1]:
+        getattr(L, n).restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def _check(rc, allowed=(RN_OK,)):
+    if rc in allowed:
+        return rc
+    raise RnError(rc, lib().rn_last_error().decode())
+
+
+def _f32(a, n=None):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    if n is not None and a.size != n:
+        raise ValueError(f"expected {n} floats, got {a.size}")
+    return a
+
+
+class GPUSolver:
+    """The reference's ``GPUSolver`` (solver.js:677) on a B200 via librn.so."""
+
+    def __init__(self, Nx=0, Nr=0):
+        self.h = ctypes.c_void_p()
+        self.Nx = self.Nr = 0
+        self.stepCount = 0
+        self.spray = None
+        self._async = None
+        if Nx and Nr:
+            self.resize(Nx, Nr)
+
+    # ---- lifetime
+    def resize(self, Nx, Nr):
+        """solver.js:759-789"""
+        L = lib()
+        if self.h.value:
+            _check(L.rn_resize(self.h, int(Nx), int(Nr)))
+        else:
+            _check(L.rn_create(int(Nx), int(Nr), ctypes.byref(self.h)))
+        self.Nx, self.Nr = int(Nx), int(Nr)
+        self._async = None
+        if self.spray is not None:
+            self.spray.resize()
+
+    def close(self):
+        if self.h.value:
+            lib().rn_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- uploads
+    def setMask(self, u8):
+        """solver.js:791-799"""
+        m = np.ascontiguousarray(u8, dtype=np.uint8)
+        _check(lib().rn_set_mask(self.h, m.ctypes.data))
+        self.maskData = u8
+
+    def setGeometry(self, geo):
+        """solver.js:801-814"""
+        N, NF = self.Nx * self.Nr, (self.Nx + 1) * (self.Nr + 1)
+        m = np.ascontiguousarray(geo["mask"], dtype=np.uint8)
+        gA, gG, gM = _f32(geo["geoA"], NF * 4), _f32(geo["geoG"], N * 4), _f32(geo["geoM"], N * 4)
+        jw = geo.get("jWall")
+        jwp = None
+        if jw is not None:
+            jw = _f32(jw, self.Nx * 4)
+            jwp = jw.ctypes.data
+        _check(lib().rn_set_geometry(self.h, m.ctypes.data, gA.ctypes.data, gG.ctypes.data, gM.ctypes.data, jwp))
+        self.maskData = geo["mask"]
+
+    def setState(self, A, B):
+        """solver.js:816-828: every state slot; clears dt/t and the spray ring."""
+        N = self.Nx * self.Nr * 4
+        a, b = _f32(A, N), _f32(B, N)
+        _check(lib().rn_set_state(self.h, a.ctypes.data, b.ctypes.data))
+        self.stepCount = 0
+
+    # ---- the hot path
+    def step(self, n, P):
+        """solver.js:849-891 (+ GPUSpray.step when P.inj): queued, returns at once."""
+        p = P if isinstance(P, RnParams) else params_from_P(P)
+        if p.inj and self.spray is None:
+            # the app attaches a GPUSpray on every restart (app.js:239); the
+            # handle always owns the parcel ring, so attach its front end here
+            GPUSpray(self).resize()
+        _check(lib().rn_step(self.h, int(n), ctypes.byref(p)))
+        self.stepCount += int(n)
+
+    def rescaleAmbient(self, fp, fT, du, P):
+        """solver.js:998-1010"""
+        p = P if isinstance(P, RnParams) else params_from_P(P)
+        _check(lib().rn_rescale_ambient(self.h, float(fp), float(fT), float(du), ctypes.byref(p)))
+
+    def drawWallRow(self):
+        """solver.js:986-996: returns the wall-row texture id."""
+        _check(lib().rn_draw_wall_row(self.h))
+        return RN_TEX_WALLROW
+
+    @property
+    def state(self):
+        return {"A": RN_TEX_A, "B": RN_TEX_B}
+
+    @property
+    def stepInfoTex(self):
+        return RN_TEX_STEPINFO
+
+    # ---- read-backs (solver.js:1016-1075)
+    def _readRect(self, tex, x, y, w, h):
+        out = np.empty(int(w) * int(h) * 4, dtype=np.float32)
+        _check(lib().rn_read_rect(self.h, int(tex), int(x), int(y), int(w), int(h), out.ctypes.data))
+        return out
+
+    def readStepInfo(self):
+        return self._readRect(RN_TEX_STEPINFO, 0, 0, 1, 1)
+
+    def readColumn(self, i):
+        return {"A": self._readRect(RN_TEX_A, i, 0, 1, self.Nr), "B": self._readRect(RN_TEX_B, i, 0, 1, self.Nr)}
+
+    def readCell(self, i, j):
+        return {"A": self._readRect(RN_TEX_A, i, j, 1, 1), "B": self._readRect(RN_TEX_B, i, j, 1, 1)}
+
+    def readAll(self):
+        N = self.Nx * self.Nr * 4
+        A, B = np.empty(N, dtype=np.float32), np.empty(N, dtype=np.float32)
+        _check(lib().rn_get_state(self.h, A.ctypes.data, B.ctypes.data))
+        return {"A": A, "B": B}
+
+    def requestAsync(self, reqs, tag):
+        """solver.js:1028-1048. reqs: [{name, tex, x, y, w, h}]; False while a read is in flight."""
+        arr = (RnReadReq * len(reqs))()
+        offs, floats = [], 0
+        for k, r in enumerate(reqs):
+            arr[k].tex, arr[k].x, arr[k].y, arr[k].w, arr[k].h = r["tex"], r["x"], r["y"], r["w"], r["h"]
+            offs.append(floats)
+            floats += r["w"] * r["h"] * 4
+        rc = _check(lib().rn_request_async(self.h, arr, len(reqs), int(tag)), (RN_OK, RN_BUSY))
+        if rc == RN_BUSY:
+            return False
+        self._async = {"reqs": reqs, "offs": offs, "floats": floats, "tag": tag}
+        return True
+
+    def pollAsync(self):
+        """solver.js:1050-1065: {tag, data: {name: array}} once ready, else None."""
+        a = self._async
+        if a is None:
+            return None
+        out = np.empty(max(a["floats"], 1), dtype=np.float32)
+        tag = ctypes.c_int()
+        rc = _check(lib().rn_poll_async(self.h, ctypes.byref(tag), out.ctypes.data, out.size), (RN_OK, RN_NOT_READY))
+        if rc == RN_NOT_READY:
+            return None
+        self._async = None
+        data = {r["name"]: out[o:o + r["w"] * r["h"] * 4] for r, o in zip(a["reqs"], a["offs"])}
+        return {"tag": tag.value, "data": data, "probe": a.get("probe")}
+
+    def cancelAsync(self):
+        """solver.js:1066-1070"""
+        if self.h.value:
+            lib().rn_cancel_async(self.h)
+        self._async = None
+
+    # ---- extras of the C-ABI
+    def integrals(self, setup):
+        """FP64 exit/throat/chamber read-outs (rn_integrals) in the reference's
+        normalised units, for ``setup`` from build_sim_setup."""
+        P = setup["P"]
+        s = RnIntegralSpec()
+        s.iExit, s.jExit, s.iThroat, s.iChamber = setup["iExit"], setup["jExit"], setup["iThroat"], setup["iChamber"]
+        s.dx = setup["dx"]
+        s.pAmb = P["amb"][3]
+        for k in range(3):
+            s.Rs[k] = P["Rs"][k]
+        s.RaN = P["RaN"]
+        s.inj = 1 if P["inj"] else 0
+        o = RnIntegralsOut()
+        _check(lib().rn_integrals(self.h, ctypes.byref(s), ctypes.byref(o)))
+        return {n: getattr(o, n) for n, _ in RnIntegralsOut._fields_}
+
+    def sync(self):
+        _check(lib().rn_sync(self.h))
+
+    def wait(self, timeout_ms):
+        """Bounded wait for the queued work: True when done, False on timeout."""
+        return _check(lib().rn_wait(self.h, int(timeout_ms)), (RN_OK, RN_NOT_READY)) == RN_OK
+
+    def kernelLaunches(self):
+        v = ctypes.c_longlong()
+        _check(lib().rn_kernel_launches(self.h, ctypes.byref(v)))
+        return v.value
+
+
+class GPUSpray:
+    """The reference's ``GPUSpray`` (spray.js:211-321): the parcel ring lives in
+    the solver handle; this object carries the injector table and read-outs."""
+
+    def __init__(self, solver):
+        self.s = solver
+        self.blendOk = True          # the deposit is a sorted reduction, no float blending needed
+        self.ready = False
+        solver.spray = self
+
+    def resize(self):
+        """spray.js:224-235 (the ring is allocated with the solver)."""
+        self.ready = True
+        self.reset()
+
+    def setInjector(self, inj):
+        """spray.js:236-241"""
+        if not inj or not self.ready:
+            return
+        tab = _f32(inj["tab"], 256 * 3 * 4)
+        _check(lib().rn_spray_set_injector(self.s.h, tab.ctypes.data))
+
+    def reset(self):
+        """spray.js:242-254"""
+        if not self.ready:
+            return
+        _check(lib().rn_spray_reset(self.s.h))
+
+    def stats(self, P=None):
+        """spray.js:312-320: {fuel, ox, parcels, meanD}."""
+        out = (ctypes.c_double * 4)()
+        _check(lib().rn_spray_stats(self.s.h, out))
+        return {"fuel": out[0], "ox": out[1], "parcels": int(out[2]), "meanD": out[3]}
+
+    def readParcels(self):
+        """The current parcel textures PA, PB, PC (65,536 x 4 each)."""
+        r = self.s._readRect
+        return {"PA": r(RN_TEX_PARCEL_A, 0, 0, 256, 256), "PB": r(RN_TEX_PARCEL_B, 0, 0, 256, 256),
+                "PC": r(RN_TEX_PARCEL_C, 0, 0, 256, 256)}
