@@ -150,6 +150,25 @@ int rn_sync(rn_handle h);
 int rn_wait(rn_handle h, int timeout_ms);
 /* number of kernels this handle has launched (for launch accounting) */
 int rn_kernel_launches(rn_handle h, long long* out);
+/* the handle's CUDA stream (a cudaStream_t), so a caller can order its own
+ * work (timing events, cache flushes) with the handle's kernels */
+int rn_get_stream(rn_handle h, void** stream);
+
+/* Per-kernel device time: with profiling on, every kernel the handle launches
+ * is bracketed by CUDA events on its stream. rn_profile_read waits for the
+ * stream, returns milliseconds and launch counts per kernel kind (indexed by
+ * RN_K_*) accumulated since the last read, and clears them. */
+#define RN_K_REDUCE 0
+#define RN_K_STAGE1 1
+#define RN_K_STAGE2 2
+#define RN_K_PHYSICS 3
+#define RN_K_PARCELS 4   /* parcel update + deposit sort + segment sums */
+#define RN_K_APPLY 5
+#define RN_K_OTHER 6     /* rescale, wall row, integrals */
+#define RN_NKERNELS 7
+int rn_profile(rn_handle h, int enable);
+int rn_profile_read(rn_handle h, double ms[RN_NKERNELS], long long launches[RN_NKERNELS]);
+
 /* message of the calling thread's last error ("" if none) */
 const char* rn_last_error(void);
 

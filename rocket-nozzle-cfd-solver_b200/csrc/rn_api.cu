@@ -14,6 +14,7 @@
 #include <cstring>
 #include <string>
 #include <thread>
+#include <algorithm>
 #include <vector>
 #include "rn.h"
 #include "rn_kernels.cuh"
@@ -69,6 +70,16 @@ struct rn_solver {
   bool asyncBusy = false;
   int asyncTag = 0;
   double* dInt = nullptr;
+  // per-kernel event timing
+  bool prof = false;
+  std::vector<cudaEvent_t> evPool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> evPending;
+  double profMs[RN_NKERNELS] = {0};
+  long long profN[RN_NKERNELS] = {0};
+  // per tile of the stage/physics kernels: out-of-tile members of its groups
+  int* xoff = nullptr;
+  int* xcell = nullptr;
+  int maxX = 1;
 
   Grid grid() const { return Grid{Nx, Nr, mask, geoA, geoG, geoM}; }
 };
@@ -83,6 +94,9 @@ void free_buffers(rn_solver* h) {
   cudaFree(h->PA[0]);   // base of the 6-plane parcel ring
   for (int p = 0; p < 2; p++) h->PA[p] = h->PB[p] = h->PC[p] = nullptr;
   cudaFree(h->src); cudaFree(h->tab); cudaFree(h->dep); cudaFree(h->key); cudaFree(h->sortTemp);
+  cudaFree(h->xoff); cudaFree(h->xcell);
+  h->xoff = h->xcell = nullptr;
+  h->maxX = 1;
   h->geoA = h->geoG = h->geoM = h->jw = h->wallRow = nullptr;
   h->mask = nullptr; h->stepTex = nullptr; h->wmax = nullptr; h->dInt = nullptr;
   h->src = h->tab = h->dep = nullptr;
@@ -152,12 +166,98 @@ int alloc_buffers(rn_solver* h, int Nx, int Nr) {
   CK(cudaMalloc(&h->sortTemp, h->sortTempBytes > 0 ? h->sortTempBytes : 16));
   h->cur = 0; h->stepIdx = 0; h->wslot = 0; h->wvalid = false; h->stepCount = 0;
   h->seed = 1;
+  // empty per-tile member lists until a geometry is set
+  const int nT = ((Nx + TX - 1) / TX) * ((Nr + TY - 1) / TY);
+  CK(cudaMalloc(&h->xoff, sizeof(int) * (nT + 1)));
+  CK(cudaMemsetAsync(h->xoff, 0, sizeof(int) * (nT + 1), h->stream));
+  CK(cudaMalloc(&h->xcell, sizeof(int)));
+  CK(cudaMemsetAsync(h->xcell, 0, sizeof(int), h->stream));
+  h->maxX = 1;
   return spray_reset_dev(h);
+}
+
+constexpr int MAXX_CAP = MAXX;   // out-of-tile group members one tile may list
+
+// Per tile, the cells outside it that belong to a cut-cell group with a cell
+// inside it (a sliver merged across the tile edge). Groups are a host plus the
+// slaves of its slave mask (geoM.z bits 1/2/4/8, cutcell.js:168-174).
+int build_member_lists(rn_solver* h, const uint8_t* mask, const float* geoM) {
+  const int Nx = h->Nx, Nr = h->Nr, tx = (Nx + TX - 1) / TX, nT = tx * ((Nr + TY - 1) / TY);
+  std::vector<std::vector<int>> lists(nT);
+  auto tile_of = [&](int k) { return ((k / Nx) / TY) * tx + (k % Nx) / TX; };
+  for (int k = 0; k < Nx * Nr; k++) {
+    if (mask[k] || geoM[4 * k] != 0.0f || geoM[4 * k + 1] != 0.0f) continue;   // hosts only
+    const int sm = int(std::lrint(geoM[4 * k + 2])) & 15;
+    if (!sm) continue;
+    int mem[5], nm = 0;
+    mem[nm++] = k;
+    if (sm & 1) mem[nm++] = k - 1;
+    if (sm & 2) mem[nm++] = k + 1;
+    if (sm & 4) mem[nm++] = k - Nx;
+    if (sm & 8) mem[nm++] = k + Nx;
+    for (int a = 0; a < nm; a++) {
+      const int t = tile_of(mem[a]);
+      for (int b = 0; b < nm; b++) {
+        if (tile_of(mem[b]) == t) continue;
+        std::vector<int>& L = lists[t];
+        bool have = false;
+        for (int c : L) have |= (c == mem[b]);
+        if (!have) L.push_back(mem[b]);
+      }
+    }
+  }
+  std::vector<int> off(nT + 1, 0), cells;
+  int maxX = 1;
+  for (int t = 0; t < nT; t++) {
+    off[t + 1] = off[t] + int(lists[t].size());
+    maxX = std::max(maxX, int(lists[t].size()));
+    cells.insert(cells.end(), lists[t].begin(), lists[t].end());
+  }
+  if (maxX > MAXX_CAP)
+    return fail(RN_ERR_ARG, "rn_set_geometry: a tile has " + std::to_string(maxX) + " out-of-tile group members (limit " +
+                                std::to_string(MAXX_CAP) + ")");
+  if (cells.empty()) cells.push_back(0);
+  cudaFree(h->xcell);
+  h->xcell = nullptr;
+  CK(cudaMalloc(&h->xcell, sizeof(int) * cells.size()));
+  CK(cudaMemcpyAsync(h->xoff, off.data(), sizeof(int) * (nT + 1), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->xcell, cells.data(), sizeof(int) * cells.size(), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->maxX = maxX;
+  return RN_OK;
 }
 
 bool valid(rn_solver* h) { return h != nullptr && h->SA[0] != nullptr; }
 
-void make_grid_copy(const rn_solver* h, Grid& g) { g = h->grid(); }
+cudaEvent_t prof_event(rn_solver* h) {
+  if (!h->evPool.empty()) {
+    cudaEvent_t e = h->evPool.back();
+    h->evPool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  cudaEventCreate(&e);
+  return e;
+}
+// brackets one kernel launch (or a launch group) with events when profiling
+struct ProfScope {
+  rn_solver* h;
+  int kind;
+  cudaEvent_t e0 = nullptr;
+  ProfScope(rn_solver* h_, int kind_) : h(h_), kind(kind_) {
+    if (h->prof) {
+      e0 = prof_event(h);
+      cudaEventRecord(e0, h->stream);
+    }
+  }
+  ~ProfScope() {
+    if (h->prof && e0) {
+      cudaEvent_t e1 = prof_event(h);
+      cudaEventRecord(e1, h->stream);
+      h->evPending.push_back({kind, {e0, e1}});
+    }
+  }
+};
 
 }  // namespace
 
@@ -177,6 +277,16 @@ int rn_create(int Nx, int Nr, rn_handle* out) {
   if (e != cudaSuccess) { delete h; return cuda_fail(e, "cudaStreamCreate"); }
   e = cudaEventCreateWithFlags(&h->asyncEv, cudaEventDisableTiming);
   if (e != cudaSuccess) { cudaStreamDestroy(h->stream); delete h; return cuda_fail(e, "cudaEventCreate"); }
+  static bool kernels_ready = false;
+  if (!kernels_ready) {
+    if (stage_kernels_init() != 0) {
+      cudaEventDestroy(h->asyncEv);
+      cudaStreamDestroy(h->stream);
+      delete h;
+      return fail(RN_ERR_CUDA, "rn_create: cannot size the stage kernels' shared memory");
+    }
+    kernels_ready = true;
+  }
   int rc = alloc_buffers(h, Nx, Nr);
   if (rc != RN_OK) {
     std::string msg = g_err;
@@ -195,6 +305,8 @@ int rn_destroy(rn_handle h) {
   cudaStreamSynchronize(h->stream);
   free_buffers(h);
   if (h->pinned) cudaFreeHost(h->pinned);
+  for (auto& p : h->evPending) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
+  for (auto e : h->evPool) cudaEventDestroy(e);
   cudaEventDestroy(h->asyncEv);
   cudaStreamDestroy(h->stream);
   delete h;
@@ -236,7 +348,9 @@ int rn_set_geometry(rn_handle h, const uint8_t* mask, const float* geoA, const f
     if (((sm & 1) && i == 0) || ((sm & 2) && i == Nx - 1) || ((sm & 4) && j == 0) || ((sm & 8) && j == Nr - 1))
       return fail(RN_ERR_ARG, "rn_set_geometry: slave bit of cell " + std::to_string(k) + " points outside the grid");
   }
-  int rc = rn_set_mask(h, mask);
+  int rc = build_member_lists(h, mask, geoM);
+  if (rc != RN_OK) return rc;
+  rc = rn_set_mask(h, mask);
   if (rc != RN_OK) return rc;
   const size_t N = size_t(Nx) * Nr, NF = size_t(Nx + 1) * (Nr + 1);
   CK(cudaMemcpyAsync(h->geoA, geoA, sizeof(float4) * NF, cudaMemcpyHostToDevice, h->stream));
@@ -278,6 +392,7 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
     unsigned* wOut = h->wmax + (1 - h->wslot);
     if (!h->wvalid) {
       CK(cudaMemsetAsync(wIn, 0, sizeof(unsigned), h->stream));
+      ProfScope ps(h, RN_K_REDUCE);
       launch_reduce(g, h->SA[s0], h->SB[s0], wIn, h->stream);
       h->launches++;
     }
@@ -289,7 +404,11 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
     a.oA = h->SA[s1]; a.oB = h->SB[s1];
     a.stPrev = stPrev; a.stNew = stNew; a.wIn = wIn; a.wOut = wOut;
     a.finalCfl = 0;
-    launch_stage1(a, *P, h->stream);
+    a.xoff = h->xoff; a.xcell = h->xcell; a.maxX = h->maxX;
+    {
+      ProfScope ps(h, RN_K_STAGE1);
+      launch_stage1(a, *P, h->stream);
+    }
     h->launches++;
     if (inj) {
       SprayArgs sp;
@@ -301,6 +420,7 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
       sp.key = h->key; sp.val = h->val; sp.dep = h->dep;
       sp.head = int(h->head); sp.seed = int(h->seed);
       int launched = 0;
+      ProfScope ps(h, RN_K_PARCELS);
       if (launch_spray(sp, *P, h->sortTemp, h->sortTempBytes, h->keyS, h->valS, h->src, h->stream, &launched) != 0)
         return fail(RN_ERR_CUDA, "rn_step: deposit sort failed");
       h->launches += launched;
@@ -309,7 +429,10 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
     b.A = h->SA[s1]; b.B = h->SB[s1]; b.A0 = h->SA[s0]; b.B0 = h->SB[s0];
     b.oA = h->SA[s2]; b.oB = h->SB[s2];
     b.finalCfl = (!phys && !inj) ? 1 : 0;
-    launch_stage2(b, *P, h->stream);
+    {
+      ProfScope ps(h, RN_K_STAGE2);
+      launch_stage2(b, *P, h->stream);
+    }
     h->launches++;
     h->cur = s2;
     if (phys) {
@@ -318,7 +441,11 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
       p.A1 = h->SA[s1]; p.B1 = h->SB[s1]; p.A2 = h->SA[s2]; p.B2 = h->SB[s2];
       p.oA = h->SA[s0]; p.oB = h->SB[s0];
       p.st = stNew; p.wOut = wOut; p.finalCfl = inj ? 0 : 1;
-      launch_physics(p, *P, h->stream);
+      p.xoff = h->xoff; p.xcell = h->xcell; p.maxX = h->maxX;
+      {
+        ProfScope ps(h, RN_K_PHYSICS);
+        launch_physics(p, *P, h->stream);
+      }
       h->launches++;
       h->cur = s0;
     }
@@ -329,7 +456,10 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
       ap.A = h->SA[h->cur]; ap.B = h->SB[h->cur]; ap.src = h->src;
       ap.oA = h->SA[out]; ap.oB = h->SB[out];
       ap.wOut = wOut; ap.finalCfl = 1;
-      launch_apply(ap, *P, h->stream);
+      {
+        ProfScope ps(h, RN_K_APPLY);
+        launch_apply(ap, *P, h->stream);
+      }
       h->launches++;
       h->cur = out;
       h->scur = 1 - h->scur;
@@ -349,7 +479,10 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
 int rn_rescale_ambient(rn_handle h, float fp, float fT, float du, const rn_params* P) {
   if (!valid(h) || !P) return fail(RN_ERR_ARG, "rn_rescale_ambient: bad argument");
   const int s0 = h->cur, s1 = (h->cur + 1) % 3;
-  launch_rescale(h->grid(), h->SA[s0], h->SB[s0], h->SA[s1], h->SB[s1], fp, fT, du, *P, h->stream);
+  {
+    ProfScope ps(h, RN_K_OTHER);
+    launch_rescale(h->grid(), h->SA[s0], h->SB[s0], h->SA[s1], h->SB[s1], fp, fT, du, *P, h->stream);
+  }
   h->launches++;
   h->cur = s1;
   h->wvalid = false;
@@ -516,6 +649,39 @@ int rn_wait(rn_handle h, int timeout_ms) {
     if (ms >= timeout_ms) return RN_NOT_READY;
     std::this_thread::sleep_for(std::chrono::microseconds(200));
   }
+}
+
+int rn_get_stream(rn_handle h, void** stream) {
+  if (!h || !stream) return fail(RN_ERR_ARG, "rn_get_stream: bad argument");
+  *stream = (void*)h->stream;
+  return RN_OK;
+}
+
+int rn_profile(rn_handle h, int enable) {
+  if (!h) return fail(RN_ERR_ARG, "rn_profile: NULL handle");
+  h->prof = enable != 0;
+  return RN_OK;
+}
+
+int rn_profile_read(rn_handle h, double ms[RN_NKERNELS], long long launches[RN_NKERNELS]) {
+  if (!h || !ms || !launches) return fail(RN_ERR_ARG, "rn_profile_read: bad argument");
+  CK(cudaStreamSynchronize(h->stream));
+  for (auto& p : h->evPending) {
+    float t = 0.0f;
+    CK(cudaEventElapsedTime(&t, p.second.first, p.second.second));
+    h->profMs[p.first] += t;
+    h->profN[p.first] += 1;
+    h->evPool.push_back(p.second.first);
+    h->evPool.push_back(p.second.second);
+  }
+  h->evPending.clear();
+  for (int k = 0; k < RN_NKERNELS; k++) {
+    ms[k] = h->profMs[k];
+    launches[k] = h->profN[k];
+    h->profMs[k] = 0.0;
+    h->profN[k] = 0;
+  }
+  return RN_OK;
 }
 
 int rn_kernel_launches(rn_handle h, long long* out) {

@@ -9,6 +9,8 @@ namespace rn {
 
 // Tile of one stage/physics block: TX x TY cells, one thread per cell.
 constexpr int TX = 32, TY = 8, NT = TX * TY;
+// Most out-of-tile group members one tile may list (set_geometry rejects more).
+constexpr int MAXX = 64;
 
 struct StageArgs {
   Grid g;
@@ -20,6 +22,9 @@ struct StageArgs {
   const unsigned* wIn;                  // stage 1: max wave speed of the step's input state
   unsigned* wOut;                       // cleared by stage 1, accumulated by the step's last kernel
   int finalCfl;                         // this kernel writes the step's final state
+  const int* xoff;                      // per tile: out-of-tile members of its cut-cell groups (CSR)
+  const int* xcell;
+  int maxX;                             // largest per-tile list (sizes the dynamic shared memory)
 };
 
 struct PhysArgs {
@@ -30,6 +35,9 @@ struct PhysArgs {
   const float4* st;
   unsigned* wOut;
   int finalCfl;
+  const int* xoff;
+  const int* xcell;
+  int maxX;
 };
 
 struct SprayArgs {
@@ -65,5 +73,8 @@ int launch_spray(const SprayArgs& a, const rn_params& P, void* sortTemp, size_t 
                  unsigned* valOut, float4* src, cudaStream_t s, int* launches);
 void launch_apply(const ApplyArgs& a, const rn_params& P, cudaStream_t s);
 size_t spray_sort_temp_bytes(int Ncells);
+int stage_kernels_init();           // opts the kernels into the dynamic shared memory they need
+size_t stage_smem(int maxX);        // dynamic shared memory of a stage launch
+size_t physics_smem(int maxX);      // dynamic shared memory of a physics launch
 
 }  // namespace rn

@@ -140,16 +140,20 @@ RN_DEV void interior_prim(const Grid& g, const float4* __restrict__ A, const flo
 // solver.js:133-259). Inputs are the 4 cells along the face normal (padded
 // W/Wb values) and the raw W of the 4 transverse sensor cells
 // (k1+t, k1-t, ij+t, ij-t).
+// 2 max(ab, 0) / den with den = a + b, or 1 where |den| <= 1e-30. For ab <= 0
+// the quotient is a zero carrying den's sign, so the division is skipped; the
+// result is the same float for every input that is not NaN.
 RN_DEV float van_leer(float a, float b) {
   float ab = a * b, den = a + b;
   den = mixf(den, 1.0f, (1e-30f < fabsf(den)) ? 0.0f : 1.0f);   // step(abs(den), 1e-30)
-  return 2.0f * fmaxf(ab, 0.0f) / den;
+  return ab > 0.0f ? 2.0f * ab / den : copysignf(0.0f, den);
 }
 RN_DEV float jump_ratio(float a, float b) { return fabsf(a - b) / fminf(a, b); }
 
-template <bool DIR_R>
-RN_DEV Flux face_flux(float area, float4 w0, float4 b0, float4 w1, float4 b1, float4 w2, float4 b2, float4 w3,
-                      float4 b3, float4 sa1, float4 sb1, float4 sa2, float4 sb2, const rn_params& P) {
+// DIR_R selects the r-direction (normal velocity in .z); one instance of the
+// code serves both directions.
+RN_DEV Flux face_flux(bool DIR_R, float area, float4 w0, float4 b0, float4 w1, float4 b1, float4 w2, float4 b2,
+                      float4 w3, float4 b3, float4 sa1, float4 sb1, float4 sa2, float4 sb2, const rn_params& P) {
   Flux out;
   out.F = make_float4(0.f, 0.f, 0.f, 0.f);
   out.Y = out.F;
@@ -168,8 +172,16 @@ RN_DEV Flux face_flux(float area, float4 w0, float4 b0, float4 w1, float4 b1, fl
     float p1 = w1.w, p2 = w2.w;
     float pa1 = sa1.x < 0.0f ? p1 : sa1.w, pb1 = sb1.x < 0.0f ? p1 : sb1.w;
     float pa2 = sa2.x < 0.0f ? p2 : sa2.w, pb2 = sb2.x < 0.0f ? p2 : sb2.w;
-    float jm = fmaxf(fmaxf(jump_ratio(pa1, p1), jump_ratio(pb1, p1)), fmaxf(jump_ratio(pa2, p2), jump_ratio(pb2, p2)));
-    hllw = smoothstepf(0.15f, 0.6f, jm * P.hllBlend);
+    // Smooth pressure (every jump ratio times hllBlend clearly below the 0.15
+    // start of the smoothstep) gives hllw = 0 exactly; only test the ratios
+    // where a jump is near. The margin (0.1 against 0.15) dwarfs rounding.
+    const float hb = P.hllBlend;
+    bool smooth = fabsf(pa1 - p1) * hb < 0.1f * fminf(pa1, p1) && fabsf(pb1 - p1) * hb < 0.1f * fminf(pb1, p1) &&
+                  fabsf(pa2 - p2) * hb < 0.1f * fminf(pa2, p2) && fabsf(pb2 - p2) * hb < 0.1f * fminf(pb2, p2);
+    if (!smooth) {
+      float jm = fmaxf(fmaxf(jump_ratio(pa1, p1), jump_ratio(pb1, p1)), fmaxf(jump_ratio(pa2, p2), jump_ratio(pb2, p2)));
+      hllw = smoothstepf(0.15f, 0.6f, jm * hb);
+    }
   }
   float4 WLw, WLs, WRw, WRs;
   if (s1) { WRw = w2; WRs = b2; WLw = w2; WLw.y = -WLw.y; WLs = b2; }
@@ -313,9 +325,8 @@ RN_DEV void vcell(float4 w0, float4 sc, float4 wE, float4 wW, float4 wN, float4 
 // makeViscFluxShader (solver.js:499-536) for one face; returns false for a
 // zero flux. (w1, s1, t1, m1) is the cell behind the face, (w2, s2, t2, m2) the
 // cell the face belongs to; j is the face's row.
-template <bool DIR_R>
-RN_DEV void visc_flux(float4 w1, float4 s1, float4 t1, float4 m1, float4 w2, float4 s2, float4 t2, float4 m2, int j,
-                      float4& F, float4& FY) {
+RN_DEV void visc_flux(bool DIR_R, float4 w1, float4 s1, float4 t1, float4 m1, float4 w2, float4 s2, float4 t2,
+                      float4 m2, int j, float4& F, float4& FY) {
   float mu = 0.5f * (m1.x + m2.x);
   float uf = 0.5f * (w1.y + w2.y), vf = 0.5f * (w1.z + w2.z);
   float ttx = 0.5f * (t1.x + t2.x), tty = 0.5f * (t1.y + t2.y), ttz = 0.5f * (t1.z + t2.z), ttw = 0.5f * (t1.w + t2.w);

@@ -6,9 +6,14 @@
 // once (makeFluxShader, solver.js:133-259) into shared memory, then updates
 // each cell over its merged cut-cell group (FS_UPDATE, solver.js:264-363).
 // The reference's 7 full-grid passes per stage (prim, 2 flux, update, CFL
-// chain) and its 6 face textures never touch HBM here. Group members that lie
-// outside the tile (slivers merged across a tile edge) get their faces from a
-// slow path that recomputes them from global memory.
+// chain) and its 6 face textures never touch HBM here.
+//
+// Group members outside the tile (slivers merged across a tile edge) are
+// listed per tile at set_geometry (xoff/xcell). For each listed member the
+// block adds a 5x5 block of primitives around it to the primitive phase and its
+// 4 faces to the face phase: the same loops and the same single instance of
+// the face code run them, so blocks along the walls do no serial or cold-code
+// work.
 //
 // The step's last kernel folds the CFL wave speed of the cells it writes into
 // one atomicMax per block (FS_REDUCE1/2, solver.js:368-397); the next step's
@@ -23,7 +28,12 @@
 
 namespace rn {
 
-constexpr int PX = TX + 4, PY = TY + 4;   // primitive tile with a 2-cell halo
+constexpr int PX = TX + 4, PY = TY + 4;      // primitive tile with a 2-cell halo
+constexpr int NPT = PX * PY;                  // tile primitives
+constexpr int NXF = TY * (TX + 1);            // x-faces of a tile
+constexpr int NRF = (TY + 1) * TX;            // r-faces of a tile
+constexpr int TW = TX + 2;                    // vcell ring width (tile + 1)
+constexpr int NTT = (TX + 2) * (TY + 2);      // vcell ring cells
 
 // --------------------------------------------------------------------------
 // block-wide max of non-negative floats -> one atomicMax on the bit pattern
@@ -39,44 +49,109 @@ __device__ __forceinline__ void block_max_to(float w, unsigned* out, float* red)
   }
 }
 
-// --------------------------------------------------------------------------
-// Slow path: one inviscid face recomputed from global memory.
-template <bool DIR_R>
-__device__ __noinline__ Flux face_flux_global(const Grid g, const float4* __restrict__ A, const float4* __restrict__ B,
-                                               int i, int j, float t, const rn_params& P) {
-  Flux f;
-  f.F = make_float4(0.f, 0.f, 0.f, 0.f);
-  f.Y = f.F;
-  f.O = 0.0f;
-  float4 geo = g.geoA[j * (g.Nx + 1) + i];
-  float area = DIR_R ? geo.w : geo.z;
-  if (area == 0.0f || (DIR_R && j == 0)) return f;
-  const int dx = DIR_R ? 0 : 1, dy = DIR_R ? 1 : 0, tx = DIR_R ? 1 : 0, ty = DIR_R ? 0 : 1;
-  float4 w0, b0, w1, b1, w2, b2, w3, b3, sa1, sb1, sa2, sb2, dum;
-  ghost_prim(g, A, B, i - 2 * dx, j - 2 * dy, t, P, w0, b0);
-  ghost_prim(g, A, B, i - dx, j - dy, t, P, w1, b1);
-  ghost_prim(g, A, B, i, j, t, P, w2, b2);
-  ghost_prim(g, A, B, i + dx, j + dy, t, P, w3, b3);
-  ghost_prim(g, A, B, i - dx + tx, j - dy + ty, t, P, sa1, dum);
-  ghost_prim(g, A, B, i - dx - tx, j - dy - ty, t, P, sb1, dum);
-  ghost_prim(g, A, B, i + tx, j + ty, t, P, sa2, dum);
-  ghost_prim(g, A, B, i - tx, j - ty, t, P, sb2, dum);
-  return face_flux<DIR_R>(area, w0, b0, w1, b1, w2, b2, w3, b3, sa1, sb1, sa2, sb2, P);
+// Shared-memory index of the primitive of cell (i, j): tile cells live in the
+// PX x PY tile array, listed members' neighbourhoods in 5x5 blocks after it.
+__device__ __forceinline__ int ext_prim(int e, int dx, int dy) { return NPT + e * 25 + (dy + 2) * 5 + (dx + 2); }
+
+// Coordinates of primitive slot k (tile first, then one 5x5 block per member).
+__device__ __forceinline__ void prim_slot(int k, int x0, int y0, const int* xc, int Nx, int& i, int& j) {
+  if (k < NPT) {
+    const int ly = k / PX;
+    i = x0 - 2 + (k - ly * PX);
+    j = y0 - 2 + ly;
+  } else {
+    const int q = k - NPT, e = q / 25, r = q - e * 25, m = xc[e];
+    const int dy = r / 5;
+    i = m % Nx + (r - dy * 5) - 2;
+    j = m / Nx + dy - 2;
+  }
+}
+
+// Stencil of face slot k: the 4 cells along the normal (c0..c3), the 4
+// transverse sensor cells (k1+t, k1-t, ij+t, ij-t) as primitive slots, the
+// face position (i, j), its direction, and whether the reference draws it.
+struct FaceSlot {
+  int c[4], s[4];
+  int i, j;
+  bool dirR, valid;
+};
+__device__ __forceinline__ FaceSlot face_slot(int k, int x0, int y0, const int* xc, int Nx, int Nr) {
+  FaceSlot f;
+  if (k < NXF) {                                   // x-face (i, j): west face of cell (i, j)
+    const int ly = k / (TX + 1), lx = k - ly * (TX + 1), py = ly + 2;
+    f.i = x0 + lx; f.j = y0 + ly; f.dirR = false;
+    f.valid = f.i <= Nx && f.j < Nr;
+    const int b = py * PX + lx;
+    f.c[0] = b; f.c[1] = b + 1; f.c[2] = b + 2; f.c[3] = b + 3;
+    f.s[0] = b + PX + 1; f.s[1] = b - PX + 1; f.s[2] = b + PX + 2; f.s[3] = b - PX + 2;
+  } else if (k < NXF + NRF) {                      // r-face (i, j): south face of cell (i, j)
+    const int kk = k - NXF, ly = kk / TX, lx = kk - ly * TX, px = lx + 2;
+    f.i = x0 + lx; f.j = y0 + ly; f.dirR = true;
+    f.valid = f.i < Nx && f.j <= Nr && f.j != 0;
+    const int b = ly * PX + px;
+    f.c[0] = b; f.c[1] = b + PX; f.c[2] = b + 2 * PX; f.c[3] = b + 3 * PX;
+    f.s[0] = b + PX + 1; f.s[1] = b + PX - 1; f.s[2] = b + 2 * PX + 1; f.s[3] = b + 2 * PX - 1;
+  } else {                                         // faces of listed member e: W, E, S, N
+    const int q = k - NXF - NRF, e = q >> 2, w = q & 3, m = xc[e];
+    const int mx = m % Nx, my = m / Nx;
+    if (w < 2) {
+      const int o = w;                             // face at mx + o
+      f.i = mx + o; f.j = my; f.dirR = false; f.valid = true;
+      f.c[0] = ext_prim(e, o - 2, 0); f.c[1] = ext_prim(e, o - 1, 0);
+      f.c[2] = ext_prim(e, o, 0); f.c[3] = ext_prim(e, o + 1, 0);
+      f.s[0] = ext_prim(e, o - 1, 1); f.s[1] = ext_prim(e, o - 1, -1);
+      f.s[2] = ext_prim(e, o, 1); f.s[3] = ext_prim(e, o, -1);
+    } else {
+      const int o = w - 2;                         // face at my + o
+      f.i = mx; f.j = my + o; f.dirR = true; f.valid = f.j != 0;
+      f.c[0] = ext_prim(e, 0, o - 2); f.c[1] = ext_prim(e, 0, o - 1);
+      f.c[2] = ext_prim(e, 0, o); f.c[3] = ext_prim(e, 0, o + 1);
+      f.s[0] = ext_prim(e, 1, o - 1); f.s[1] = ext_prim(e, -1, o - 1);
+      f.s[2] = ext_prim(e, 1, o); f.s[3] = ext_prim(e, -1, o);
+    }
+  }
+  return f;
+}
+
+// The four face slots (W, E, S, N) of group member (cx, cy).
+__device__ __forceinline__ void member_faces(int cx, int cy, int x0, int y0, const int* xc, int xn, int Nx,
+                                             int& fw, int& fe, int& fs, int& fn) {
+  const int mx = cx - x0, my = cy - y0;
+  if (mx >= 0 && mx < TX && my >= 0 && my < TY) {
+    fw = my * (TX + 1) + mx;
+    fe = fw + 1;
+    fs = NXF + my * TX + mx;
+    fn = fs + TX;
+  } else {
+    const int mc = cy * Nx + cx;
+    int e = 0;
+    while (e < xn - 1 && xc[e] != mc) e++;
+    fw = NXF + NRF + 4 * e;
+    fe = fw + 1;
+    fs = fw + 2;
+    fn = fw + 3;
+  }
 }
 
 // --------------------------------------------------------------------------
 template <int STAGE>
 __global__ void __launch_bounds__(NT) k_stage(StageArgs a, rn_params P) {
-  __shared__ float4 sW[PY][PX], sWb[PY][PX];
-  __shared__ float4 sXF[TY][TX + 1], sXY[TY][TX + 1];
-  __shared__ float sXO[TY][TX + 1];
-  __shared__ float4 sRF[TY + 1][TX], sRY[TY + 1][TX];
-  __shared__ float sRO[TY + 1][TX];
+  extern __shared__ float4 sm[];
   __shared__ float red[NT / 32];
+  __shared__ int xc[MAXX];
   const Grid g = a.g;
   const int Nx = g.Nx, Nr = g.Nr, W1 = Nx + 1;
   const int tid = threadIdx.x;
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const int tileId = blockIdx.y * gridDim.x + blockIdx.x;
+  const int xb = a.xoff[tileId], xn = a.xoff[tileId + 1] - xb;
+  const int NP = NPT + 25 * xn, NF = NXF + NRF + 4 * xn;
+  float4* sW = sm;
+  float4* sWb = sW + NP;
+  float4* sF = sWb + NP;
+  float4* sY = sF + NF;
+  float* sO = reinterpret_cast<float*>(sY + NF);
+  for (int q = tid; q < xn; q += NT) xc[q] = a.xcell[xb + q];
 
   float dt, t;
   if (STAGE == 1) {
@@ -94,51 +169,33 @@ __global__ void __launch_bounds__(NT) k_stage(StageArgs a, rn_params P) {
     dt = st.x;
     t = st.z;                                     // inlet ramp at t_new
   }
+  __syncthreads();
 
-  // ---- ghost-cell primitives of the tile + 2-cell halo
-  for (int k = tid; k < PX * PY; k += NT) {
-    int ly = k / PX, lx = k - ly * PX;
-    int i = x0 - 2 + lx, j = y0 - 2 + ly;
+  // ---- ghost-cell primitives: tile + 2-cell halo, then the members' blocks
+  for (int k = tid; k < NP; k += NT) {
+    int i, j;
+    prim_slot(k, x0, y0, xc, Nx, i, j);
     float4 W, Wb;
     if (i <= Nx + 1 && j <= Nr + 1) ghost_prim(g, a.A, a.B, i, j, t, P, W, Wb);
     else { W = make_float4(-1.f, 0.f, 0.f, 1.f); Wb = make_float4(0.f, 0.f, 0.f, 0.f); }
-    sW[ly][lx] = W;
-    sWb[ly][lx] = Wb;
+    sW[k] = W;
+    sWb[k] = Wb;
   }
   __syncthreads();
 
-  // ---- face fluxes: x-faces (TX+1) x TY, r-faces TX x (TY+1)
-  for (int k = tid; k < TY * (TX + 1); k += NT) {
-    int ly = k / (TX + 1), lx = k - ly * (TX + 1);
-    int i = x0 + lx, j = y0 + ly;
+  // ---- face fluxes: tile x-faces, tile r-faces, members' faces
+  for (int k = tid; k < NF; k += NT) {
+    const FaceSlot s = face_slot(k, x0, y0, xc, Nx, Nr);
     Flux f;
     f.F = make_float4(0.f, 0.f, 0.f, 0.f); f.Y = f.F; f.O = 0.f;
-    if (i <= Nx && j < Nr) {
-      float area = g.geoA[j * W1 + i].z;
-      if (area != 0.0f) {
-        const int py = ly + 2;
-        f = face_flux<false>(area, sW[py][lx], sWb[py][lx], sW[py][lx + 1], sWb[py][lx + 1], sW[py][lx + 2],
-                             sWb[py][lx + 2], sW[py][lx + 3], sWb[py][lx + 3], sW[py + 1][lx + 1], sW[py - 1][lx + 1],
-                             sW[py + 1][lx + 2], sW[py - 1][lx + 2], P);
-      }
+    if (s.valid) {
+      float4 geo = g.geoA[s.j * W1 + s.i];
+      float area = s.dirR ? geo.w : geo.z;
+      if (area != 0.0f)
+        f = face_flux(s.dirR, area, sW[s.c[0]], sWb[s.c[0]], sW[s.c[1]], sWb[s.c[1]], sW[s.c[2]], sWb[s.c[2]],
+                      sW[s.c[3]], sWb[s.c[3]], sW[s.s[0]], sW[s.s[1]], sW[s.s[2]], sW[s.s[3]], P);
     }
-    sXF[ly][lx] = f.F; sXY[ly][lx] = f.Y; sXO[ly][lx] = f.O;
-  }
-  for (int k = tid; k < (TY + 1) * TX; k += NT) {
-    int ly = k / TX, lx = k - ly * TX;
-    int i = x0 + lx, j = y0 + ly;
-    Flux f;
-    f.F = make_float4(0.f, 0.f, 0.f, 0.f); f.Y = f.F; f.O = 0.f;
-    if (i < Nx && j <= Nr && j != 0) {
-      float area = g.geoA[j * W1 + i].w;
-      if (area != 0.0f) {
-        const int px = lx + 2;
-        f = face_flux<true>(area, sW[ly][px], sWb[ly][px], sW[ly + 1][px], sWb[ly + 1][px], sW[ly + 2][px],
-                            sWb[ly + 2][px], sW[ly + 3][px], sWb[ly + 3][px], sW[ly + 1][px + 1], sW[ly + 1][px - 1],
-                            sW[ly + 2][px + 1], sW[ly + 2][px - 1], P);
-      }
-    }
-    sRF[ly][lx] = f.F; sRY[ly][lx] = f.Y; sRO[ly][lx] = f.O;
+    sF[k] = f.F; sY[k] = f.Y; sO[k] = f.O;
   }
   __syncthreads();
 
@@ -161,36 +218,25 @@ __global__ void __launch_bounds__(NT) k_stage(StageArgs a, rn_params P) {
       Prim q = to_prim(A, B);
       float4 L = make_float4(0.f, 0.f, 0.f, 0.f), LY = L;
       float LO = 0.0f;
-      const int sm = iround(g.geoM[kh].z);
+      const int sm_ = iround(g.geoM[kh].z);
       for (int m = 0; m < 5; m++) {
         int cx = Hx, cy = Hy;
-        if (m == 1) { if (!(sm & 1)) continue; cx -= 1; }
-        else if (m == 2) { if (!(sm & 2)) continue; cx += 1; }
-        else if (m == 3) { if (!(sm & 4)) continue; cy -= 1; }
-        else if (m == 4) { if (!(sm & 8)) continue; cy += 1; }
+        if (m == 1) { if (!(sm_ & 1)) continue; cx -= 1; }
+        else if (m == 2) { if (!(sm_ & 2)) continue; cx += 1; }
+        else if (m == 3) { if (!(sm_ & 4)) continue; cy -= 1; }
+        else if (m == 4) { if (!(sm_ & 8)) continue; cy += 1; }
         float4 gc = g.geoA[cy * W1 + cx];
         float aw = fabsf(gc.z), ae = fabsf(g.geoA[cy * W1 + cx + 1].z);
         float as_ = fabsf(gc.w), an = fabsf(g.geoA[(cy + 1) * W1 + cx].w);
-        const int mx = cx - x0, my = cy - y0;
-        Flux fw, fe, fs, fn;
-        if (mx >= 0 && mx < TX && my >= 0 && my < TY) {
-          fw.F = sXF[my][mx]; fw.Y = sXY[my][mx]; fw.O = sXO[my][mx];
-          fe.F = sXF[my][mx + 1]; fe.Y = sXY[my][mx + 1]; fe.O = sXO[my][mx + 1];
-          fs.F = sRF[my][mx]; fs.Y = sRY[my][mx]; fs.O = sRO[my][mx];
-          fn.F = sRF[my + 1][mx]; fn.Y = sRY[my + 1][mx]; fn.O = sRO[my + 1][mx];
-        } else {
-          fw = face_flux_global<false>(g, a.A, a.B, cx, cy, t, P);
-          fe = face_flux_global<false>(g, a.A, a.B, cx + 1, cy, t, P);
-          fs = face_flux_global<true>(g, a.A, a.B, cx, cy, t, P);
-          fn = face_flux_global<true>(g, a.A, a.B, cx, cy + 1, t, P);
-        }
-        sub4(L, ae, fe.F, aw, fw.F);
-        sub4(L, an, fn.F, as_, fs.F);
-        sub4(LY, ae, fe.Y, aw, fw.Y);
-        sub4(LY, an, fn.Y, as_, fs.Y);
+        int fw, fe, fs, fn;
+        member_faces(cx, cy, x0, y0, xc, xn, Nx, fw, fe, fs, fn);
+        sub4(L, ae, sF[fe], aw, sF[fw]);
+        sub4(L, an, sF[fn], as_, sF[fs]);
+        sub4(LY, ae, sY[fe], aw, sY[fw]);
+        sub4(LY, an, sY[fn], as_, sY[fs]);
         if (P.inj) {
-          LO -= ae * fe.O - aw * fw.O;
-          LO -= an * fn.O - as_ * fs.O;
+          LO -= ae * sO[fe] - aw * sO[fw];
+          LO -= an * sO[fn] - as_ * sO[fs];
         }
       }
       // embedded wall: pressure force along the r-weighted wall vector
@@ -248,104 +294,107 @@ __global__ void __launch_bounds__(NT) k_stage(StageArgs a, rn_params P) {
 }
 
 // --------------------------------------------------------------------------
-// Slow path for the physics kernel: one viscous face from global memory.
-__device__ __noinline__ void vcell_global(const Grid g, const float4* __restrict__ A, const float4* __restrict__ B,
-                                          int i, int j, float t, float dt, const rn_params& P, float4& T1, float4& T2) {
-  float4 w0, s0, wE, wW, wN, wS, d;
-  ghost_prim(g, A, B, i, j, t, P, w0, s0);
-  ghost_prim(g, A, B, i + 1, j, t, P, wE, d);
-  ghost_prim(g, A, B, i - 1, j, t, P, wW, d);
-  ghost_prim(g, A, B, i, j + 1, t, P, wN, d);
-  ghost_prim(g, A, B, i, j - 1, t, P, wS, d);
-  vcell(w0, s0, wE, wW, wN, wS, i, j, g.geoM[j * g.Nx + i].w, dt, P, T1, T2);
+// vcell slot k: the tile + 1 ring first, then 5 cells per listed member
+// (itself, W, E, S, N). Returns the cell and the primitive slots of the cell
+// and its E, W, N, S neighbours.
+__device__ __forceinline__ void vcell_slot(int k, int x0, int y0, const int* xc, int Nx, int& i, int& j, int& c,
+                                           int& e_, int& w_, int& n_, int& s_) {
+  if (k < NTT) {
+    const int ly = k / TW, lx = k - ly * TW;
+    i = x0 - 1 + lx; j = y0 - 1 + ly;
+    c = (ly + 1) * PX + lx + 1;
+    e_ = c + 1; w_ = c - 1; n_ = c + PX; s_ = c - PX;
+  } else {
+    const int q = k - NTT, e = q / 5, r = q - e * 5, m = xc[e];
+    const int dx = r == 1 ? -1 : r == 2 ? 1 : 0, dy = r == 3 ? -1 : r == 4 ? 1 : 0;
+    i = m % Nx + dx; j = m / Nx + dy;
+    c = ext_prim(e, dx, dy);
+    e_ = c + 1; w_ = c - 1; n_ = c + 5; s_ = c - 5;
+  }
 }
 
-template <bool DIR_R>
-__device__ __noinline__ void vflux_global(const Grid g, const float4* __restrict__ A, const float4* __restrict__ B,
-                                          int i, int j, float t, float dt, const rn_params& P, float4& F, float4& FY) {
-  F = make_float4(0.f, 0.f, 0.f, 0.f);
-  FY = F;
-  float4 geo = g.geoA[j * (g.Nx + 1) + i];
-  int k1x, k1y;
-  if (DIR_R) {
-    if (geo.w == 0.0f || j == 0 || j >= g.Nr) return;
-    k1x = i; k1y = j - 1;
-  } else {
-    if (geo.z == 0.0f || i == 0 || i >= g.Nx) return;
-    k1x = i - 1; k1y = j;
-  }
-  float4 w1, s1, w2, s2;
-  ghost_prim(g, A, B, k1x, k1y, t, P, w1, s1);
-  ghost_prim(g, A, B, i, j, t, P, w2, s2);
-  if (w1.x < 0.0f || w2.x < 0.0f) return;
-  float4 t1, m1, t2, m2;
-  vcell_global(g, A, B, k1x, k1y, t, dt, P, t1, m1);
-  vcell_global(g, A, B, i, j, t, dt, P, t2, m2);
-  visc_flux<DIR_R>(w1, s1, t1, m1, w2, s2, t2, m2, j, F, FY);
-}
+// vcell slot of cell (i, j) for the viscous faces: tile ring, or member e's 5 cells
+__device__ __forceinline__ int tile_vslot(int i, int j, int x0, int y0) { return (j - y0 + 1) * TW + (i - x0 + 1); }
 
 // --------------------------------------------------------------------------
 __global__ void __launch_bounds__(NT) k_physics(PhysArgs a, rn_params P) {
-  __shared__ float4 sW[PY][PX], sWb[PY][PX];
-  __shared__ float4 sT1[TY + 2][TX + 2], sT2[TY + 2][TX + 2];
-  __shared__ float4 sXF[TY][TX + 1], sXY[TY][TX + 1];
-  __shared__ float4 sRF[TY + 1][TX], sRY[TY + 1][TX];
+  extern __shared__ float4 sm[];
   __shared__ float red[NT / 32];
+  __shared__ int xc[MAXX];
   const Grid g = a.g;
   const int Nx = g.Nx, Nr = g.Nr, W1 = Nx + 1;
   const int tid = threadIdx.x;
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
   const float4 st = *a.st;
   const float dt = st.x, t = st.z;
+  const int tileId = blockIdx.y * gridDim.x + blockIdx.x;
+  const int xb = a.xoff[tileId], xn = P.visc ? a.xoff[tileId + 1] - xb : 0;
+  const int NP = NPT + 25 * xn, NV = NTT + 5 * xn, NF = NXF + NRF + 4 * xn;
+  float4* sW = sm;
+  float4* sWb = sW + NP;
+  float4* sT1 = sWb + NP;
+  float4* sT2 = sT1 + NV;
+  float4* sF = sT2 + NV;
+  float4* sY = sF + NF;
+  for (int q = tid; q < xn; q += NT) xc[q] = a.xcell[xb + q];
+  __syncthreads();
 
-  for (int k = tid; k < PX * PY; k += NT) {
-    int ly = k / PX, lx = k - ly * PX;
-    int i = x0 - 2 + lx, j = y0 - 2 + ly;
+  for (int k = tid; k < NP; k += NT) {
+    int i, j;
+    prim_slot(k, x0, y0, xc, Nx, i, j);
     float4 W, Wb;
     if (i <= Nx + 1 && j <= Nr + 1) ghost_prim(g, a.A1, a.B1, i, j, t, P, W, Wb);
     else { W = make_float4(-1.f, 0.f, 0.f, 1.f); Wb = make_float4(0.f, 0.f, 0.f, 0.f); }
-    sW[ly][lx] = W;
-    sWb[ly][lx] = Wb;
+    sW[k] = W;
+    sWb[k] = Wb;
   }
   __syncthreads();
-  // vcell over the tile + 1 ring
-  for (int k = tid; k < (TX + 2) * (TY + 2); k += NT) {
-    int ly = k / (TX + 2), lx = k - ly * (TX + 2);
-    int i = x0 - 1 + lx, j = y0 - 1 + ly;
+  // vcell over the tile + 1 ring and the members' cells
+  for (int k = tid; k < NV; k += NT) {
+    int i, j, c, e_, w_, n_, s_;
+    vcell_slot(k, x0, y0, xc, Nx, i, j, c, e_, w_, n_, s_);
     float4 T1 = make_float4(0.f, 0.f, 0.f, 0.f), T2 = T1;
-    if (i >= 0 && i < Nx && j >= 0 && j < Nr) {
-      const int px = lx + 1, py = ly + 1;
-      vcell(sW[py][px], sWb[py][px], sW[py][px + 1], sW[py][px - 1], sW[py + 1][px], sW[py - 1][px], i, j,
-            g.geoM[j * Nx + i].w, dt, P, T1, T2);
-    }
-    sT1[ly][lx] = T1;
-    sT2[ly][lx] = T2;
+    if (i >= 0 && i < Nx && j >= 0 && j < Nr)
+      vcell(sW[c], sWb[c], sW[e_], sW[w_], sW[n_], sW[s_], i, j, g.geoM[j * Nx + i].w, dt, P, T1, T2);
+    sT1[k] = T1;
+    sT2[k] = T2;
   }
   __syncthreads();
   if (P.visc) {
-    for (int k = tid; k < TY * (TX + 1); k += NT) {
-      int ly = k / (TX + 1), lx = k - ly * (TX + 1);
-      int i = x0 + lx, j = y0 + ly;
+    for (int k = tid; k < NF; k += NT) {
       float4 F = make_float4(0.f, 0.f, 0.f, 0.f), FY = F;
-      if (i > 0 && i < Nx && j < Nr && g.geoA[j * W1 + i].z != 0.0f) {
-        float4 w1 = sW[ly + 2][lx + 1], w2 = sW[ly + 2][lx + 2];
-        if (!(w1.x < 0.0f || w2.x < 0.0f))
-          visc_flux<false>(w1, sWb[ly + 2][lx + 1], sT1[ly + 1][lx], sT2[ly + 1][lx], w2, sWb[ly + 2][lx + 2],
-                           sT1[ly + 1][lx + 1], sT2[ly + 1][lx + 1], j, F, FY);
+      bool dirR, ok;
+      int i, j, p1, p2, v1, v2;          // primitive and vcell slots of the cells behind (1) and at (2) the face
+      if (k < NXF) {
+        const int ly = k / (TX + 1), lx = k - ly * (TX + 1);
+        i = x0 + lx; j = y0 + ly; dirR = false;
+        ok = i > 0 && i < Nx && j < Nr;
+        p2 = (ly + 2) * PX + lx + 2; p1 = p2 - 1;
+        v2 = (ly + 1) * TW + lx + 1; v1 = v2 - 1;
+      } else if (k < NXF + NRF) {
+        const int kk = k - NXF, ly = kk / TX, lx = kk - ly * TX;
+        i = x0 + lx; j = y0 + ly; dirR = true;
+        ok = i < Nx && j > 0 && j < Nr;
+        p2 = (ly + 2) * PX + lx + 2; p1 = p2 - PX;
+        v2 = (ly + 1) * TW + lx + 1; v1 = v2 - TW;
+      } else {
+        const int q = k - NXF - NRF, e = q >> 2, w = q & 3, m = xc[e];
+        const int mx = m % Nx, my = m / Nx, vb = NTT + 5 * e;
+        if (w == 0) { i = mx; j = my; dirR = false; p1 = ext_prim(e, -1, 0); p2 = ext_prim(e, 0, 0); v1 = vb + 1; v2 = vb; }
+        else if (w == 1) { i = mx + 1; j = my; dirR = false; p1 = ext_prim(e, 0, 0); p2 = ext_prim(e, 1, 0); v1 = vb; v2 = vb + 2; }
+        else if (w == 2) { i = mx; j = my; dirR = true; p1 = ext_prim(e, 0, -1); p2 = ext_prim(e, 0, 0); v1 = vb + 3; v2 = vb; }
+        else { i = mx; j = my + 1; dirR = true; p1 = ext_prim(e, 0, 0); p2 = ext_prim(e, 0, 1); v1 = vb; v2 = vb + 4; }
+        ok = dirR ? (i < Nx && j > 0 && j < Nr) : (i > 0 && i < Nx && j < Nr);
       }
-      sXF[ly][lx] = F; sXY[ly][lx] = FY;
-    }
-    for (int k = tid; k < (TY + 1) * TX; k += NT) {
-      int ly = k / TX, lx = k - ly * TX;
-      int i = x0 + lx, j = y0 + ly;
-      float4 F = make_float4(0.f, 0.f, 0.f, 0.f), FY = F;
-      if (i < Nx && j > 0 && j < Nr && g.geoA[j * W1 + i].w != 0.0f) {
-        float4 w1 = sW[ly + 1][lx + 2], w2 = sW[ly + 2][lx + 2];
-        if (!(w1.x < 0.0f || w2.x < 0.0f))
-          visc_flux<true>(w1, sWb[ly + 1][lx + 2], sT1[ly][lx + 1], sT2[ly][lx + 1], w2, sWb[ly + 2][lx + 2],
-                          sT1[ly + 1][lx + 1], sT2[ly + 1][lx + 1], j, F, FY);
+      if (ok) {
+        float4 geo = g.geoA[j * W1 + i];
+        float area = dirR ? geo.w : geo.z;
+        float4 w1 = sW[p1], w2 = sW[p2];
+        if (area != 0.0f && !(w1.x < 0.0f || w2.x < 0.0f))
+          visc_flux(dirR, w1, sWb[p1], sT1[v1], sT2[v1], w2, sWb[p2], sT1[v2], sT2[v2], j, F, FY);
       }
-      sRF[ly][lx] = F; sRY[ly][lx] = FY;
+      sF[k] = F;
+      sY[k] = FY;
     }
   }
   __syncthreads();
@@ -372,33 +421,25 @@ __global__ void __launch_bounds__(NT) k_physics(PhysArgs a, rn_params P) {
       float V = fmaxf(gg.x, 1e-6f);
       float Rm = rmix(q.s, P), Tg = p / (rho * Rm);
       float4 L = make_float4(0.f, 0.f, 0.f, 0.f), LY = L;
-      float4 T1h = sT1[Hy - y0 + 1][Hx - x0 + 1], T2h = sT2[Hy - y0 + 1][Hx - x0 + 1];
+      const int vh = tile_vslot(Hx, Hy, x0, y0);
+      float4 T1h = sT1[vh], T2h = sT2[vh];
       if (P.visc) {
-        const int sm = iround(g.geoM[kh].z);
+        const int sm_ = iround(g.geoM[kh].z);
         for (int m = 0; m < 5; m++) {
           int cx = Hx, cy = Hy;
-          if (m == 1) { if (!(sm & 1)) continue; cx -= 1; }
-          else if (m == 2) { if (!(sm & 2)) continue; cx += 1; }
-          else if (m == 3) { if (!(sm & 4)) continue; cy -= 1; }
-          else if (m == 4) { if (!(sm & 8)) continue; cy += 1; }
+          if (m == 1) { if (!(sm_ & 1)) continue; cx -= 1; }
+          else if (m == 2) { if (!(sm_ & 2)) continue; cx += 1; }
+          else if (m == 3) { if (!(sm_ & 4)) continue; cy -= 1; }
+          else if (m == 4) { if (!(sm_ & 8)) continue; cy += 1; }
           float4 gc = g.geoA[cy * W1 + cx];
           float aw = fabsf(gc.z), ae = fabsf(g.geoA[cy * W1 + cx + 1].z);
           float as_ = fabsf(gc.w), an = fabsf(g.geoA[(cy + 1) * W1 + cx].w);
-          const int mx = cx - x0, my = cy - y0;
-          float4 fwF, fwY, feF, feY, fsF, fsY, fnF, fnY;
-          if (mx >= 0 && mx < TX && my >= 0 && my < TY) {
-            fwF = sXF[my][mx]; fwY = sXY[my][mx]; feF = sXF[my][mx + 1]; feY = sXY[my][mx + 1];
-            fsF = sRF[my][mx]; fsY = sRY[my][mx]; fnF = sRF[my + 1][mx]; fnY = sRY[my + 1][mx];
-          } else {
-            vflux_global<false>(g, a.A1, a.B1, cx, cy, t, dt, P, fwF, fwY);
-            vflux_global<false>(g, a.A1, a.B1, cx + 1, cy, t, dt, P, feF, feY);
-            vflux_global<true>(g, a.A1, a.B1, cx, cy, t, dt, P, fsF, fsY);
-            vflux_global<true>(g, a.A1, a.B1, cx, cy + 1, t, dt, P, fnF, fnY);
-          }
-          sub4(L, ae, feF, aw, fwF);
-          sub4(L, an, fnF, as_, fsF);
-          sub4(LY, ae, feY, aw, fwY);
-          sub4(LY, an, fnY, as_, fsY);
+          int fw, fe, fs, fn;
+          member_faces(cx, cy, x0, y0, xc, xn, Nx, fw, fe, fs, fn);
+          sub4(L, ae, sF[fe], aw, sF[fw]);
+          sub4(L, an, sF[fn], as_, sF[fs]);
+          sub4(LY, ae, sY[fe], aw, sY[fw]);
+          sub4(LY, an, sY[fn], as_, sY[fs]);
         }
         // axisymmetric hoop stress
         float r = V / fmaxf(gg.y, 1e-6f), vor = vely / r;
@@ -425,7 +466,7 @@ __global__ void __launch_bounds__(NT) k_physics(PhysArgs a, rn_params P) {
           L.w -= clampf(qw, -qmax, qmax) * wl;
         }
         // shock / boundary-layer interaction on the bit-16 band
-        if (sm & 16) {
+        if (sm_ & 16) {
           float up = len2(velx, vely), Mn = up / sqrtf((1.0f + 1.0f / G) * p / rho);
           if (Mn > 1.0f) {
             float shx = velx / up, shy = vely / up;
@@ -548,10 +589,9 @@ struct Neu {
 };
 __device__ double warp_sum_exact(Neu n) {
   // combine the lanes' (s, c) pairs in lane order on lane 0: deterministic
-  double s = n.s, c = n.c;
   __shared__ double bs[32], bc[32];
-  bs[threadIdx.x] = s;
-  bc[threadIdx.x] = c;
+  bs[threadIdx.x] = n.s;
+  bc[threadIdx.x] = n.c;
   __syncwarp();
   double r = 0.0;
   if (threadIdx.x == 0) {
@@ -617,10 +657,38 @@ __global__ void k_integrals(Grid g, const float4* __restrict__ A, const float4* 
 
 // --------------------------------------------------------------------------
 static dim3 tiles(const Grid& g) { return dim3((g.Nx + TX - 1) / TX, (g.Nr + TY - 1) / TY); }
+// dynamic shared memory for a largest per-tile member list of maxX cells
+size_t stage_smem(int maxX) {
+  return sizeof(float4) * (2 * (NPT + 25 * maxX) + 2 * (NXF + NRF + 4 * maxX)) + sizeof(float) * (NXF + NRF + 4 * maxX);
+}
+size_t physics_smem(int maxX) {
+  return sizeof(float4) * (2 * (NPT + 25 * maxX) + 2 * (NTT + 5 * maxX) + 2 * (NXF + NRF + 4 * maxX));
+}
 
-void launch_stage1(const StageArgs& a, const rn_params& P, cudaStream_t s) { k_stage<1><<<tiles(a.g), NT, 0, s>>>(a, P); }
-void launch_stage2(const StageArgs& a, const rn_params& P, cudaStream_t s) { k_stage<2><<<tiles(a.g), NT, 0, s>>>(a, P); }
-void launch_physics(const PhysArgs& a, const rn_params& P, cudaStream_t s) { k_physics<<<tiles(a.g), NT, 0, s>>>(a, P); }
+// Raises the dynamic shared-memory limit of the stage and physics kernels to
+// what a member list of MAXX cells needs (a process-wide function attribute).
+int stage_kernels_init() {
+  if (cudaFuncSetAttribute(k_stage<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(stage_smem(MAXX))) !=
+      cudaSuccess)
+    return -1;
+  if (cudaFuncSetAttribute(k_stage<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(stage_smem(MAXX))) !=
+      cudaSuccess)
+    return -1;
+  if (cudaFuncSetAttribute(k_physics, cudaFuncAttributeMaxDynamicSharedMemorySize, int(physics_smem(MAXX))) !=
+      cudaSuccess)
+    return -1;
+  return 0;
+}
+
+void launch_stage1(const StageArgs& a, const rn_params& P, cudaStream_t s) {
+  k_stage<1><<<tiles(a.g), NT, stage_smem(a.maxX), s>>>(a, P);
+}
+void launch_stage2(const StageArgs& a, const rn_params& P, cudaStream_t s) {
+  k_stage<2><<<tiles(a.g), NT, stage_smem(a.maxX), s>>>(a, P);
+}
+void launch_physics(const PhysArgs& a, const rn_params& P, cudaStream_t s) {
+  k_physics<<<tiles(a.g), NT, physics_smem(a.maxX), s>>>(a, P);
+}
 void launch_reduce(const Grid& g, const float4* A, const float4* B, unsigned* w, cudaStream_t s) {
   int N = g.Nx * g.Nr;
   int blocks = (N + NT - 1) / NT;

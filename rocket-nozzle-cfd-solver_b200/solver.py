@@ -28,7 +28,8 @@ EXPORTS = ("rn_create", "rn_destroy", "rn_resize", "rn_set_mask", "rn_set_geomet
            "rn_get_state", "rn_step", "rn_rescale_ambient", "rn_draw_wall_row", "rn_read_rect",
            "rn_read_step_info", "rn_request_async", "rn_poll_async", "rn_cancel_async", "rn_spray_set_injector",
            "rn_spray_reset", "rn_spray_stats", "rn_integrals", "rn_sync", "rn_wait", "rn_kernel_launches",
-           "rn_last_error")
+           "rn_get_stream", "rn_profile", "rn_profile_read", "rn_last_error")
+KERNEL_KINDS = ("reduce", "stage1", "stage2", "physics", "parcels", "apply", "other")
 
 
 class RnError(RuntimeError):
@@ -139,6 +140,9 @@ def lib():
     L.rn_sync.argtypes = [H]
     L.rn_wait.argtypes = [H, i]
     L.rn_kernel_launches.argtypes = [H, ctypes.POINTER(ctypes.c_longlong)]
+    L.rn_get_stream.argtypes = [H, ctypes.POINTER(ctypes.c_void_p)]
+    L.rn_profile.argtypes = [H, i]
+    L.rn_profile_read.argtypes = [H, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)]
     L.rn_last_error.restype = ctypes.c_char_p
     for n in EXPORTS[:-1]:
         getattr(L, n).restype = ctypes.c_int
@@ -329,6 +333,23 @@ class GPUSolver:
     def wait(self, timeout_ms):
         """Bounded wait for the queued work: True when done, False on timeout."""
         return _check(lib().rn_wait(self.h, int(timeout_ms)), (RN_OK, RN_NOT_READY)) == RN_OK
+
+    def stream(self):
+        """The handle's CUDA stream as an integer handle (cudaStream_t)."""
+        v = ctypes.c_void_p()
+        _check(lib().rn_get_stream(self.h, ctypes.byref(v)))
+        return v.value or 0
+
+    def profile(self, enable):
+        """Bracket every kernel with CUDA events on the handle's stream."""
+        _check(lib().rn_profile(self.h, 1 if enable else 0))
+
+    def profileRead(self):
+        """{kind: (milliseconds, launches)} since the last read."""
+        ms = (ctypes.c_double * len(KERNEL_KINDS))()
+        n = (ctypes.c_longlong * len(KERNEL_KINDS))()
+        _check(lib().rn_profile_read(self.h, ms, n))
+        return {k: (ms[q], n[q]) for q, k in enumerate(KERNEL_KINDS)}
 
     def kernelLaunches(self):
         v = ctypes.c_longlong()
