@@ -181,6 +181,7 @@ def run_reference(args, rank, world):
 def run_ours(args, rank, world, local_rank):
     import torch
     rn = ge.load_package()
+    from rocket_nozzle_cfd_solver_b200 import replicas
     torch.cuda.set_device(local_rank)
     setup = make_setup(rn)
     cells = setup.Nx * setup.Nr
@@ -220,11 +221,8 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
     launches = g.kernelLaunches() - launches0
     ms = sum(a.elapsed_time(b) for a, b in evs)
-    if world > 1:
-        t = torch.tensor([ms], device=f"cuda:{local_rank}", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-        torch.distributed.barrier()
+    dev = f"cuda:{local_rank}"
+    ms = replicas.max_over_ranks(ms, dev)
     value = world * cells * SOLVER_STEPS * args.steps / (ms * 1e-3)
 
     # ---- per-kernel profile over the same number of bench steps (roofline)
@@ -280,11 +278,7 @@ def run_ours(args, rank, world, local_rank):
             res = g.pollAsync()
         d = res["data"]
         perf = rn.exit_performance(setup, {"A": d["colA"], "B": d["colB"]})
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        t = torch.tensor([e2e_s], device=f"cuda:{local_rank}", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = replicas.max_over_ranks(time.perf_counter() - t0, dev)
     e2e = world * cells * SOLVER_STEPS * args.steps / e2e_s
     g.close()
 

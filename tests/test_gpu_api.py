@@ -1,0 +1,227 @@
+"""The reference-facing API over librn.so on a B200: golden fixtures, read-back
+paths, FP64 read-outs, ambient rescale, sprays, full-size grids and argument
+errors. Floating-point bar: relative L2 per conserved field <= 1e-4 against
+the oracle after N steps (the kernels use IEEE division/sqrt and no
+multiply-add contraction, so most values match bit for bit; pow/exp/log/sin/cos
+may differ in the last bit from the host's libm)."""
+import math
+import os
+
+import numpy as np
+import pytest
+
+from helpers import field_rel_l2, run_oracle
+
+pytestmark = pytest.mark.gpu
+HERE = os.path.dirname(os.path.abspath(__file__))
+TOL = 1e-4
+
+
+def golden_case(rn, name):
+    import sys
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    import make_golden
+    return make_golden.case_setup(rn, name)
+
+
+def gpu(rn, s, n=0, state=None):
+    g = rn.GPUSolver(s.Nx, s.Nr)
+    g.setGeometry(s.geo)
+    init = state if state is not None else s.initialState()
+    g.setState(init["A"], init["B"])
+    if s.injector is not None:
+        rn.GPUSpray(g).resize()
+        g.spray.setInjector(s.injector)
+    if n:
+        g.step(n, s.P)
+    return g
+
+
+def assert_close(a, b, tol=TOL):
+    for k in ("A", "B"):
+        e = field_rel_l2(a[k], b[k])
+        assert max(e) <= tol, (k, e)
+
+
+@pytest.mark.parametrize("name", ["plain", "viscous", "spray"])
+def test_golden_fixtures(rn, name):
+    s, steps = golden_case(rn, name)
+    gold = np.load(os.path.join(HERE, "golden", f"oracle_{name}.npz"))
+    g = gpu(rn, s, steps)
+    out = g.readAll()
+    assert_close(out, {"A": gold["A"], "B": gold["B"]}, 1e-5)
+    same = np.mean(out["A"] == gold["A"])
+    print(f"{name}: {100 * same:.2f} % of A floats bit-identical to the oracle")
+    assert np.allclose(g.readStepInfo(), gold["stepinfo"], rtol=1e-6)
+    g.close()
+
+
+def test_readbacks_agree(rn):
+    s, _ = golden_case(rn, "plain")
+    g = gpu(rn, s, 25)
+    full = g.readAll()
+    A, B = full["A"].reshape(s.Nr, s.Nx, 4), full["B"].reshape(s.Nr, s.Nx, 4)
+    col = g.readColumn(s.iExit)
+    assert np.array_equal(col["A"].reshape(-1, 4), A[:, s.iExit])
+    assert np.array_equal(col["B"].reshape(-1, 4), B[:, s.iExit])
+    cell = g.readCell(s.iChamber, 3)
+    assert np.array_equal(cell["A"], A[3, s.iChamber])
+    st = g.state
+    reqs = [{"name": "step", "tex": g.stepInfoTex, "x": 0, "y": 0, "w": 1, "h": 1},
+            {"name": "colA", "tex": st["A"], "x": s.iExit, "y": 0, "w": 1, "h": s.Nr},
+            {"name": "blkB", "tex": st["B"], "x": 2, "y": 1, "w": 5, "h": 3}]
+    assert g.requestAsync(reqs, 7)
+    assert g.requestAsync(reqs, 8) is False                 # one read in flight at a time
+    res = None
+    for _ in range(100000):
+        res = g.pollAsync()
+        if res is not None:
+            break
+    assert res["tag"] == 7
+    assert np.array_equal(res["data"]["step"], g.readStepInfo())
+    assert np.array_equal(res["data"]["colA"].reshape(-1, 4), A[:, s.iExit])
+    assert np.array_equal(res["data"]["blkB"].reshape(3, 5, 4), B[1:4, 2:7])
+    assert g.pollAsync() is None
+    assert g.requestAsync(reqs[:1], 9)
+    g.cancelAsync()
+    assert g.pollAsync() is None
+    with pytest.raises(rn.RnError):
+        g._readRect(st["A"], s.Nx - 1, 0, 2, 1)              # out of range
+    g.close()
+
+
+def test_integrals_match_js_readout(rn):
+    from rocket_nozzle_cfd_solver_b200.physics import P_REF, RHO_REF, U_REF
+    s, _ = golden_case(rn, "plain")
+    g = gpu(rn, s, 300)
+    integ = g.integrals(s)
+    col = g.readColumn(s.iExit)
+    perf = rn.exit_performance(s, col)
+    assert integ["F"] * P_REF == pytest.approx(perf["F"], rel=1e-10, abs=1e-9)
+    assert integ["mdot"] * RHO_REF * U_REF == pytest.approx(perf["mdot"], rel=1e-10, abs=1e-12)
+    ch = g.readCell(s.iChamber, 0)
+    c = rn.cell_prim_si(s, ch["A"], ch["B"])
+    assert integ["chamber_p"] * P_REF == pytest.approx(c["p"], rel=1e-12)
+    si = g.readStepInfo()
+    assert integ["dt"] == float(si[0]) and integ["t"] == float(si[2])
+    g.close()
+
+
+def test_rescale_ambient_matches_oracle(rn, oracle):
+    """Altitude change 0 -> 20 km at a fixed step (the app's live change made
+    step-indexed): FS_RESCALE then steps with the new parameter block."""
+    from rocket_nozzle_cfd_solver_b200 import configs
+    cfg = configs.viscous_plume(96, 36)[0]
+    s = rn.build_sim_setup(cfg)
+    cfg2 = dict(s.cfg, alt=20000.0)
+    P2 = rn.compute_params(cfg2, s.contour, s.dx, cfg["Pc"], s.atm["p"])
+    fp, fT, du = P2["amb"][3] / s.P["amb"][3], P2["Ta"] / s.P["Ta"], P2["amb"][1] - s.P["amb"][1]
+    g = gpu(rn, s, 60)
+    g.rescaleAmbient(fp, fT, du, P2)
+    g.step(40, P2)
+    o = run_oracle(oracle, s, 60)
+    o.rescaleAmbient(fp, fT, du, P2)
+    o.step(40, P2)
+    assert_close(g.readAll(), o.readAll())
+    g.close()
+
+
+def test_wall_row_matches_oracle(rn, oracle):
+    s, _ = golden_case(rn, "viscous")
+    g = gpu(rn, s, 80)
+    o = run_oracle(oracle, s, 80)
+    row = g._readRect(g.drawWallRow(), 0, 0, s.Nx, 1)
+    ref = o.readWallRow()
+    assert np.allclose(row, ref, rtol=1e-5, atol=1e-6)
+    g.close()
+
+
+def test_spray_parcels_match_oracle(rn, oracle):
+    s, _ = golden_case(rn, "spray")
+    g = gpu(rn, s, 150)
+    o = run_oracle(oracle, s, 150)
+    par, ref = g.spray.readParcels(), o.readParcels()
+    alive_g = par["PB"].reshape(-1, 4)[:, 1] > 0
+    alive_o = ref["PB"].reshape(-1, 4)[:, 1] > 0
+    assert np.array_equal(alive_g, alive_o)
+    for k in ("PA", "PB"):
+        assert max(field_rel_l2(par[k], ref[k])) < TOL
+    st = g.spray.stats()
+    PB = ref["PB"].reshape(-1, 4)
+    assert st["parcels"] == int(alive_o.sum())
+    assert st["ox"] == pytest.approx(float(PB[alive_o & (PB[:, 2] >= 0.5), 1].sum()), rel=1e-4)
+    assert_close(g.readAll(), o.readAll())
+    g.close()
+
+
+def test_full_size_viscous_plume(rn, oracle):
+    """BASELINE's viscous plume grid (512 x 192), 100 steps."""
+    from rocket_nozzle_cfd_solver_b200 import configs
+    s = rn.build_sim_setup(configs.viscous_plume()[0])
+    g = gpu(rn, s, 100)
+    assert_close(g.readAll(), run_oracle(oracle, s, 100).readAll())
+    g.close()
+
+
+def test_large_grid_and_conservation_of_topology(rn, oracle):
+    """1024 x 384 (the batched config's largest grid): 20 steps against the oracle."""
+    from rocket_nozzle_cfd_solver_b200 import configs
+    s = rn.build_sim_setup(configs.viscous_plume(1024, 384)[0])
+    g = gpu(rn, s, 20)
+    assert_close(g.readAll(), run_oracle(oracle, s, 20).readAll())
+    g.close()
+
+
+def test_set_state_resets_and_resumes(rn):
+    s, _ = golden_case(rn, "plain")
+    g = gpu(rn, s, 30)
+    snap = g.readAll()
+    si = g.readStepInfo()
+    g.step(20, s.P)
+    after = g.readAll()
+    # resume from the snapshot: state restored, dt/t cleared (setState resets the step info)
+    g.setState(snap["A"], snap["B"])
+    again = g.readAll()
+    assert np.array_equal(again["A"], snap["A"]) and np.array_equal(g.readStepInfo(), np.zeros(4, np.float32))
+    assert si[2] > 0 and not np.array_equal(after["A"], snap["A"])
+    g.close()
+
+
+def test_bad_geometry_rejected(rn):
+    s, _ = golden_case(rn, "plain")
+    g = rn.GPUSolver(s.Nx, s.Nr)
+    geo = dict(s.geo)
+    gm = geo["geoM"].copy().reshape(-1, 4)
+    k = int(np.nonzero(s.mask == 0)[0][5])
+    gm[k, 0] = 2.0                                           # host two cells away: not a neighbour
+    geo["geoM"] = gm.reshape(-1)
+    with pytest.raises(rn.RnError) as e:
+        g.setGeometry(geo)
+    assert e.value.code == -1
+    with pytest.raises(ValueError):
+        g.setState(np.zeros(3, np.float32), np.zeros(3, np.float32))
+    g.close()
+
+
+def test_bounded_wait(rn):
+    s, _ = golden_case(rn, "viscous")
+    g = gpu(rn, s)
+    g.step(400, s.P)
+    assert g.wait(120000)                                    # finishes well inside the limit
+    assert g.wait(0)                                         # nothing queued: immediate
+    g.close()
+
+
+def test_kernel_launch_accounting(rn):
+    s, _ = golden_case(rn, "viscous")
+    g = gpu(rn, s)
+    n0 = g.kernelLaunches()
+    g.step(10, s.P)
+    g.sync()
+    assert g.kernelLaunches() - n0 == 1 + 3 * 10         # first-step CFL reduction + 3 kernels per step
+    g.profile(True)
+    g.step(5, s.P)
+    prof = g.profileRead()
+    assert prof["stage1"][1] == 5 and prof["stage2"][1] == 5 and prof["physics"][1] == 5
+    assert all(v[0] > 0 for k, v in prof.items() if v[1])
+    g.close()
