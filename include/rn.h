@@ -150,6 +150,19 @@ int rn_sync(rn_handle h);
 int rn_wait(rn_handle h, int timeout_ms);
 /* number of kernels this handle has launched (for launch accounting) */
 int rn_kernel_launches(rn_handle h, long long* out);
+/* Arithmetic of the step kernels. The reference's shaders run in GLSL highp,
+ * whose division and square root may be off by up to a few ulp.
+ *   RN_PRECISION_FAST (default): the hardware's approximate division and
+ *     square root (within 2 ulp), the same latitude;
+ *   RN_PRECISION_EXACT: IEEE-rounded division and square root, so the state
+ *     reproduces the CPU oracle of the shader passes bit for bit except where
+ *     pow/exp/log/sin/cos differ in the last bit. About 1.7x slower.
+ * No reference counterpart (the reference has one shader build). */
+#define RN_PRECISION_FAST 0
+#define RN_PRECISION_EXACT 1
+int rn_set_precision(rn_handle h, int mode);
+int rn_get_precision(rn_handle h, int* mode);
+
 /* the handle's CUDA stream (a cudaStream_t), so a caller can order its own
  * work (timing events, cache flushes) with the handle's kernels */
 int rn_get_stream(rn_handle h, void** stream);

@@ -80,6 +80,8 @@ struct rn_solver {
   int* xoff = nullptr;
   int* xcell = nullptr;
   int maxX = 1;
+  // kernels of the selected precision (rn_set_precision)
+  const KernelSet* K = &kernels_fast;
 
   Grid grid() const { return Grid{Nx, Nr, mask, geoA, geoG, geoM}; }
 };
@@ -162,7 +164,7 @@ int alloc_buffers(rn_solver* h, int Nx, int Nr) {
   h->val = h->key + SPRAY_N;
   h->keyS = h->key + 2 * SPRAY_N;
   h->valS = h->key + 3 * SPRAY_N;
-  h->sortTempBytes = spray_sort_temp_bytes(int(N));
+  h->sortTempBytes = std::max(kernels_exact.sortTempBytes(int(N)), kernels_fast.sortTempBytes(int(N)));
   CK(cudaMalloc(&h->sortTemp, h->sortTempBytes > 0 ? h->sortTempBytes : 16));
   h->cur = 0; h->stepIdx = 0; h->wslot = 0; h->wvalid = false; h->stepCount = 0;
   h->seed = 1;
@@ -279,7 +281,7 @@ int rn_create(int Nx, int Nr, rn_handle* out) {
   if (e != cudaSuccess) { cudaStreamDestroy(h->stream); delete h; return cuda_fail(e, "cudaEventCreate"); }
   static bool kernels_ready = false;
   if (!kernels_ready) {
-    if (stage_kernels_init() != 0) {
+    if (kernels_exact.init() != 0 || kernels_fast.init() != 0) {
       cudaEventDestroy(h->asyncEv);
       cudaStreamDestroy(h->stream);
       delete h;
@@ -393,7 +395,7 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
     if (!h->wvalid) {
       CK(cudaMemsetAsync(wIn, 0, sizeof(unsigned), h->stream));
       ProfScope ps(h, RN_K_REDUCE);
-      launch_reduce(g, h->SA[s0], h->SB[s0], wIn, h->stream);
+      h->K->reduce(g, h->SA[s0], h->SB[s0], wIn, h->stream);
       h->launches++;
     }
     float4* stPrev = h->stepTex + h->stepIdx;
@@ -407,7 +409,7 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
     a.xoff = h->xoff; a.xcell = h->xcell; a.maxX = h->maxX;
     {
       ProfScope ps(h, RN_K_STAGE1);
-      launch_stage1(a, *P, h->stream);
+      h->K->stage1(a, *P, h->stream);
     }
     h->launches++;
     if (inj) {
@@ -421,7 +423,7 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
       sp.head = int(h->head); sp.seed = int(h->seed);
       int launched = 0;
       ProfScope ps(h, RN_K_PARCELS);
-      if (launch_spray(sp, *P, h->sortTemp, h->sortTempBytes, h->keyS, h->valS, h->src, h->stream, &launched) != 0)
+      if (h->K->spray(sp, *P, h->sortTemp, h->sortTempBytes, h->keyS, h->valS, h->src, h->stream, &launched) != 0)
         return fail(RN_ERR_CUDA, "rn_step: deposit sort failed");
       h->launches += launched;
     }
@@ -431,7 +433,7 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
     b.finalCfl = (!phys && !inj) ? 1 : 0;
     {
       ProfScope ps(h, RN_K_STAGE2);
-      launch_stage2(b, *P, h->stream);
+      h->K->stage2(b, *P, h->stream);
     }
     h->launches++;
     h->cur = s2;
@@ -444,7 +446,7 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
       p.xoff = h->xoff; p.xcell = h->xcell; p.maxX = h->maxX;
       {
         ProfScope ps(h, RN_K_PHYSICS);
-        launch_physics(p, *P, h->stream);
+        h->K->physics(p, *P, h->stream);
       }
       h->launches++;
       h->cur = s0;
@@ -458,7 +460,7 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
       ap.wOut = wOut; ap.finalCfl = 1;
       {
         ProfScope ps(h, RN_K_APPLY);
-        launch_apply(ap, *P, h->stream);
+        h->K->apply(ap, *P, h->stream);
       }
       h->launches++;
       h->cur = out;
@@ -481,7 +483,7 @@ int rn_rescale_ambient(rn_handle h, float fp, float fT, float du, const rn_param
   const int s0 = h->cur, s1 = (h->cur + 1) % 3;
   {
     ProfScope ps(h, RN_K_OTHER);
-    launch_rescale(h->grid(), h->SA[s0], h->SB[s0], h->SA[s1], h->SB[s1], fp, fT, du, *P, h->stream);
+    h->K->rescale(h->grid(), h->SA[s0], h->SB[s0], h->SA[s1], h->SB[s1], fp, fT, du, *P, h->stream);
   }
   h->launches++;
   h->cur = s1;
@@ -492,7 +494,7 @@ int rn_rescale_ambient(rn_handle h, float fp, float fT, float du, const rn_param
 
 int rn_draw_wall_row(rn_handle h) {
   if (!valid(h)) return fail(RN_ERR_ARG, "rn_draw_wall_row: bad handle");
-  launch_wallrow(h->grid(), h->SA[h->cur], h->SB[h->cur], h->jw, h->wallRow, h->stream);
+  h->K->wallrow(h->grid(), h->SA[h->cur], h->SB[h->cur], h->jw, h->wallRow, h->stream);
   h->launches++;
   CK(cudaGetLastError());
   return RN_OK;
@@ -620,7 +622,7 @@ int rn_integrals(rn_handle h, const rn_integral_spec* spec, rn_integrals_out* ou
   if (spec->iExit < 0 || spec->iExit + 1 > h->Nx || spec->jExit < 0 || spec->jExit > h->Nr || spec->iThroat < 0 ||
       spec->iThroat >= h->Nx || spec->iChamber < 0 || spec->iChamber >= h->Nx)
     return fail(RN_ERR_ARG, "rn_integrals: column index out of range");
-  launch_integrals(h->grid(), h->SA[h->cur], h->SB[h->cur], h->geoA, *spec, h->stepTex + h->stepIdx, h->dInt,
+  h->K->integrals(h->grid(), h->SA[h->cur], h->SB[h->cur], h->geoA, *spec, h->stepTex + h->stepIdx, h->dInt,
                    h->stream);
   h->launches++;
   double r[12];
@@ -649,6 +651,19 @@ int rn_wait(rn_handle h, int timeout_ms) {
     if (ms >= timeout_ms) return RN_NOT_READY;
     std::this_thread::sleep_for(std::chrono::microseconds(200));
   }
+}
+
+int rn_set_precision(rn_handle h, int mode) {
+  if (!h || (mode != RN_PRECISION_FAST && mode != RN_PRECISION_EXACT))
+    return fail(RN_ERR_ARG, "rn_set_precision: bad handle or mode");
+  h->K = mode == RN_PRECISION_EXACT ? &kernels_exact : &kernels_fast;
+  return RN_OK;
+}
+
+int rn_get_precision(rn_handle h, int* mode) {
+  if (!h || !mode) return fail(RN_ERR_ARG, "rn_get_precision: bad argument");
+  *mode = h->K == &kernels_exact ? RN_PRECISION_EXACT : RN_PRECISION_FAST;
+  return RN_OK;
 }
 
 int rn_get_stream(rn_handle h, void** stream) {

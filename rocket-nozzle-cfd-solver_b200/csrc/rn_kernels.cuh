@@ -60,21 +60,32 @@ struct ApplyArgs {
   int finalCfl;
 };
 
-void launch_stage1(const StageArgs& a, const rn_params& P, cudaStream_t s);
-void launch_stage2(const StageArgs& a, const rn_params& P, cudaStream_t s);
-void launch_physics(const PhysArgs& a, const rn_params& P, cudaStream_t s);
-void launch_reduce(const Grid& g, const float4* A, const float4* B, unsigned* w, cudaStream_t s);
-void launch_rescale(const Grid& g, const float4* A, const float4* B, float4* oA, float4* oB, float fp, float fT,
-                    float du, const rn_params& P, cudaStream_t s);
-void launch_wallrow(const Grid& g, const float4* A, const float4* B, const float4* jw, float4* row, cudaStream_t s);
-void launch_integrals(const Grid& g, const float4* A, const float4* B, const float4* geoAx, const rn_integral_spec& spec,
-                      const float4* st, double* out, cudaStream_t s);
-int launch_spray(const SprayArgs& a, const rn_params& P, void* sortTemp, size_t sortTempBytes, unsigned* keyOut,
-                 unsigned* valOut, float4* src, cudaStream_t s, int* launches);
-void launch_apply(const ApplyArgs& a, const rn_params& P, cudaStream_t s);
-size_t spray_sort_temp_bytes(int Ncells);
-int stage_kernels_init();           // opts the kernels into the dynamic shared memory they need
-size_t stage_smem(int maxX);        // dynamic shared memory of a stage launch
-size_t physics_smem(int maxX);      // dynamic shared memory of a physics launch
+// The kernels are compiled twice from the same sources (rn_variant.cu):
+//   exact -- IEEE division and square root: every float operation rounds as
+//            written, so the state matches the CPU oracle bit for bit wherever
+//            pow/exp/log/sin/cos agree with the host's libm;
+//   fast  -- the hardware's approximate division (div.full) and square root
+//            (within 2 ulp, the latitude GLSL highp gives the reference's
+//            shaders); agrees with the oracle to ~1e-6 relative L2.
+// A solver handle launches through one of the two sets.
+struct KernelSet {
+  const char* name;
+  void (*stage1)(const StageArgs& a, const rn_params& P, cudaStream_t s);
+  void (*stage2)(const StageArgs& a, const rn_params& P, cudaStream_t s);
+  void (*physics)(const PhysArgs& a, const rn_params& P, cudaStream_t s);
+  void (*reduce)(const Grid& g, const float4* A, const float4* B, unsigned* w, cudaStream_t s);
+  void (*rescale)(const Grid& g, const float4* A, const float4* B, float4* oA, float4* oB, float fp, float fT,
+                  float du, const rn_params& P, cudaStream_t s);
+  void (*wallrow)(const Grid& g, const float4* A, const float4* B, const float4* jw, float4* row, cudaStream_t s);
+  void (*integrals)(const Grid& g, const float4* A, const float4* B, const float4* geoAx,
+                    const rn_integral_spec& spec, const float4* st, double* out, cudaStream_t s);
+  int (*spray)(const SprayArgs& a, const rn_params& P, void* sortTemp, size_t sortTempBytes, unsigned* keyOut,
+               unsigned* valOut, float4* src, cudaStream_t s, int* launches);
+  void (*apply)(const ApplyArgs& a, const rn_params& P, cudaStream_t s);
+  size_t (*sortTempBytes)(int Ncells);
+  int (*init)();                    // opts the kernels into the dynamic shared memory they need
+};
+extern const KernelSet kernels_exact;
+extern const KernelSet kernels_fast;
 
 }  // namespace rn

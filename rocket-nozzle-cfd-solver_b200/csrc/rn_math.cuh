@@ -235,15 +235,6 @@ RN_DEV Flux face_flux(bool DIR_R, float area, float4 w0, float4 b0, float4 w1, f
   if (SL >= 0.0f) { F0 = FL0; F1 = FL1; F2 = FL2; F3 = FL3; Y0 = YL0; Y1 = YL1; Y2 = YL2; uf = uL; Gf = GL; }
   else if (SR <= 0.0f) { F0 = FR0; F1 = FR1; F2 = FR2; F3 = FR3; Y0 = YR0; Y1 = YR1; Y2 = YR2; uf = uR; Gf = GR; }
   else {
-    float inv = 1.0f / (SR - SL);
-    float SLR = SL * SR;
-    float H0 = (SR * FL0 - SL * FR0 + SLR * (rR - rL)) * inv;
-    float H1 = (SR * FL1 - SL * FR1 + SLR * (mR - mL)) * inv;
-    float H2 = (SR * FL2 - SL * FR2 + SLR * (rR * vR - rL * vL)) * inv;
-    float H3 = (SR * FL3 - SL * FR3 + SLR * (ER - EL)) * inv;
-    float HY0 = (SR * YL0 - SL * YR0 + SLR * (rR * WRs.x - rL * WLs.x)) * inv;
-    float HY1 = (SR * YL1 - SL * YR1 + SLR * (rR * WRs.y - rL * WLs.y)) * inv;
-    float HY2 = (SR * YL2 - SL * YR2 + SLR * (rR * WRs.w - rL * WLs.w)) * inv;
     float Ss = (pR - pL + mL * (SL - uL) - mR * (SR - uR)) / (rL * (SL - uL) - rR * (SR - uR));
     bool left = Ss >= 0.0f;
     float rK = left ? rL : rR, uK = left ? uL : uR, vK = left ? vL : vR, pK = left ? pL : pR;
@@ -257,8 +248,24 @@ RN_DEV Flux face_flux(bool DIR_R, float area, float4 w0, float4 b0, float4 w1, f
     float C0 = FK0 + SK * (Us0 - rK), C1 = FK1 + SK * (Us1 - UK1), C2 = FK2 + SK * (Us2 - UK2), C3 = FK3 + SK * (Us3 - EK);
     float CY0 = FYK0 + SK * (kk * YK0 - rK * YK0), CY1 = FYK1 + SK * (kk * YK1 - rK * YK1);
     float CY2 = FYK2 + SK * (kk * YK2 - rK * YK2);
-    F0 = mixf(C0, H0, hllw); F1 = mixf(C1, H1, hllw); F2 = mixf(C2, H2, hllw); F3 = mixf(C3, H3, hllw);
-    Y0 = mixf(CY0, HY0, hllw); Y1 = mixf(CY1, HY1, hllw); Y2 = mixf(CY2, HY2, hllw);
+    if (hllw != 0.0f) {
+      float inv = 1.0f / (SR - SL);
+      float SLR = SL * SR;
+      float H0 = (SR * FL0 - SL * FR0 + SLR * (rR - rL)) * inv;
+      float H1 = (SR * FL1 - SL * FR1 + SLR * (mR - mL)) * inv;
+      float H2 = (SR * FL2 - SL * FR2 + SLR * (rR * vR - rL * vL)) * inv;
+      float H3 = (SR * FL3 - SL * FR3 + SLR * (ER - EL)) * inv;
+      float HY0 = (SR * YL0 - SL * YR0 + SLR * (rR * WRs.x - rL * WLs.x)) * inv;
+      float HY1 = (SR * YL1 - SL * YR1 + SLR * (rR * WRs.y - rL * WLs.y)) * inv;
+      float HY2 = (SR * YL2 - SL * YR2 + SLR * (rR * WRs.w - rL * WLs.w)) * inv;
+      F0 = mixf(C0, H0, hllw); F1 = mixf(C1, H1, hllw); F2 = mixf(C2, H2, hllw); F3 = mixf(C3, H3, hllw);
+      Y0 = mixf(CY0, HY0, hllw); Y1 = mixf(CY1, HY1, hllw); Y2 = mixf(CY2, HY2, hllw);
+    } else {
+      // mix(Fc, Fhll, 0) = Fc + 0 Fhll: the HLL flux only decides the sign of
+      // a zero component, so it is not computed where the sensor is quiet
+      F0 = C0; F1 = C1; F2 = C2; F3 = C3;
+      Y0 = CY0; Y1 = CY1; Y2 = CY2;
+    }
     uf = uK + SK * ((SK - uK) / (SK - Ss) - 1.0f);
     Gf = left ? GL : GR;
   }

@@ -19,8 +19,9 @@
 #include "rn_kernels.cuh"
 
 namespace rn {
+namespace RN_VARIANT {
 
-constexpr int SPRAY_W = 256, SPRAY_N = 65536, SPRAY_PER_STEP = 4;   // spray.js:16-17
+constexpr int SPRAY_N = 65536, SPRAY_PER_STEP = 4;   // 256 x 256 ring, 4 born per step (spray.js:16-17)
 
 // pcg / rnd (spray.js:33-34): 32-bit integer hash, bit-exact with the shader
 __device__ __forceinline__ uint32_t pcg(uint32_t v) {
@@ -249,4 +250,5 @@ void launch_apply(const ApplyArgs& a, const rn_params& P, cudaStream_t s) {
   k_apply<<<(N + 255) / 256, 256, 0, s>>>(a, P);
 }
 
+}  // namespace RN_VARIANT
 }  // namespace rn

@@ -27,6 +27,7 @@
 #include "rn_kernels.cuh"
 
 namespace rn {
+namespace RN_VARIANT {
 
 constexpr int PX = TX + 4, PY = TY + 4;      // primitive tile with a 2-cell halo
 constexpr int NPT = PX * PY;                  // tile primitives
@@ -708,4 +709,5 @@ void launch_integrals(const Grid& g, const float4* A, const float4* B, const flo
   k_integrals<<<1, 32, 0, s>>>(g, A, B, geoAx, spec, st, out);
 }
 
+}  // namespace RN_VARIANT
 }  // namespace rn

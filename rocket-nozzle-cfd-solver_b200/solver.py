@@ -28,7 +28,9 @@ EXPORTS = ("rn_create", "rn_destroy", "rn_resize", "rn_set_mask", "rn_set_geomet
            "rn_get_state", "rn_step", "rn_rescale_ambient", "rn_draw_wall_row", "rn_read_rect",
            "rn_read_step_info", "rn_request_async", "rn_poll_async", "rn_cancel_async", "rn_spray_set_injector",
            "rn_spray_reset", "rn_spray_stats", "rn_integrals", "rn_sync", "rn_wait", "rn_kernel_launches",
-           "rn_get_stream", "rn_profile", "rn_profile_read", "rn_last_error")
+           "rn_set_precision", "rn_get_precision", "rn_get_stream", "rn_profile", "rn_profile_read",
+           "rn_last_error")
+PRECISION = {"fast": 0, "exact": 1}
 KERNEL_KINDS = ("reduce", "stage1", "stage2", "physics", "parcels", "apply", "other")
 
 
@@ -141,6 +143,8 @@ def lib():
     L.rn_wait.argtypes = [H, i]
     L.rn_kernel_launches.argtypes = [H, ctypes.POINTER(ctypes.c_longlong)]
     L.rn_get_stream.argtypes = [H, ctypes.POINTER(ctypes.c_void_p)]
+    L.rn_set_precision.argtypes = [H, i]
+    L.rn_get_precision.argtypes = [H, ctypes.POINTER(i)]
     L.rn_profile.argtypes = [H, i]
     L.rn_profile_read.argtypes = [H, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)]
     L.rn_last_error.restype = ctypes.c_char_p
@@ -333,6 +337,18 @@ class GPUSolver:
     def wait(self, timeout_ms):
         """Bounded wait for the queued work: True when done, False on timeout."""
         return _check(lib().rn_wait(self.h, int(timeout_ms)), (RN_OK, RN_NOT_READY)) == RN_OK
+
+    def setPrecision(self, mode):
+        """'fast' (default: hardware approximate division/sqrt, GLSL highp
+        latitude) or 'exact' (IEEE division/sqrt: bit for bit with the CPU
+        oracle except where pow/exp/log/sin/cos differ in the last bit)."""
+        _check(lib().rn_set_precision(self.h, PRECISION[mode]))
+
+    @property
+    def precision(self):
+        v = ctypes.c_int()
+        _check(lib().rn_get_precision(self.h, ctypes.byref(v)))
+        return {b: a for a, b in PRECISION.items()}[v.value]
 
     def stream(self):
         """The handle's CUDA stream as an integer handle (cudaStream_t)."""
