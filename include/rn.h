@@ -182,6 +182,24 @@ int rn_get_stream(rn_handle h, void** stream);
 int rn_profile(rn_handle h, int enable);
 int rn_profile_read(rn_handle h, double ms[RN_NKERNELS], long long launches[RN_NKERNELS]);
 
+/* FP64 read-outs without any device allocation. No counterpart in the
+ * reference (its read-outs are JavaScript over read-back columns). Same
+ * results as rn_integrals, for callers that cannot allocate device memory
+ * when they need a read-out: an application that reserves the whole device
+ * memory budget up front and forbids later allocation, or a latency-critical
+ * loop that cannot take cudaMalloc's implicit synchronisation. The caller
+ * passes its own device buffers: state planes A and B (Nx*Nr float4), geoA
+ * ((Nx+1)*(Nr+1) float4), mask (Nx*Nr bytes) and the step-info float4;
+ * stream is a cudaStream_t or NULL. Scratch lives in a file-scope __device__
+ * array (per-row terms of up to RN_STATIC_MAX_ROWS rows, 256 KiB, held by
+ * every GPU that loads the library until exit); Nr above that limit is
+ * rejected with RN_ERR_ARG. The first call on a device looks up the array's
+ * device address; make it before any stream capture. Calls share the array:
+ * calls that overlap on the GPU race. Blocks until `out` is filled. */
+#define RN_STATIC_MAX_ROWS 4096
+int rn_integrals_static(const float* A, const float* B, const float* geoA, const uint8_t* mask, int Nx, int Nr,
+                        const float* stepinfo, const rn_integral_spec* spec, rn_integrals_out* out, void* stream);
+
 /* message of the calling thread's last error ("" if none) */
 const char* rn_last_error(void);
 

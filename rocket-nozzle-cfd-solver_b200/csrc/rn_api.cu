@@ -42,6 +42,9 @@ constexpr int SPRAY_N = 65536;
 
 }  // namespace
 
+// Shared with rn_static.cu so its errors also reach rn_last_error().
+int rn_record_error(int code, const std::string& msg) { return fail(code, msg); }
+
 struct rn_solver {
   int Nx = 0, Nr = 0, device = 0;
   cudaStream_t stream = nullptr;

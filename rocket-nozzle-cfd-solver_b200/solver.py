@@ -29,6 +29,7 @@ EXPORTS = ("rn_create", "rn_destroy", "rn_resize", "rn_set_mask", "rn_set_geomet
            "rn_read_step_info", "rn_request_async", "rn_poll_async", "rn_cancel_async", "rn_spray_set_injector",
            "rn_spray_reset", "rn_spray_stats", "rn_integrals", "rn_sync", "rn_wait", "rn_kernel_launches",
            "rn_set_precision", "rn_get_precision", "rn_get_stream", "rn_profile", "rn_profile_read",
+           "rn_integrals_static",
            "rn_last_error")
 PRECISION = {"fast": 0, "exact": 1}
 KERNEL_KINDS = ("reduce", "stage1", "stage2", "physics", "parcels", "apply", "other")
@@ -139,6 +140,9 @@ def lib():
     L.rn_spray_reset.argtypes = [H]
     L.rn_spray_stats.argtypes = [H, ctypes.POINTER(ctypes.c_double)]
     L.rn_integrals.argtypes = [H, ctypes.POINTER(RnIntegralSpec), ctypes.POINTER(RnIntegralsOut)]
+    # read-outs from caller-owned device buffers, no device allocation (include/rn.h)
+    L.rn_integrals_static.argtypes = [ctypes.c_void_p] * 4 + [i, i, ctypes.c_void_p, ctypes.POINTER(RnIntegralSpec),
+                                                              ctypes.POINTER(RnIntegralsOut), ctypes.c_void_p]
     L.rn_sync.argtypes = [H]
     L.rn_wait.argtypes = [H, i]
     L.rn_kernel_launches.argtypes = [H, ctypes.POINTER(ctypes.c_longlong)]
