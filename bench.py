@@ -281,6 +281,11 @@ def run_ours(args, rank, world, local_rank):
     e2e_s = replicas.max_over_ranks(time.perf_counter() - t0, dev)
     e2e = world * cells * SOLVER_STEPS * args.steps / e2e_s
     g.close()
+    del flush
+    torch.cuda.empty_cache()
+    batched = None
+    if world == 1 and args.batch_instances > 0:
+        batched = run_batched(args, local_rank)
 
     if rank != 0:
         return
@@ -300,8 +305,95 @@ def run_ours(args, rank, world, local_rank):
             "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "exit_thrust_N": perf["F"] if perf else None},
             "steady_state_value": steady,
-            "gpu_launches": launches, "clocks": clk.summary()}
+            "gpu_launches": launches, "clocks": clk.summary(), "batched": batched}
     print(json.dumps(line), flush=True)
+
+
+def run_batched(args, local_rank):
+    """The batched workload: `--batch-instances` seeded nozzles (grids drawn
+    from 128x48 .. 1024x384, expansion 4-40, p0 10-100 bar, gamma 1.2/1.4,
+    altitude 0-30 km, all viscous) stepped by one SolverBatch (one launch per
+    kernel kind per step, 6-step periods replayed from a CUDA graph, tile shape
+    from the batch autotuner), against the same handles stepped one at a time
+    with rn_step. Both are device times from CUDA events; the batch's state
+    (~1 GB with geometry) is far larger than L2, so no flush is needed."""
+    import torch
+    rn = ge.load_package()
+    from rocket_nozzle_cfd_solver_b200 import configs
+    cfgs = configs.batched(args.batch_instances, seed=2024)
+    t0 = time.perf_counter()
+    setups = [rn.build_sim_setup(c) for c in cfgs]
+    t_setup = time.perf_counter() - t0
+    handles = []
+    for s in setups:
+        g = rn.GPUSolver(s.Nx, s.Nr)
+        g.setGeometry(s.geo)
+        init = s.initialState()
+        g.setState(init["A"], init["B"])
+        handles.append(g)
+    cells = sum(s.Nx * s.Nr for s in setups)
+    batch = rn.SolverBatch()
+    for g, s in zip(handles, setups):
+        batch.add(g, s.P)
+    tile = batch.autotune(steps=12)
+    stream = torch.cuda.ExternalStream(batch.stream())
+    nsteps = args.batch_steps
+    for _ in range(args.warmup):
+        batch.step(nsteps)
+    batch.sync()
+    l0 = batch.kernelLaunches()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            evs[k][0].record(stream)
+        batch.step(nsteps)
+        with torch.cuda.stream(stream):
+            evs[k][1].record(stream)
+    batch.sync()
+    launches = batch.kernelLaunches() - l0
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    value = cells * nsteps * args.steps / (ms * 1e-3)
+    # FP64 read-outs of every member after the batch run (thrust, mass flow)
+    F = [g.integrals(s) for g, s in zip(handles, setups)]
+    finite = all(math.isfinite(x["F"]) and math.isfinite(x["mdot"]) for x in F)
+    # the same handles one at a time (rn_step per instance, its own stream)
+    for g in handles:
+        batch.remove(g)
+    batch.close()
+    rounds = max(1, min(args.steps, 5))
+    p_list = [rn.params_from_P(s.P) for s in setups]
+    for g, p in zip(handles, p_list):
+        g.step(nsteps, p)
+    for g in handles:
+        g.sync()
+    single_ms = 0.0
+    t0 = time.perf_counter()
+    for _ in range(rounds):
+        for g, p in zip(handles, p_list):
+            st = torch.cuda.ExternalStream(g.stream())
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(st):
+                a.record(st)
+            g.step(nsteps, p)
+            with torch.cuda.stream(st):
+                b.record(st)
+            b.synchronize()
+            single_ms += a.elapsed_time(b)
+    single_wall = time.perf_counter() - t0
+    single = cells * nsteps * rounds / (single_ms * 1e-3)
+    for g in handles:
+        g.close()
+    sizes = {}
+    for s in setups:
+        sizes[f"{s.Nx}x{s.Nr}"] = sizes.get(f"{s.Nx}x{s.Nr}", 0) + 1
+    return {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "instances": len(setups),
+            "cells": cells, "grids": sizes, "solver_steps_per_bench_step": nsteps, "steps": args.steps,
+            "ms_per_step": ms / args.steps, "tile": tile, "gpu_launches": launches,
+            "launches_per_solver_step": launches / (nsteps * args.steps),
+            "one_at_a_time": {"value": single, "unit": "cell-updates/s", "wall_value":
+                              cells * nsteps * rounds / single_wall, "rounds": rounds},
+            "speedup_vs_one_at_a_time": value / single, "fp64_readouts_finite": finite,
+            "setup_s": t_setup, "l2": "state ~1 GB > L2: no flush"}
 
 
 def main():
@@ -311,6 +403,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--batch-instances", type=int, default=64,
+                    help="instances of the batched workload measured after the main line's (0: skip)")
+    ap.add_argument("--batch-steps", type=int, default=30, help="time steps per batched bench step")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -163,6 +163,48 @@ int rn_kernel_launches(rn_handle h, long long* out);
 int rn_set_precision(rn_handle h, int mode);
 int rn_get_precision(rn_handle h, int* mode);
 
+/* Tile shape of the stage/physics kernels (one thread per cell):
+ * RN_TILE_16x16 (default) or RN_TILE_16x8. rn_autotune times `steps` steps
+ * with each shape on a copy of the handle's current state (the state, step
+ * info and spray ring are restored afterwards), keeps the fastest and returns
+ * it in *chosen. No reference counterpart (the reference draws full-screen
+ * fragment passes). */
+#define RN_TILE_16x16 0
+#define RN_TILE_16x8 1
+int rn_set_tile(rn_handle h, int shape);
+int rn_get_tile(rn_handle h, int* shape);
+int rn_autotune(rn_handle h, const rn_params* P, int steps, int* chosen);
+
+/* Batched stepping (no reference counterpart; the reference runs one grid
+ * per page). A batch steps many solver handles of uneven grid sizes with one
+ * launch per kernel kind per step: every tile of every member is a block of
+ * the same grid. Members must share the physics flags (visc, chem, inj) and
+ * the precision; each keeps its own state, geometry, dt and parameter block.
+ * rn_batch_step captures the periodic 6-step launch sequence in a CUDA graph
+ * and replays it. While in a batch a handle must not be stepped on its own;
+ * all other handle calls (reads, integrals) work between batch steps.
+ * Removing a member leaves its handle where the batch left it. */
+typedef struct rn_batch_t* rn_batch;
+int rn_batch_create(rn_batch* out);
+int rn_batch_destroy(rn_batch b);
+/* adds h with parameter block P; *slot receives its index in the batch */
+int rn_batch_add(rn_batch b, rn_handle h, const rn_params* P, int* slot);
+int rn_batch_remove(rn_batch b, rn_handle h);
+int rn_batch_set_params(rn_batch b, rn_handle h, const rn_params* P);
+int rn_batch_size(rn_batch b, int* members, long long* cells);
+int rn_batch_step(rn_batch b, int n);
+int rn_batch_sync(rn_batch b);
+/* tile shape of the batch's launches (RN_TILE_*) */
+int rn_batch_set_tile(rn_batch b, int shape);
+/* times `steps` batch steps with each tile shape on copies of the members'
+ * current states (states, step info and spray rings are restored), keeps the
+ * fastest and returns it in *chosen */
+int rn_batch_autotune(rn_batch b, int steps, int* chosen);
+/* the batch's CUDA stream (a cudaStream_t) */
+int rn_batch_stream(rn_batch b, void** stream);
+/* number of kernels the batch has launched (graph replays included) */
+int rn_batch_kernel_launches(rn_batch b, long long* out);
+
 /* the handle's CUDA stream (a cudaStream_t), so a caller can order its own
  * work (timing events, cache flushes) with the handle's kernels */
 int rn_get_stream(rn_handle h, void** stream);

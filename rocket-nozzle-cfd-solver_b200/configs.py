@@ -63,3 +63,30 @@ def preset(key, Nx, aspect=0.28):
     if "inj" in e:
         cfg.update(e["inj"])
     return cfg
+
+
+BATCH_SIZES = ((128, 48), (256, 96), (512, 192), (1024, 384))
+
+
+def batched_instance(rng, size=None):
+    """One nozzle of the batched workload: grid uniform over BATCH_SIZES,
+    expansion ratio uniform 4-40, p0 log-uniform 10-100 bar, gamma 1.2 or 1.4,
+    altitude uniform 0-30 km; viscous with the afterburning scalars (every
+    instance has the same physics flags, so all share one batch)."""
+    Nx, Nr = size if size is not None else BATCH_SIZES[int(rng.integers(len(BATCH_SIZES)))]
+    eps = float(rng.uniform(4.0, 40.0))
+    Pc = float(10.0 ** rng.uniform(1.0, 2.0)) * 1e5
+    gamma = (1.2, 1.4)[int(rng.integers(2))]
+    alt = float(rng.uniform(0.0, 30.0)) * 1000.0
+    Dt = 0.030
+    cfg = dict(BASE, prop="methalox", Dt=Dt, De=Dt * math.sqrt(eps), type="bell", bellPct=80, coneAngle=15,
+               CR=5, chamberLen=1.5, Pc=Pc, Tc=3500.0, gamma=gamma, Mw=20.5, alt=alt, domainL=1.2,
+               Nx=Nx, aspect=Nr / Nx, cfl=0.6, viscous=True, afterburn=True, qAb=3.0, sAir=0.8)
+    return cfg
+
+
+def batched(count=64, seed=2024):
+    """The batched workload: `count` seeded instances (batched_instance)."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    return [batched_instance(rng) for _ in range(count)]

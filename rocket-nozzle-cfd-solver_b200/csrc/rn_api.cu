@@ -17,7 +17,7 @@
 #include <algorithm>
 #include <vector>
 #include "rn.h"
-#include "rn_kernels.cuh"
+#include "rn_internal.h"
 
 using namespace rn;
 
@@ -42,52 +42,9 @@ constexpr int SPRAY_N = 65536;
 
 }  // namespace
 
-// Shared with rn_static.cu so its errors also reach rn_last_error().
+// Shared with rn_static.cu and rn_batch.cu so their errors also reach rn_last_error().
 int rn_record_error(int code, const std::string& msg) { return fail(code, msg); }
-
-struct rn_solver {
-  int Nx = 0, Nr = 0, device = 0;
-  cudaStream_t stream = nullptr;
-  float4* SA[3] = {nullptr, nullptr, nullptr};
-  float4* SB[3] = {nullptr, nullptr, nullptr};
-  int cur = 0;
-  float4 *geoA = nullptr, *geoG = nullptr, *geoM = nullptr, *jw = nullptr, *wallRow = nullptr;
-  uint8_t* mask = nullptr;
-  float4* stepTex = nullptr;      // [2]
-  unsigned* wmax = nullptr;       // [2]
-  int stepIdx = 0, wslot = 0;
-  bool wvalid = false;
-  long long stepCount = 0, launches = 0;
-  // spray
-  float4 *PA[2] = {nullptr, nullptr}, *PB[2] = {nullptr, nullptr}, *PC[2] = {nullptr, nullptr};
-  float4 *src = nullptr, *tab = nullptr, *dep = nullptr;
-  unsigned *key = nullptr, *val = nullptr, *keyS = nullptr, *valS = nullptr;
-  void* sortTemp = nullptr;
-  size_t sortTempBytes = 0;
-  int scur = 0;
-  uint32_t head = 0, seed = 1;
-  // asynchronous read-back
-  float* pinned = nullptr;
-  size_t pinnedCap = 0, asyncFloats = 0;
-  cudaEvent_t asyncEv = nullptr;
-  bool asyncBusy = false;
-  int asyncTag = 0;
-  double* dInt = nullptr;
-  // per-kernel event timing
-  bool prof = false;
-  std::vector<cudaEvent_t> evPool;
-  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> evPending;
-  double profMs[RN_NKERNELS] = {0};
-  long long profN[RN_NKERNELS] = {0};
-  // per tile of the stage/physics kernels: out-of-tile members of its groups
-  int* xoff = nullptr;
-  int* xcell = nullptr;
-  int maxX = 1;
-  // kernels of the selected precision (rn_set_precision)
-  const KernelSet* K = &kernels_fast;
-
-  Grid grid() const { return Grid{Nx, Nr, mask, geoA, geoG, geoM}; }
-};
+int rn_record_cuda(cudaError_t e, const char* what) { return cuda_fail(e, what); }
 
 namespace {
 
@@ -171,23 +128,26 @@ int alloc_buffers(rn_solver* h, int Nx, int Nr) {
   CK(cudaMalloc(&h->sortTemp, h->sortTempBytes > 0 ? h->sortTempBytes : 16));
   h->cur = 0; h->stepIdx = 0; h->wslot = 0; h->wvalid = false; h->stepCount = 0;
   h->seed = 1;
-  // empty per-tile member lists until a geometry is set
-  const int nT = ((Nx + TX - 1) / TX) * ((Nr + TY - 1) / TY);
-  CK(cudaMalloc(&h->xoff, sizeof(int) * (nT + 1)));
-  CK(cudaMemsetAsync(h->xoff, 0, sizeof(int) * (nT + 1), h->stream));
-  CK(cudaMalloc(&h->xcell, sizeof(int)));
-  CK(cudaMemsetAsync(h->xcell, 0, sizeof(int), h->stream));
-  h->maxX = 1;
+  // empty topology (no groups) until a geometry is set
+  h->hostMask.assign(N, 0);
+  h->hostGeoM.assign(N * 4, 0.0f);
+  int rc = rn_build_member_lists(h);
+  if (rc != RN_OK) return rc;
   return spray_reset_dev(h);
 }
 
-constexpr int MAXX_CAP = MAXX;   // out-of-tile group members one tile may list
+bool valid(rn_solver* h) { return h != nullptr && h->SA[0] != nullptr; }
+
+}  // namespace
 
 // Per tile, the cells outside it that belong to a cut-cell group with a cell
 // inside it (a sliver merged across the tile edge). Groups are a host plus the
 // slaves of its slave mask (geoM.z bits 1/2/4/8, cutcell.js:168-174).
-int build_member_lists(rn_solver* h, const uint8_t* mask, const float* geoM) {
+int rn_build_member_lists(rn_solver* h) {
+  const int TX = TILE_TX[h->tile], TY = TILE_TY[h->tile];
   const int Nx = h->Nx, Nr = h->Nr, tx = (Nx + TX - 1) / TX, nT = tx * ((Nr + TY - 1) / TY);
+  const uint8_t* mask = h->hostMask.data();
+  const float* geoM = h->hostGeoM.data();
   std::vector<std::vector<int>> lists(nT);
   auto tile_of = [&](int k) { return ((k / Nx) / TY) * tx + (k % Nx) / TX; };
   for (int k = 0; k < Nx * Nr; k++) {
@@ -218,12 +178,15 @@ int build_member_lists(rn_solver* h, const uint8_t* mask, const float* geoM) {
     maxX = std::max(maxX, int(lists[t].size()));
     cells.insert(cells.end(), lists[t].begin(), lists[t].end());
   }
-  if (maxX > MAXX_CAP)
+  if (maxX > MAXX)
     return fail(RN_ERR_ARG, "rn_set_geometry: a tile has " + std::to_string(maxX) + " out-of-tile group members (limit " +
-                                std::to_string(MAXX_CAP) + ")");
+                                std::to_string(MAXX) + ")");
   if (cells.empty()) cells.push_back(0);
+  CK(cudaStreamSynchronize(h->stream));
+  cudaFree(h->xoff);
   cudaFree(h->xcell);
-  h->xcell = nullptr;
+  h->xoff = h->xcell = nullptr;
+  CK(cudaMalloc(&h->xoff, sizeof(int) * (nT + 1)));
   CK(cudaMalloc(&h->xcell, sizeof(int) * cells.size()));
   CK(cudaMemcpyAsync(h->xoff, off.data(), sizeof(int) * (nT + 1), cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync(h->xcell, cells.data(), sizeof(int) * cells.size(), cudaMemcpyHostToDevice, h->stream));
@@ -232,7 +195,7 @@ int build_member_lists(rn_solver* h, const uint8_t* mask, const float* geoM) {
   return RN_OK;
 }
 
-bool valid(rn_solver* h) { return h != nullptr && h->SA[0] != nullptr; }
+namespace {
 
 cudaEvent_t prof_event(rn_solver* h) {
   if (!h->evPool.empty()) {
@@ -265,6 +228,22 @@ struct ProfScope {
 };
 
 }  // namespace
+
+// The CFL wave speed of the current state into wmax[wslot] (the value the
+// previous step's last kernel would have left there).
+int rn_ensure_wave_speed(rn_solver* h) {
+  if (h->wvalid) return RN_OK;
+  unsigned* w = h->wmax + h->wslot;
+  CK(cudaMemsetAsync(w, 0, sizeof(unsigned), h->stream));
+  {
+    ProfScope ps(h, RN_K_REDUCE);
+    h->K->reduce(h->grid(), h->SA[h->cur], h->SB[h->cur], w, h->stream);
+  }
+  h->launches++;
+  h->wvalid = true;
+  CK(cudaGetLastError());
+  return RN_OK;
+}
 
 extern "C" {
 
@@ -307,6 +286,7 @@ int rn_create(int Nx, int Nr, rn_handle* out) {
 
 int rn_destroy(rn_handle h) {
   if (!h) return RN_OK;
+  rn_batch_detach(h);
   cudaStreamSynchronize(h->stream);
   free_buffers(h);
   if (h->pinned) cudaFreeHost(h->pinned);
@@ -353,11 +333,22 @@ int rn_set_geometry(rn_handle h, const uint8_t* mask, const float* geoA, const f
     if (((sm & 1) && i == 0) || ((sm & 2) && i == Nx - 1) || ((sm & 4) && j == 0) || ((sm & 8) && j == Nr - 1))
       return fail(RN_ERR_ARG, "rn_set_geometry: slave bit of cell " + std::to_string(k) + " points outside the grid");
   }
-  int rc = build_member_lists(h, mask, geoM);
-  if (rc != RN_OK) return rc;
+  const size_t N = size_t(Nx) * Nr, NF = size_t(Nx + 1) * (Nr + 1);
+  std::vector<uint8_t> oldMask = std::move(h->hostMask);
+  std::vector<float> oldGeoM = std::move(h->hostGeoM);
+  h->hostMask.resize(N);
+  for (size_t k = 0; k < N; k++) h->hostMask[k] = mask[k] ? 1 : 0;
+  h->hostGeoM.assign(geoM, geoM + 4 * N);
+  int rc = rn_build_member_lists(h);
+  if (rc != RN_OK) {
+    std::string msg = g_err;
+    h->hostMask = std::move(oldMask);
+    h->hostGeoM = std::move(oldGeoM);
+    rn_build_member_lists(h);
+    return fail(rc, msg);
+  }
   rc = rn_set_mask(h, mask);
   if (rc != RN_OK) return rc;
-  const size_t N = size_t(Nx) * Nr, NF = size_t(Nx + 1) * (Nr + 1);
   CK(cudaMemcpyAsync(h->geoA, geoA, sizeof(float4) * NF, cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync(h->geoG, geoG, sizeof(float4) * N, cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync(h->geoM, geoM, sizeof(float4) * N, cudaMemcpyHostToDevice, h->stream));
@@ -389,6 +380,7 @@ int rn_get_state(rn_handle h, float* A, float* B) {
 
 int rn_step(rn_handle h, int n, const rn_params* P) {
   if (!valid(h) || !P || n < 0) return fail(RN_ERR_ARG, "rn_step: bad argument");
+  if (h->batch) return fail(RN_ERR_STATE, "rn_step: the handle is stepped by a batch");
   const Grid g = h->grid();
   const bool phys = P->visc || P->chem, inj = P->inj != 0;
   for (int k = 0; k < n; k++) {
@@ -396,10 +388,8 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
     unsigned* wIn = h->wmax + h->wslot;
     unsigned* wOut = h->wmax + (1 - h->wslot);
     if (!h->wvalid) {
-      CK(cudaMemsetAsync(wIn, 0, sizeof(unsigned), h->stream));
-      ProfScope ps(h, RN_K_REDUCE);
-      h->K->reduce(g, h->SA[s0], h->SB[s0], wIn, h->stream);
-      h->launches++;
+      int rc = rn_ensure_wave_speed(h);
+      if (rc != RN_OK) return rc;
     }
     float4* stPrev = h->stepTex + h->stepIdx;
     float4* stNew = h->stepTex + (1 - h->stepIdx);
@@ -412,7 +402,7 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
     a.xoff = h->xoff; a.xcell = h->xcell; a.maxX = h->maxX;
     {
       ProfScope ps(h, RN_K_STAGE1);
-      h->K->stage1(a, *P, h->stream);
+      h->K->stage1(a, *P, h->tile, h->stream);
     }
     h->launches++;
     if (inj) {
@@ -436,7 +426,7 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
     b.finalCfl = (!phys && !inj) ? 1 : 0;
     {
       ProfScope ps(h, RN_K_STAGE2);
-      h->K->stage2(b, *P, h->stream);
+      h->K->stage2(b, *P, h->tile, h->stream);
     }
     h->launches++;
     h->cur = s2;
@@ -449,7 +439,7 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
       p.xoff = h->xoff; p.xcell = h->xcell; p.maxX = h->maxX;
       {
         ProfScope ps(h, RN_K_PHYSICS);
-        h->K->physics(p, *P, h->stream);
+        h->K->physics(p, *P, h->tile, h->stream);
       }
       h->launches++;
       h->cur = s0;
@@ -660,6 +650,97 @@ int rn_set_precision(rn_handle h, int mode) {
   if (!h || (mode != RN_PRECISION_FAST && mode != RN_PRECISION_EXACT))
     return fail(RN_ERR_ARG, "rn_set_precision: bad handle or mode");
   h->K = mode == RN_PRECISION_EXACT ? &kernels_exact : &kernels_fast;
+  return RN_OK;
+}
+
+int rn_set_tile(rn_handle h, int shape) {
+  if (!valid(h) || shape < 0 || shape >= NTILES) return fail(RN_ERR_ARG, "rn_set_tile: bad handle or shape");
+  if (h->batch) return fail(RN_ERR_STATE, "rn_set_tile: the handle is in a batch");
+  if (shape == h->tile) return RN_OK;
+  const int old = h->tile;
+  h->tile = shape;
+  int rc = rn_build_member_lists(h);
+  if (rc != RN_OK) {
+    std::string msg = g_err;
+    h->tile = old;
+    rn_build_member_lists(h);
+    return fail(rc, msg);
+  }
+  return RN_OK;
+}
+
+int rn_get_tile(rn_handle h, int* shape) {
+  if (!h || !shape) return fail(RN_ERR_ARG, "rn_get_tile: bad argument");
+  *shape = h->tile;
+  return RN_OK;
+}
+
+int rn_autotune(rn_handle h, const rn_params* P, int steps, int* chosen) {
+  if (!valid(h) || !P || steps < 1) return fail(RN_ERR_ARG, "rn_autotune: bad argument");
+  if (h->batch) return fail(RN_ERR_STATE, "rn_autotune: the handle is in a batch");
+  // save everything a step changes
+  const size_t N = size_t(h->Nx) * h->Nr;
+  const size_t stateBytes = sizeof(float4) * N * 6, sprayBytes = sizeof(float4) * SPRAY_N * 6;
+  char* save = nullptr;
+  CK(cudaMalloc(&save, stateBytes + sprayBytes + sizeof(float4) * 2 + sizeof(unsigned) * 2));
+  auto copy_all = [&](bool toSave) -> cudaError_t {
+    char* p = save;
+    cudaError_t e;
+    const cudaMemcpyKind k = cudaMemcpyDeviceToDevice;
+    e = toSave ? cudaMemcpyAsync(p, h->SA[0], stateBytes, k, h->stream) : cudaMemcpyAsync(h->SA[0], p, stateBytes, k, h->stream);
+    if (e != cudaSuccess) return e;
+    p += stateBytes;
+    e = toSave ? cudaMemcpyAsync(p, h->PA[0], sprayBytes, k, h->stream) : cudaMemcpyAsync(h->PA[0], p, sprayBytes, k, h->stream);
+    if (e != cudaSuccess) return e;
+    p += sprayBytes;
+    e = toSave ? cudaMemcpyAsync(p, h->stepTex, sizeof(float4) * 2, k, h->stream)
+               : cudaMemcpyAsync(h->stepTex, p, sizeof(float4) * 2, k, h->stream);
+    if (e != cudaSuccess) return e;
+    p += sizeof(float4) * 2;
+    return toSave ? cudaMemcpyAsync(p, h->wmax, sizeof(unsigned) * 2, k, h->stream)
+                  : cudaMemcpyAsync(h->wmax, p, sizeof(unsigned) * 2, k, h->stream);
+  };
+  const int cur = h->cur, stepIdx = h->stepIdx, wslot = h->wslot, scur = h->scur;
+  const bool wvalid = h->wvalid;
+  const long long stepCount = h->stepCount, launches = h->launches;
+  const uint32_t head = h->head, seed = h->seed;
+  const bool prof = h->prof;
+  h->prof = false;
+  cudaError_t e = copy_all(true);
+  int best = h->tile, rc = RN_OK;
+  float bestMs = 1e30f;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  for (int shape = 0; shape < NTILES && e == cudaSuccess && rc == RN_OK; shape++) {
+    h->tile = shape;
+    rc = rn_build_member_lists(h);
+    if (rc != RN_OK) { rc = RN_OK; continue; }          // this shape cannot hold the geometry's lists
+    rc = rn_step(h, 2, P);                                // warm-up
+    if (rc == RN_OK) e = cudaEventRecord(e0, h->stream);
+    if (rc == RN_OK && e == cudaSuccess) rc = rn_step(h, steps, P);
+    if (rc == RN_OK && e == cudaSuccess) e = cudaEventRecord(e1, h->stream);
+    float ms = 0.0f;
+    if (rc == RN_OK && e == cudaSuccess) e = cudaEventSynchronize(e1);
+    if (rc == RN_OK && e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (rc == RN_OK && e == cudaSuccess && ms < bestMs) { bestMs = ms; best = shape; }
+    // restore the state the trial advanced
+    if (e == cudaSuccess) e = copy_all(false);
+    h->cur = cur; h->stepIdx = stepIdx; h->wslot = wslot; h->scur = scur; h->wvalid = wvalid;
+    h->stepCount = stepCount; h->head = head; h->seed = seed;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaStreamSynchronize(h->stream);
+  cudaFree(save);
+  h->launches = launches;
+  h->prof = prof;
+  h->tile = best;
+  int rc2 = rn_build_member_lists(h);
+  if (e != cudaSuccess) return cuda_fail(e, "rn_autotune");
+  if (rc != RN_OK) return rc;
+  if (rc2 != RN_OK) return rc2;
+  if (chosen) *chosen = best;
   return RN_OK;
 }
 

@@ -1,0 +1,609 @@
+// rn_batch.cu -- batched stepping of many solver handles (declared in rn.h).
+//
+// No reference counterpart: the reference runs one grid per browser page
+// (solver.js:849-891 steps it). A batch is the serving form of the same step:
+// every tile of every member is one block of a single 1-D launch per kernel
+// kind, so small grids share the 148 SMs instead of each leaving most of them
+// idle, and a step of the whole batch costs 2-3 launches instead of 2-3 per
+// member.
+//
+// Each block finds its member in a block->member table and that member's
+// descriptor (BatchInst: buffers, ring position, parameter block) in a device
+// array. The descriptor's ring position is normalised to the batch's step
+// counter, so it stays the same from call to call while the members are only
+// stepped by the batch, and the launch sequence repeats with a period of 6
+// steps (3 ring shifts x 2 step-info parities). Without sprays that period is
+// captured once in a CUDA graph and replayed.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "rn.h"
+#include "rn_internal.h"
+
+using namespace rn;
+
+namespace {
+constexpr int PERIOD = 6;
+constexpr int SPRAY_N = 65536;
+
+struct Flags {
+  int visc = 0, chem = 0, inj = 0;
+  bool phys() const { return visc || chem; }
+  // how far the state ring turns per step (rn_step's slot bookkeeping):
+  // 2 kernels write s1 then s2; physics writes s0 back; the spray apply
+  // writes the slot after the current one
+  int delta() const {
+    int d = 2;
+    if (phys()) d = 0;
+    if (inj) d = (d + 1) % 3;
+    return d;
+  }
+  bool operator==(const Flags& o) const { return visc == o.visc && chem == o.chem && inj == o.inj; }
+};
+Flags flags_of(const rn_params& P) {
+  Flags f;
+  f.visc = P.visc != 0;
+  f.chem = P.chem != 0;
+  f.inj = P.inj != 0;
+  return f;
+}
+}  // namespace
+
+struct rn_batch_t {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t done = nullptr;           // end of the last rn_batch_step
+  cudaEvent_t staged = nullptr;         // the last descriptor upload has read the pinned buffer
+  int tile = 0;
+  Flags flags;
+  std::vector<rn_solver*> members;
+  std::vector<rn_params> params;
+  std::vector<cudaEvent_t> fence;       // per member: its stream's work before a batch step
+  int ctr = 0;                          // steps since the descriptors were normalised, mod PERIOD
+  // device tables and their host images
+  BatchInst* dInst = nullptr;
+  size_t instCap = 0;
+  int* dBlock = nullptr;
+  size_t blockCap = 0;
+  BatchInst* hInst = nullptr;           // pinned staging
+  size_t hInstCap = 0;
+  std::vector<BatchInst> uploaded;      // what dInst holds
+  std::vector<int> layout;              // (Nx, Nr) per member the block table was built for
+  int nblocks = 0, maxX = 1;
+  const KernelSet* K = nullptr;
+  // the graph of one period
+  cudaGraphExec_t graph = nullptr;
+  const KernelSet* graphK = nullptr;
+  int graphBlocks = -1, graphTile = -1, graphMaxX = -1;
+  Flags graphFlags;
+  long long launches = 0;
+};
+
+namespace {
+
+int bfail(int code, const std::string& msg) { return rn_record_error(code, msg); }
+#define BCK(call)                                             \
+  do {                                                        \
+    cudaError_t e_ = (call);                                  \
+    if (e_ != cudaSuccess) return rn_record_cuda(e_, #call);  \
+  } while (0)
+
+void drop_graph(rn_batch_t* b) {
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  b->graph = nullptr;
+  b->graphK = nullptr;
+  b->graphBlocks = b->graphTile = b->graphMaxX = -1;
+}
+
+int index_of(const rn_batch_t* b, const rn_solver* h) {
+  for (size_t m = 0; m < b->members.size(); m++)
+    if (b->members[m] == h) return int(m);
+  return -1;
+}
+
+// Normalised ring position of member h at batch step counter ctr: the kernels
+// of batch step c use slot (cur0 + c*delta) % 3 and parity stepIdx0 ^ (c & 1).
+void normalise(const rn_batch_t* b, const rn_solver* h, int& cur0, int& si0, int& ws0) {
+  const int sh = (b->ctr * b->flags.delta()) % 3, par = b->ctr & 1;
+  cur0 = (h->cur - sh + 3) % 3;
+  si0 = h->stepIdx ^ par;
+  ws0 = h->wslot ^ par;
+}
+
+// Brings the block table, the descriptors on the device and the members'
+// member lists up to date with the handles.
+int refresh(rn_batch_t* b) {
+  const int nm = int(b->members.size());
+  const int TX = TILE_TX[b->tile], TY = TILE_TY[b->tile];
+  // block table: rebuilt when a member's grid size changed
+  std::vector<int> layout(2 * nm);
+  for (int m = 0; m < nm; m++) {
+    layout[2 * m] = b->members[m]->Nx;
+    layout[2 * m + 1] = b->members[m]->Nr;
+  }
+  std::vector<int> first(nm), tilesX(nm);
+  int nb = 0;
+  for (int m = 0; m < nm; m++) {
+    first[m] = nb;
+    tilesX[m] = (layout[2 * m] + TX - 1) / TX;
+    nb += tilesX[m] * ((layout[2 * m + 1] + TY - 1) / TY);
+  }
+  if (layout != b->layout || nb != b->nblocks) {
+    std::vector<int> table(std::max(nb, 1), 0);
+    for (int m = 0; m < nm; m++)
+      for (int q = first[m]; q < (m + 1 < nm ? first[m + 1] : nb); q++) table[q] = m;
+    BCK(cudaStreamSynchronize(b->stream));
+    if (size_t(nb) > b->blockCap) {
+      cudaFree(b->dBlock);
+      b->dBlock = nullptr;
+      b->blockCap = 0;
+      BCK(cudaMalloc(&b->dBlock, sizeof(int) * size_t(nb)));
+      b->blockCap = size_t(nb);
+    }
+    BCK(cudaMemcpy(b->dBlock, table.data(), sizeof(int) * table.size(), cudaMemcpyHostToDevice));
+    b->layout = layout;
+    b->nblocks = nb;
+  }
+  // descriptors: uploaded when one differs from what the device holds
+  std::vector<BatchInst> inst(nm);
+  int maxX = 1;
+  for (int m = 0; m < nm; m++) {
+    const rn_solver* h = b->members[m];
+    BatchInst& d = inst[m];
+    std::memset(&d, 0, sizeof(d));
+    d.g = h->grid();
+    for (int s = 0; s < 3; s++) {
+      d.SA[s] = h->SA[s];
+      d.SB[s] = h->SB[s];
+    }
+    d.stepTex = h->stepTex;
+    d.wmax = h->wmax;
+    d.xoff = h->xoff;
+    d.xcell = h->xcell;
+    normalise(b, h, d.cur0, d.stepIdx0, d.wslot0);
+    d.firstBlock = first[m];
+    d.tilesX = tilesX[m];
+    d.P = b->params[m];
+    maxX = std::max(maxX, h->maxX);
+  }
+  b->maxX = maxX;
+  const bool same = inst.size() == b->uploaded.size() &&
+                    (inst.empty() || std::memcmp(inst.data(), b->uploaded.data(), sizeof(BatchInst) * inst.size()) == 0);
+  if (!same && nm > 0) {
+    if (size_t(nm) > b->instCap) {
+      BCK(cudaStreamSynchronize(b->stream));
+      cudaFree(b->dInst);
+      b->dInst = nullptr;
+      b->instCap = 0;
+      BCK(cudaMalloc(&b->dInst, sizeof(BatchInst) * size_t(nm)));
+      b->instCap = size_t(nm);
+      drop_graph(b);
+    }
+    if (size_t(nm) > b->hInstCap) {
+      BCK(cudaEventSynchronize(b->staged));
+      cudaFreeHost(b->hInst);
+      b->hInst = nullptr;
+      b->hInstCap = 0;
+      BCK(cudaHostAlloc(reinterpret_cast<void**>(&b->hInst), sizeof(BatchInst) * size_t(nm), cudaHostAllocDefault));
+      b->hInstCap = size_t(nm);
+    }
+    // the previous upload must have left the pinned buffer before it is reused
+    BCK(cudaEventSynchronize(b->staged));
+    std::memcpy(b->hInst, inst.data(), sizeof(BatchInst) * size_t(nm));
+    BCK(cudaMemcpyAsync(b->dInst, b->hInst, sizeof(BatchInst) * size_t(nm), cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaEventRecord(b->staged, b->stream));
+    b->uploaded = inst;
+  }
+  return RN_OK;
+}
+
+// The launches of batch step c (counter value at the step) on the batch stream.
+// With sprays, the per-member parcel and apply launches go between them.
+int launch_step(rn_batch_t* b, int c, bool withSpray) {
+  const Flags f = b->flags;
+  const int delta = f.delta();
+  BatchPhase ph;
+  ph.shift = (c * delta) % 3;
+  ph.par = c & 1;
+  ph.maxX = b->maxX;
+  const int nb = b->nblocks;
+  ph.finalCfl = 0;
+  b->K->batchStage1(b->dInst, b->dBlock, nb, ph, b->tile, b->stream);
+  b->launches++;
+  if (f.inj && withSpray) {
+    // GPUSpray.step between the two stages (solver.js:865-871), per member
+    for (size_t m = 0; m < b->members.size(); m++) {
+      rn_solver* h = b->members[m];
+      const BatchInst& d = b->uploaded[m];
+      const int s0 = (d.cur0 + ph.shift) % 3, s1 = (s0 + 1) % 3;
+      const int si = d.stepIdx0 ^ ph.par;
+      SprayArgs sp;
+      sp.g = h->grid();
+      sp.A1 = h->SA[s1]; sp.B1 = h->SB[s1];
+      sp.PA = h->PA[h->scur]; sp.PB = h->PB[h->scur];
+      sp.oPA = h->PA[1 - h->scur]; sp.oPB = h->PB[1 - h->scur]; sp.oPC = h->PC[1 - h->scur];
+      sp.tab = h->tab; sp.st = h->stepTex + (1 - si);
+      sp.key = h->key; sp.val = h->val; sp.dep = h->dep;
+      sp.head = int(h->head); sp.seed = int(h->seed);
+      int launched = 0;
+      if (b->K->spray(sp, b->params[m], h->sortTemp, h->sortTempBytes, h->keyS, h->valS, h->src, b->stream,
+                      &launched) != 0)
+        return bfail(RN_ERR_CUDA, "rn_batch_step: deposit sort failed");
+      b->launches += launched;
+    }
+  }
+  ph.finalCfl = (!f.phys() && !f.inj) ? 1 : 0;
+  b->K->batchStage2(b->dInst, b->dBlock, nb, ph, b->tile, b->stream);
+  b->launches++;
+  if (f.phys()) {
+    ph.finalCfl = f.inj ? 0 : 1;
+    b->K->batchPhysics(b->dInst, b->dBlock, nb, ph, b->tile, b->stream);
+    b->launches++;
+  }
+  if (f.inj && withSpray) {
+    for (size_t m = 0; m < b->members.size(); m++) {
+      rn_solver* h = b->members[m];
+      const BatchInst& d = b->uploaded[m];
+      const int s0 = (d.cur0 + ph.shift) % 3;
+      const int cur = f.phys() ? s0 : (s0 + 2) % 3, out = (cur + 1) % 3;
+      const int ws = d.wslot0 ^ ph.par;
+      ApplyArgs ap;
+      ap.g = h->grid();
+      ap.A = h->SA[cur]; ap.B = h->SB[cur]; ap.src = h->src;
+      ap.oA = h->SA[out]; ap.oB = h->SB[out];
+      ap.wOut = h->wmax + (1 - ws);
+      ap.finalCfl = 1;
+      b->K->apply(ap, b->params[m], b->stream);
+      b->launches++;
+      h->scur = 1 - h->scur;
+      h->head = (h->head + 4) % SPRAY_N;
+      h->seed = h->seed + 1u;
+    }
+  }
+  return RN_OK;
+}
+
+int build_graph(rn_batch_t* b) {
+  drop_graph(b);
+  cudaGraph_t g = nullptr;
+  BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  const long long before = b->launches;
+  int rc = RN_OK;
+  for (int c = 0; c < PERIOD && rc == RN_OK; c++) rc = launch_step(b, c, false);
+  cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+  b->launches = before;   // capturing launches nothing
+  if (rc != RN_OK) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return rn_record_cuda(e, "cudaStreamEndCapture");
+  e = cudaGraphInstantiate(&b->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    b->graph = nullptr;
+    return rn_record_cuda(e, "cudaGraphInstantiate");
+  }
+  b->graphK = b->K;
+  b->graphBlocks = b->nblocks;
+  b->graphTile = b->tile;
+  b->graphMaxX = b->maxX;
+  b->graphFlags = b->flags;
+  return RN_OK;
+}
+
+int launches_per_step(const rn_batch_t* b) { return 2 + (b->flags.phys() ? 1 : 0); }
+
+}  // namespace
+
+// Removes h from its batch (rn_destroy of a member).
+void rn_batch_detach(rn_solver* h) {
+  if (h && h->batch) rn_batch_remove(h->batch, h);
+}
+
+extern "C" {
+
+int rn_batch_create(rn_batch* out) {
+  if (!out) return bfail(RN_ERR_ARG, "rn_batch_create: out is NULL");
+  *out = nullptr;
+  rn_batch_t* b = new rn_batch_t();
+  cudaError_t e = cudaGetDevice(&b->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->staged, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    if (b->staged) cudaEventDestroy(b->staged);
+    if (b->done) cudaEventDestroy(b->done);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return rn_record_cuda(e, "rn_batch_create");
+  }
+  *out = b;
+  return RN_OK;
+}
+
+int rn_batch_destroy(rn_batch b) {
+  if (!b) return bfail(RN_ERR_ARG, "rn_batch_destroy: NULL batch");
+  cudaStreamSynchronize(b->stream);
+  for (rn_solver* h : b->members) h->batch = nullptr;
+  for (cudaEvent_t e : b->fence) cudaEventDestroy(e);
+  drop_graph(b);
+  cudaFree(b->dInst);
+  cudaFree(b->dBlock);
+  cudaFreeHost(b->hInst);
+  cudaEventDestroy(b->staged);
+  cudaEventDestroy(b->done);
+  cudaStreamDestroy(b->stream);
+  delete b;
+  return RN_OK;
+}
+
+int rn_batch_add(rn_batch b, rn_handle h, const rn_params* P, int* slot) {
+  if (!b || !h || !P || !h->SA[0]) return bfail(RN_ERR_ARG, "rn_batch_add: bad argument");
+  if (h->batch) return bfail(RN_ERR_STATE, "rn_batch_add: the handle is already in a batch");
+  if (h->device != b->device) return bfail(RN_ERR_ARG, "rn_batch_add: the handle is on another device");
+  const Flags f = flags_of(*P);
+  if (!b->members.empty()) {
+    if (!(f == b->flags)) return bfail(RN_ERR_ARG, "rn_batch_add: physics flags (visc, chem, inj) differ from the batch's");
+    if (h->K != b->members[0]->K) return bfail(RN_ERR_ARG, "rn_batch_add: precision differs from the batch's");
+  }
+  if (h->tile != b->tile) {
+    int rc = rn_set_tile(h, b->tile);
+    if (rc != RN_OK) return rc;
+  }
+  cudaEvent_t ev = nullptr;
+  BCK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  if (b->members.empty()) b->flags = f;
+  b->members.push_back(h);
+  b->params.push_back(*P);
+  b->fence.push_back(ev);
+  h->batch = b;
+  if (slot) *slot = int(b->members.size()) - 1;
+  return RN_OK;
+}
+
+int rn_batch_remove(rn_batch b, rn_handle h) {
+  if (!b || !h) return bfail(RN_ERR_ARG, "rn_batch_remove: bad argument");
+  const int m = index_of(b, h);
+  if (m < 0) return bfail(RN_ERR_ARG, "rn_batch_remove: the handle is not in this batch");
+  // the handle's later work waits for the batch's queued steps
+  cudaEventRecord(b->done, b->stream);
+  cudaStreamWaitEvent(h->stream, b->done, 0);
+  cudaEventDestroy(b->fence[m]);
+  b->members.erase(b->members.begin() + m);
+  b->params.erase(b->params.begin() + m);
+  b->fence.erase(b->fence.begin() + m);
+  h->batch = nullptr;
+  return RN_OK;
+}
+
+int rn_batch_set_params(rn_batch b, rn_handle h, const rn_params* P) {
+  if (!b || !h || !P) return bfail(RN_ERR_ARG, "rn_batch_set_params: bad argument");
+  const int m = index_of(b, h);
+  if (m < 0) return bfail(RN_ERR_ARG, "rn_batch_set_params: the handle is not in this batch");
+  if (!(flags_of(*P) == b->flags) && b->members.size() > 1)
+    return bfail(RN_ERR_ARG, "rn_batch_set_params: physics flags (visc, chem, inj) differ from the batch's");
+  if (b->members.size() == 1) b->flags = flags_of(*P);
+  b->params[m] = *P;
+  return RN_OK;
+}
+
+int rn_batch_size(rn_batch b, int* members, long long* cells) {
+  if (!b) return bfail(RN_ERR_ARG, "rn_batch_size: NULL batch");
+  long long c = 0;
+  for (const rn_solver* h : b->members) c += (long long)h->Nx * h->Nr;
+  if (members) *members = int(b->members.size());
+  if (cells) *cells = c;
+  return RN_OK;
+}
+
+int rn_batch_set_tile(rn_batch b, int shape) {
+  if (!b || shape < 0 || shape >= NTILES) return bfail(RN_ERR_ARG, "rn_batch_set_tile: bad argument");
+  if (shape == b->tile) return RN_OK;
+  BCK(cudaStreamSynchronize(b->stream));
+  const int old = b->tile;
+  for (size_t m = 0; m < b->members.size(); m++) {
+    rn_solver* h = b->members[m];
+    h->batch = nullptr;   // rn_set_tile refuses batch members
+    int rc = rn_set_tile(h, shape);
+    h->batch = b;
+    if (rc != RN_OK) {
+      std::string msg = rn_last_error();
+      for (size_t q = 0; q < m; q++) {
+        b->members[q]->batch = nullptr;
+        rn_set_tile(b->members[q], old);
+        b->members[q]->batch = b;
+      }
+      return bfail(rc, msg);
+    }
+  }
+  b->tile = shape;
+  b->layout.clear();   // block table and descriptors are rebuilt by the next step
+  b->uploaded.clear();
+  return RN_OK;
+}
+
+int rn_batch_step(rn_batch b, int n) {
+  if (!b || n < 0) return bfail(RN_ERR_ARG, "rn_batch_step: bad argument");
+  if (b->members.empty() || n == 0) return RN_OK;
+  const KernelSet* K = b->members[0]->K;
+  for (rn_solver* h : b->members) {
+    if (h->K != K) return bfail(RN_ERR_STATE, "rn_batch_step: members have different precisions");
+    if (h->tile != b->tile) return bfail(RN_ERR_STATE, "rn_batch_step: a member's tile shape differs from the batch's");
+    if (!h->SA[0]) return bfail(RN_ERR_STATE, "rn_batch_step: a member has no buffers");
+  }
+  b->K = K;
+  // each member's CFL wave speed of its current state, and its queued work,
+  // before the batch's kernels
+  for (size_t m = 0; m < b->members.size(); m++) {
+    rn_solver* h = b->members[m];
+    int rc = rn_ensure_wave_speed(h);
+    if (rc != RN_OK) return rc;
+    BCK(cudaEventRecord(b->fence[m], h->stream));
+    BCK(cudaStreamWaitEvent(b->stream, b->fence[m], 0));
+  }
+  int rc = refresh(b);
+  if (rc != RN_OK) return rc;
+  const Flags f = b->flags;
+  int done = 0;
+  if (f.inj) {
+    // parcel heads and seeds change every step: launched step by step
+    for (; done < n; done++) {
+      rc = launch_step(b, b->ctr, true);
+      if (rc != RN_OK) return rc;
+      b->ctr = (b->ctr + 1) % PERIOD;
+    }
+  } else {
+    // up to the start of a period step by step, whole periods from the graph
+    while (done < n && b->ctr != 0) {
+      launch_step(b, b->ctr, false);
+      b->ctr = (b->ctr + 1) % PERIOD;
+      done++;
+    }
+    if (n - done >= PERIOD) {
+      if (!b->graph || b->graphK != b->K || b->graphBlocks != b->nblocks || b->graphTile != b->tile ||
+          b->graphMaxX != b->maxX || !(b->graphFlags == f)) {
+        rc = build_graph(b);
+        if (rc != RN_OK) return rc;
+      }
+      while (n - done >= PERIOD) {
+        BCK(cudaGraphLaunch(b->graph, b->stream));
+        b->launches += PERIOD * launches_per_step(b);
+        done += PERIOD;
+      }
+    }
+    for (; done < n; done++) {
+      launch_step(b, b->ctr, false);
+      b->ctr = (b->ctr + 1) % PERIOD;
+    }
+  }
+  BCK(cudaGetLastError());
+  // the handles' bookkeeping, as n calls of rn_step would leave it
+  const int delta = f.delta();
+  for (rn_solver* h : b->members) {
+    h->cur = int((h->cur + (long long)n * delta) % 3);
+    if (n & 1) {
+      h->stepIdx = 1 - h->stepIdx;
+      h->wslot = 1 - h->wslot;
+    }
+    h->wvalid = true;
+    h->stepCount += n;
+  }
+  // later work of each member waits for the batch
+  BCK(cudaEventRecord(b->done, b->stream));
+  for (rn_solver* h : b->members) BCK(cudaStreamWaitEvent(h->stream, b->done, 0));
+  return RN_OK;
+}
+
+int rn_batch_autotune(rn_batch b, int steps, int* chosen) {
+  if (!b || steps < 1) return bfail(RN_ERR_ARG, "rn_batch_autotune: bad argument");
+  if (b->members.empty()) {
+    if (chosen) *chosen = b->tile;
+    return RN_OK;
+  }
+  BCK(cudaStreamSynchronize(b->stream));
+  // everything a step changes, per member: state ring, step info, wave-speed
+  // slots, parcel ring; and the host-side positions
+  struct Saved {
+    char* buf = nullptr;
+    size_t state = 0, spray = 0;
+    int cur, stepIdx, wslot, scur;
+    bool wvalid;
+    long long stepCount;
+    uint32_t head, seed;
+  };
+  const bool inj = b->flags.inj != 0;
+  std::vector<Saved> sv(b->members.size());
+  auto release = [&]() {
+    for (Saved& s : sv) cudaFree(s.buf);
+  };
+  for (size_t m = 0; m < b->members.size(); m++) {
+    rn_solver* h = b->members[m];
+    int rc = rn_ensure_wave_speed(h);
+    if (rc != RN_OK) { release(); return rc; }
+    Saved& s = sv[m];
+    s.state = sizeof(float4) * size_t(h->Nx) * h->Nr * 6;
+    s.spray = inj ? sizeof(float4) * SPRAY_N * 6 : 0;
+    cudaError_t e = cudaMalloc(&s.buf, s.state + s.spray + sizeof(float4) * 2 + sizeof(unsigned) * 2);
+    if (e != cudaSuccess) { s.buf = nullptr; release(); return rn_record_cuda(e, "rn_batch_autotune: cudaMalloc"); }
+    s.cur = h->cur; s.stepIdx = h->stepIdx; s.wslot = h->wslot; s.scur = h->scur; s.wvalid = h->wvalid;
+    s.stepCount = h->stepCount; s.head = h->head; s.seed = h->seed;
+  }
+  auto copy_all = [&](bool toSave) -> cudaError_t {
+    for (size_t m = 0; m < b->members.size(); m++) {
+      rn_solver* h = b->members[m];
+      Saved& s = sv[m];
+      struct { void* dev; size_t n; } parts[4] = {{h->SA[0], s.state}, {h->PA[0], s.spray},
+                                                 {h->stepTex, sizeof(float4) * 2}, {h->wmax, sizeof(unsigned) * 2}};
+      char* p = s.buf;
+      for (auto& q : parts) {
+        if (!q.n) continue;
+        cudaError_t e = toSave ? cudaMemcpyAsync(p, q.dev, q.n, cudaMemcpyDeviceToDevice, h->stream)
+                               : cudaMemcpyAsync(q.dev, p, q.n, cudaMemcpyDeviceToDevice, h->stream);
+        if (e != cudaSuccess) return e;
+        p += q.n;
+      }
+      if (!toSave) {
+        h->cur = s.cur; h->stepIdx = s.stepIdx; h->wslot = s.wslot; h->scur = s.scur; h->wvalid = s.wvalid;
+        h->stepCount = s.stepCount; h->head = s.head; h->seed = s.seed;
+      }
+    }
+    return cudaSuccess;
+  };
+  const int ctr = b->ctr;
+  const long long launches = b->launches;
+  const int old = b->tile;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t e = copy_all(true);
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  int best = old, rc = RN_OK;
+  float bestMs = 1e30f;
+  for (int shape = 0; shape < NTILES && e == cudaSuccess && rc == RN_OK; shape++) {
+    if (rn_batch_set_tile(b, shape) != RN_OK) continue;    // a member's lists do not fit this shape
+    rc = rn_batch_step(b, PERIOD);                          // warm-up (builds the graph)
+    float ms = 0.0f;
+    if (rc == RN_OK) e = cudaEventRecord(e0, b->stream);
+    if (rc == RN_OK && e == cudaSuccess) rc = rn_batch_step(b, steps);
+    if (rc == RN_OK && e == cudaSuccess) e = cudaEventRecord(e1, b->stream);
+    if (rc == RN_OK && e == cudaSuccess) e = cudaEventSynchronize(e1);
+    if (rc == RN_OK && e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (rc == RN_OK && e == cudaSuccess && ms < bestMs) { bestMs = ms; best = shape; }
+    // members' streams wait for the batch (rn_batch_step), then restore
+    if (e == cudaSuccess) e = copy_all(false);
+    b->ctr = ctr;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  for (rn_solver* h : b->members) cudaStreamSynchronize(h->stream);
+  release();
+  b->launches = launches;
+  b->uploaded.clear();
+  int rc2 = rn_batch_set_tile(b, best);
+  if (e != cudaSuccess) return rn_record_cuda(e, "rn_batch_autotune");
+  if (rc != RN_OK) return rc;
+  if (rc2 != RN_OK) return rc2;
+  if (chosen) *chosen = best;
+  return RN_OK;
+}
+
+int rn_batch_sync(rn_batch b) {
+  if (!b) return bfail(RN_ERR_ARG, "rn_batch_sync: NULL batch");
+  BCK(cudaStreamSynchronize(b->stream));
+  return RN_OK;
+}
+
+int rn_batch_stream(rn_batch b, void** stream) {
+  if (!b || !stream) return bfail(RN_ERR_ARG, "rn_batch_stream: bad argument");
+  *stream = reinterpret_cast<void*>(b->stream);
+  return RN_OK;
+}
+
+int rn_batch_kernel_launches(rn_batch b, long long* out) {
+  if (!b || !out) return bfail(RN_ERR_ARG, "rn_batch_kernel_launches: bad argument");
+  *out = b->launches;
+  return RN_OK;
+}
+
+}  // extern "C"

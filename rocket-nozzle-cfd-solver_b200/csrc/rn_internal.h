@@ -1,0 +1,77 @@
+// rn_internal.h -- the solver handle and helpers shared by the C-ABI sources
+// (rn_api.cu, rn_batch.cu). Not part of the public interface.
+#pragma once
+#include <cuda_runtime.h>
+#include <string>
+#include <utility>
+#include <vector>
+#include "rn.h"
+#include "rn_kernels.cuh"
+
+// One solver instance: all of its device memory and its stream. The layout in
+// HBM is the reference's texture layout as plain arrays (see rn_api.cu).
+struct rn_solver {
+  int Nx = 0, Nr = 0, device = 0;
+  cudaStream_t stream = nullptr;
+  float4* SA[3] = {nullptr, nullptr, nullptr};
+  float4* SB[3] = {nullptr, nullptr, nullptr};
+  int cur = 0;
+  float4 *geoA = nullptr, *geoG = nullptr, *geoM = nullptr, *jw = nullptr, *wallRow = nullptr;
+  uint8_t* mask = nullptr;
+  float4* stepTex = nullptr;      // [2]
+  unsigned* wmax = nullptr;       // [2]
+  int stepIdx = 0, wslot = 0;
+  bool wvalid = false;
+  long long stepCount = 0, launches = 0;
+  // spray
+  float4 *PA[2] = {nullptr, nullptr}, *PB[2] = {nullptr, nullptr}, *PC[2] = {nullptr, nullptr};
+  float4 *src = nullptr, *tab = nullptr, *dep = nullptr;
+  unsigned *key = nullptr, *val = nullptr, *keyS = nullptr, *valS = nullptr;
+  void* sortTemp = nullptr;
+  size_t sortTempBytes = 0;
+  int scur = 0;
+  uint32_t head = 0, seed = 1;
+  // asynchronous read-back
+  float* pinned = nullptr;
+  size_t pinnedCap = 0, asyncFloats = 0;
+  cudaEvent_t asyncEv = nullptr;
+  bool asyncBusy = false;
+  int asyncTag = 0;
+  double* dInt = nullptr;
+  // per-kernel event timing
+  bool prof = false;
+  std::vector<cudaEvent_t> evPool;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> evPending;
+  double profMs[RN_NKERNELS] = {0};
+  long long profN[RN_NKERNELS] = {0};
+  // tile shape of the stage/physics kernels and, per tile, the out-of-tile
+  // members of its cut-cell groups (built from host copies of the topology)
+  int tile = 0;
+  int* xoff = nullptr;
+  int* xcell = nullptr;
+  int maxX = 1;
+  std::vector<uint8_t> hostMask;
+  std::vector<float> hostGeoM;
+  // kernels of the selected precision (rn_set_precision)
+  const rn::KernelSet* K = &rn::kernels_fast;
+  // the batch this handle is stepped by, if any (rn_batch.cu)
+  struct rn_batch_t* batch = nullptr;
+
+  rn::Grid grid() const { return rn::Grid{Nx, Nr, mask, geoA, geoG, geoM}; }
+};
+
+// Record an error for rn_last_error() and return `code`.
+int rn_record_error(int code, const std::string& msg);
+int rn_record_cuda(cudaError_t e, const char* what);
+// (Re)build the per-tile member lists of `h` for its current tile shape.
+int rn_build_member_lists(rn_solver* h);
+// Make h->wmax[h->wslot] the wave-speed max of the current state if it is not.
+int rn_ensure_wave_speed(rn_solver* h);
+// Takes h out of its batch, if any (rn_batch.cu).
+void rn_batch_detach(rn_solver* h);
+
+#define RN_CK(call)                                            \
+  do {                                                         \
+    cudaError_t e_ = (call);                                   \
+    if (e_ != cudaSuccess) return rn_record_cuda(e_, #call);   \
+  } while (0)

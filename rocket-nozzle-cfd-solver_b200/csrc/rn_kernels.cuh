@@ -1,17 +1,19 @@
-// rn_kernels.cuh -- kernel argument blocks and launch helpers shared by the
+// rn_kernels.cuh -- kernel argument blocks and the kernel sets shared by the
 // step kernels (rn_step.cu), the spray kernels (rn_spray.cu) and the C-ABI
-// (rn_api.cu).
+// (rn_api.cu, rn_batch.cu).
 #pragma once
 #include <cuda_runtime.h>
 #include "rn_math.cuh"
 
 namespace rn {
 
-// Tile of one stage/physics block: TX x TY cells, one thread per cell.
-// Measured on the viscous plume (B200, fast precision): 16x16 beats 32x8 by
-// 4.5 % at 512x192 and 17 % at 1024x384 (fewer halo primitives and faces per
-// cell); 32x4 and 64x4 are 8-30 % slower.
-constexpr int TX = 16, TY = 16, NT = TX * TY;
+// Tile shapes of the stage/physics blocks (one thread per cell). Measured on
+// the viscous plume (B200, fast precision): 16x16 beats 32x8 by 4.5 % at
+// 512x192 and 17 % at 1024x384 (fewer halo primitives and faces per cell);
+// 16x8 gives twice the blocks for small grids. The autotuner picks per handle.
+constexpr int NTILES = 2;
+constexpr int TILE_TX[NTILES] = {16, 16};
+constexpr int TILE_TY[NTILES] = {16, 8};
 // Most out-of-tile group members one tile may list (set_geometry rejects more).
 constexpr int MAXX = 64;
 
@@ -63,6 +65,30 @@ struct ApplyArgs {
   int finalCfl;
 };
 
+// One instance of a batch: its buffers, where it stood in its state ring and
+// step-info ping-pong when the batch was (re)built, its first block in the
+// batch grid, and its parameter block. The kernels derive the slots of step k
+// from (cur0, stepIdx0, wslot0) and the step's BatchPhase.
+struct BatchInst {
+  Grid g;
+  float4* SA[3];
+  float4* SB[3];
+  float4* stepTex;                      // 2 float4
+  unsigned* wmax;                       // 2 slots
+  const int* xoff;
+  const int* xcell;
+  int cur0, stepIdx0, wslot0;
+  int firstBlock, tilesX;
+  int pad_;
+  rn_params P;
+};
+struct BatchPhase {
+  int shift;                            // ring offset of this step: state slot s0 = (cur0 + shift) % 3
+  int par;                              // step parity: stepIdx = stepIdx0 ^ par, wslot = wslot0 ^ par
+  int finalCfl;                         // the launched kernel writes the step's final state
+  int maxX;
+};
+
 // The kernels are compiled twice from the same sources (rn_variant.cu):
 //   exact -- IEEE division and square root: every float operation rounds as
 //            written, so the state matches the CPU oracle bit for bit wherever
@@ -70,12 +96,17 @@ struct ApplyArgs {
 //   fast  -- the hardware's approximate division (div.full) and square root
 //            (within 2 ulp, the latitude GLSL highp gives the reference's
 //            shaders); agrees with the oracle to ~1e-6 relative L2.
-// A solver handle launches through one of the two sets.
+// A solver handle launches through one of the two sets; `tile` selects the
+// tile shape (index into TILE_TX/TILE_TY).
 struct KernelSet {
   const char* name;
-  void (*stage1)(const StageArgs& a, const rn_params& P, cudaStream_t s);
-  void (*stage2)(const StageArgs& a, const rn_params& P, cudaStream_t s);
-  void (*physics)(const PhysArgs& a, const rn_params& P, cudaStream_t s);
+  void (*stage1)(const StageArgs& a, const rn_params& P, int tile, cudaStream_t s);
+  void (*stage2)(const StageArgs& a, const rn_params& P, int tile, cudaStream_t s);
+  void (*physics)(const PhysArgs& a, const rn_params& P, int tile, cudaStream_t s);
+  void (*batchStage1)(const BatchInst* d, const int* blockInst, int nblocks, BatchPhase ph, int tile, cudaStream_t s);
+  void (*batchStage2)(const BatchInst* d, const int* blockInst, int nblocks, BatchPhase ph, int tile, cudaStream_t s);
+  void (*batchPhysics)(const BatchInst* d, const int* blockInst, int nblocks, BatchPhase ph, int tile,
+                       cudaStream_t s);
   void (*reduce)(const Grid& g, const float4* A, const float4* B, unsigned* w, cudaStream_t s);
   void (*rescale)(const Grid& g, const float4* A, const float4* B, float4* oA, float4* oB, float fp, float fT,
                   float du, const rn_params& P, cudaStream_t s);

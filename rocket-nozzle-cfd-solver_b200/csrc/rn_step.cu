@@ -1,43 +1,53 @@
 // rn_step.cu -- fused time-step kernels for sm_100a.
 //
 // One SSP-RK2 stage is ONE kernel (k_stage): a block stages the ghost-cell
-// primitives of its TX x TY tile plus a 2-cell halo in shared memory
-// (FS_PRIM, solver.js:56-126), computes every x- and r-face flux of the tile
-// once (makeFluxShader, solver.js:133-259) into shared memory, then updates
-// each cell over its merged cut-cell group (FS_UPDATE, solver.js:264-363).
-// The reference's 7 full-grid passes per stage (prim, 2 flux, update, CFL
-// chain) and its 6 face textures never touch HBM here.
+// primitives of its tile plus a 2-cell halo in shared memory (FS_PRIM,
+// solver.js:56-126), computes every x- and r-face flux of the tile once
+// (makeFluxShader, solver.js:133-259) into shared memory, then updates each
+// cell over its merged cut-cell group (FS_UPDATE, solver.js:264-363). The
+// reference's 7 full-grid passes per stage (prim, 2 flux, update, CFL chain)
+// and its 6 face textures never touch HBM here.
 //
 // Group members outside the tile (slivers merged across a tile edge) are
 // listed per tile at set_geometry (xoff/xcell). For each listed member the
-// block adds a 5x5 block of primitives around it to the primitive phase and its
-// 4 faces to the face phase: the same loops and the same single instance of
-// the face code run them, so blocks along the walls do no serial or cold-code
-// work.
+// block adds a 5x5 block of primitives around it to the primitive phase and
+// its 4 faces to the face phase: the same loops and the same single instance
+// of the face code run them, so blocks along the walls do no serial or
+// cold-code work.
 //
 // The step's last kernel folds the CFL wave speed of the cells it writes into
 // one atomicMax per block (FS_REDUCE1/2, solver.js:368-397); the next step's
-// stage-1 kernel turns it into dt in every block and block (0,0) stores the
-// step info (FS_STEPINFO, solver.js:398-411). dt never leaves the device.
+// stage-1 kernel turns it into dt in every block and the block of tile 0
+// stores the step info (FS_STEPINFO, solver.js:398-411). dt never leaves the
+// device.
 //
 // The viscous/wall/reaction split step is ONE kernel (k_physics): vcell
 // (FS_VCELL), the viscous face fluxes (makeViscFluxShader) and FS_SOURCE fused
 // per tile, reading the stage-1 primitives (solver.js:940-941).
+//
+// Every body is a device function templated on the tile shape; a
+// single-instance kernel maps blockIdx to a tile, a batch kernel maps its 1-D
+// block index to (instance, tile) through a table and loads the instance's
+// buffers and parameter block into shared memory first.
 #include <cuda_runtime.h>
 #include "rn_kernels.cuh"
 
 namespace rn {
 namespace RN_VARIANT {
 
-constexpr int PX = TX + 4, PY = TY + 4;      // primitive tile with a 2-cell halo
-constexpr int NPT = PX * PY;                  // tile primitives
-constexpr int NXF = TY * (TX + 1);            // x-faces of a tile
-constexpr int NRF = (TY + 1) * TX;            // r-faces of a tile
-constexpr int TW = TX + 2;                    // vcell ring width (tile + 1)
-constexpr int NTT = (TX + 2) * (TY + 2);      // vcell ring cells
+template <int TX_, int TY_>
+struct TileT {
+  static constexpr int TX = TX_, TY = TY_, NT = TX * TY;
+  static constexpr int PX = TX + 4, PY = TY + 4, NPT = PX * PY;   // primitives with a 2-cell halo
+  static constexpr int NXF = TY * (TX + 1), NRF = (TY + 1) * TX;  // x- and r-faces of a tile
+  static constexpr int TW = TX + 2, NTT = (TX + 2) * (TY + 2);    // vcell ring (tile + 1)
+};
+using Tile0 = TileT<TILE_TX[0], TILE_TY[0]>;
+using Tile1 = TileT<TILE_TX[1], TILE_TY[1]>;
 
 // --------------------------------------------------------------------------
 // block-wide max of non-negative floats -> one atomicMax on the bit pattern
+template <int NT>
 __device__ __forceinline__ void block_max_to(float w, unsigned* out, float* red) {
   for (int o = 16; o > 0; o >>= 1) w = fmaxf(w, __shfl_xor_sync(0xffffffffu, w, o));
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -50,18 +60,23 @@ __device__ __forceinline__ void block_max_to(float w, unsigned* out, float* red)
   }
 }
 
-// Shared-memory index of the primitive of cell (i, j): tile cells live in the
-// PX x PY tile array, listed members' neighbourhoods in 5x5 blocks after it.
-__device__ __forceinline__ int ext_prim(int e, int dx, int dy) { return NPT + e * 25 + (dy + 2) * 5 + (dx + 2); }
+// Shared-memory index of the primitive of cell (mx + dx, my + dy) for listed
+// member e: tile cells live in the PX x PY tile array, listed members'
+// neighbourhoods in 5x5 blocks after it.
+template <class T>
+__device__ __forceinline__ int ext_prim(int e, int dx, int dy) {
+  return T::NPT + e * 25 + (dy + 2) * 5 + (dx + 2);
+}
 
 // Coordinates of primitive slot k (tile first, then one 5x5 block per member).
+template <class T>
 __device__ __forceinline__ void prim_slot(int k, int x0, int y0, const int* xc, int Nx, int& i, int& j) {
-  if (k < NPT) {
-    const int ly = k / PX;
-    i = x0 - 2 + (k - ly * PX);
+  if (k < T::NPT) {
+    const int ly = k / T::PX;
+    i = x0 - 2 + (k - ly * T::PX);
     j = y0 - 2 + ly;
   } else {
-    const int q = k - NPT, e = q / 25, r = q - e * 25, m = xc[e];
+    const int q = k - T::NPT, e = q / 25, r = q - e * 25, m = xc[e];
     const int dy = r / 5;
     i = m % Nx + (r - dy * 5) - 2;
     j = m / Nx + dy - 2;
@@ -76,77 +91,90 @@ struct FaceSlot {
   int i, j;
   bool dirR, valid;
 };
+template <class T>
 __device__ __forceinline__ FaceSlot face_slot(int k, int x0, int y0, const int* xc, int Nx, int Nr) {
+  constexpr int PX = T::PX, TX = T::TX;
   FaceSlot f;
-  if (k < NXF) {                                   // x-face (i, j): west face of cell (i, j)
+  if (k < T::NXF) {                                // x-face (i, j): west face of cell (i, j)
     const int ly = k / (TX + 1), lx = k - ly * (TX + 1), py = ly + 2;
     f.i = x0 + lx; f.j = y0 + ly; f.dirR = false;
     f.valid = f.i <= Nx && f.j < Nr;
     const int b = py * PX + lx;
     f.c[0] = b; f.c[1] = b + 1; f.c[2] = b + 2; f.c[3] = b + 3;
     f.s[0] = b + PX + 1; f.s[1] = b - PX + 1; f.s[2] = b + PX + 2; f.s[3] = b - PX + 2;
-  } else if (k < NXF + NRF) {                      // r-face (i, j): south face of cell (i, j)
-    const int kk = k - NXF, ly = kk / TX, lx = kk - ly * TX, px = lx + 2;
+  } else if (k < T::NXF + T::NRF) {                // r-face (i, j): south face of cell (i, j)
+    const int kk = k - T::NXF, ly = kk / TX, lx = kk - ly * TX, px = lx + 2;
     f.i = x0 + lx; f.j = y0 + ly; f.dirR = true;
     f.valid = f.i < Nx && f.j <= Nr && f.j != 0;
     const int b = ly * PX + px;
     f.c[0] = b; f.c[1] = b + PX; f.c[2] = b + 2 * PX; f.c[3] = b + 3 * PX;
     f.s[0] = b + PX + 1; f.s[1] = b + PX - 1; f.s[2] = b + 2 * PX + 1; f.s[3] = b + 2 * PX - 1;
   } else {                                         // faces of listed member e: W, E, S, N
-    const int q = k - NXF - NRF, e = q >> 2, w = q & 3, m = xc[e];
+    const int q = k - T::NXF - T::NRF, e = q >> 2, w = q & 3, m = xc[e];
     const int mx = m % Nx, my = m / Nx;
     if (w < 2) {
       const int o = w;                             // face at mx + o
       f.i = mx + o; f.j = my; f.dirR = false; f.valid = true;
-      f.c[0] = ext_prim(e, o - 2, 0); f.c[1] = ext_prim(e, o - 1, 0);
-      f.c[2] = ext_prim(e, o, 0); f.c[3] = ext_prim(e, o + 1, 0);
-      f.s[0] = ext_prim(e, o - 1, 1); f.s[1] = ext_prim(e, o - 1, -1);
-      f.s[2] = ext_prim(e, o, 1); f.s[3] = ext_prim(e, o, -1);
+      f.c[0] = ext_prim<T>(e, o - 2, 0); f.c[1] = ext_prim<T>(e, o - 1, 0);
+      f.c[2] = ext_prim<T>(e, o, 0); f.c[3] = ext_prim<T>(e, o + 1, 0);
+      f.s[0] = ext_prim<T>(e, o - 1, 1); f.s[1] = ext_prim<T>(e, o - 1, -1);
+      f.s[2] = ext_prim<T>(e, o, 1); f.s[3] = ext_prim<T>(e, o, -1);
     } else {
       const int o = w - 2;                         // face at my + o
       f.i = mx; f.j = my + o; f.dirR = true; f.valid = f.j != 0;
-      f.c[0] = ext_prim(e, 0, o - 2); f.c[1] = ext_prim(e, 0, o - 1);
-      f.c[2] = ext_prim(e, 0, o); f.c[3] = ext_prim(e, 0, o + 1);
-      f.s[0] = ext_prim(e, 1, o - 1); f.s[1] = ext_prim(e, -1, o - 1);
-      f.s[2] = ext_prim(e, 1, o); f.s[3] = ext_prim(e, -1, o);
+      f.c[0] = ext_prim<T>(e, 0, o - 2); f.c[1] = ext_prim<T>(e, 0, o - 1);
+      f.c[2] = ext_prim<T>(e, 0, o); f.c[3] = ext_prim<T>(e, 0, o + 1);
+      f.s[0] = ext_prim<T>(e, 1, o - 1); f.s[1] = ext_prim<T>(e, -1, o - 1);
+      f.s[2] = ext_prim<T>(e, 1, o); f.s[3] = ext_prim<T>(e, -1, o);
     }
   }
   return f;
 }
 
 // The four face slots (W, E, S, N) of group member (cx, cy).
+template <class T>
 __device__ __forceinline__ void member_faces(int cx, int cy, int x0, int y0, const int* xc, int xn, int Nx,
                                              int& fw, int& fe, int& fs, int& fn) {
   const int mx = cx - x0, my = cy - y0;
-  if (mx >= 0 && mx < TX && my >= 0 && my < TY) {
-    fw = my * (TX + 1) + mx;
+  if (mx >= 0 && mx < T::TX && my >= 0 && my < T::TY) {
+    fw = my * (T::TX + 1) + mx;
     fe = fw + 1;
-    fs = NXF + my * TX + mx;
-    fn = fs + TX;
+    fs = T::NXF + my * T::TX + mx;
+    fn = fs + T::TX;
   } else {
     const int mc = cy * Nx + cx;
     int e = 0;
     while (e < xn - 1 && xc[e] != mc) e++;
-    fw = NXF + NRF + 4 * e;
+    fw = T::NXF + T::NRF + 4 * e;
     fe = fw + 1;
     fs = fw + 2;
     fn = fw + 3;
   }
 }
 
+// Dynamic shared memory of one block for a largest member list of maxX cells.
+template <class T>
+__host__ __device__ constexpr size_t stage_smem_t(int maxX) {
+  return sizeof(float4) * (2 * (T::NPT + 25 * maxX) + 2 * (T::NXF + T::NRF + 4 * maxX)) +
+         sizeof(float) * (T::NXF + T::NRF + 4 * maxX);
+}
+template <class T>
+__host__ __device__ constexpr size_t physics_smem_t(int maxX) {
+  return sizeof(float4) * (2 * (T::NPT + 25 * maxX) + 2 * (T::NTT + 5 * maxX) + 2 * (T::NXF + T::NRF + 4 * maxX));
+}
+
 // --------------------------------------------------------------------------
-template <int STAGE>
-__global__ void __launch_bounds__(NT) k_stage(StageArgs a, rn_params P) {
-  extern __shared__ float4 sm[];
-  __shared__ float red[NT / 32];
-  __shared__ int xc[MAXX];
-  const Grid g = a.g;
+// One RK stage on tile (bx, by) = tile index tileId of the instance in `a`.
+template <class T, int STAGE>
+__device__ __forceinline__ void stage_body(const StageArgs& a, const rn_params& P, int bx, int by, int tileId,
+                                           float4* sm, float* red, int* xc) {
+  constexpr int TX = T::TX, NT = T::NT;
+  const Grid& g = a.g;
   const int Nx = g.Nx, Nr = g.Nr, W1 = Nx + 1;
   const int tid = threadIdx.x;
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-  const int tileId = blockIdx.y * gridDim.x + blockIdx.x;
+  const int x0 = bx * TX, y0 = by * T::TY;
   const int xb = a.xoff[tileId], xn = a.xoff[tileId + 1] - xb;
-  const int NP = NPT + 25 * xn, NF = NXF + NRF + 4 * xn;
+  const int NP = T::NPT + 25 * xn, NF = T::NXF + T::NRF + 4 * xn;
   float4* sW = sm;
   float4* sWb = sW + NP;
   float4* sF = sWb + NP;
@@ -161,7 +189,7 @@ __global__ void __launch_bounds__(NT) k_stage(StageArgs a, rn_params P) {
     dt = fminf(P.cfl / w, P.dtMax);
     if (prev.x > 0.0f) dt = fminf(dt, prev.x * 1.2f);
     t = prev.z;                                   // inlet ramp at t_old
-    if (blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) {
+    if (tileId == 0 && tid == 0) {
       *a.stNew = make_float4(dt, prev.z, prev.z + dt, w);
       *a.wOut = 0u;
     }
@@ -175,7 +203,7 @@ __global__ void __launch_bounds__(NT) k_stage(StageArgs a, rn_params P) {
   // ---- ghost-cell primitives: tile + 2-cell halo, then the members' blocks
   for (int k = tid; k < NP; k += NT) {
     int i, j;
-    prim_slot(k, x0, y0, xc, Nx, i, j);
+    prim_slot<T>(k, x0, y0, xc, Nx, i, j);
     float4 W, Wb;
     if (i <= Nx + 1 && j <= Nr + 1) ghost_prim(g, a.A, a.B, i, j, t, P, W, Wb);
     else { W = make_float4(-1.f, 0.f, 0.f, 1.f); Wb = make_float4(0.f, 0.f, 0.f, 0.f); }
@@ -186,7 +214,7 @@ __global__ void __launch_bounds__(NT) k_stage(StageArgs a, rn_params P) {
 
   // ---- face fluxes: tile x-faces, tile r-faces, members' faces
   for (int k = tid; k < NF; k += NT) {
-    const FaceSlot s = face_slot(k, x0, y0, xc, Nx, Nr);
+    const FaceSlot s = face_slot<T>(k, x0, y0, xc, Nx, Nr);
     Flux f;
     f.F = make_float4(0.f, 0.f, 0.f, 0.f); f.Y = f.F; f.O = 0.f;
     if (s.valid) {
@@ -230,7 +258,7 @@ __global__ void __launch_bounds__(NT) k_stage(StageArgs a, rn_params P) {
         float aw = fabsf(gc.z), ae = fabsf(g.geoA[cy * W1 + cx + 1].z);
         float as_ = fabsf(gc.w), an = fabsf(g.geoA[(cy + 1) * W1 + cx].w);
         int fw, fe, fs, fn;
-        member_faces(cx, cy, x0, y0, xc, xn, Nx, fw, fe, fs, fn);
+        member_faces<T>(cx, cy, x0, y0, xc, xn, Nx, fw, fe, fs, fn);
         sub4(L, ae, sF[fe], aw, sF[fw]);
         sub4(L, an, sF[fn], as_, sF[fs]);
         sub4(LY, ae, sY[fe], aw, sY[fw]);
@@ -291,46 +319,43 @@ __global__ void __launch_bounds__(NT) k_stage(StageArgs a, rn_params P) {
     a.oB[k] = oB;
     if (a.finalCfl && fluid) wcell = wave_speed(oA, oB);
   }
-  if (a.finalCfl) block_max_to(wcell, a.wOut, red);
+  if (a.finalCfl) block_max_to<NT>(wcell, a.wOut, red);
 }
 
 // --------------------------------------------------------------------------
 // vcell slot k: the tile + 1 ring first, then 5 cells per listed member
 // (itself, W, E, S, N). Returns the cell and the primitive slots of the cell
 // and its E, W, N, S neighbours.
+template <class T>
 __device__ __forceinline__ void vcell_slot(int k, int x0, int y0, const int* xc, int Nx, int& i, int& j, int& c,
                                            int& e_, int& w_, int& n_, int& s_) {
-  if (k < NTT) {
-    const int ly = k / TW, lx = k - ly * TW;
+  if (k < T::NTT) {
+    const int ly = k / T::TW, lx = k - ly * T::TW;
     i = x0 - 1 + lx; j = y0 - 1 + ly;
-    c = (ly + 1) * PX + lx + 1;
-    e_ = c + 1; w_ = c - 1; n_ = c + PX; s_ = c - PX;
+    c = (ly + 1) * T::PX + lx + 1;
+    e_ = c + 1; w_ = c - 1; n_ = c + T::PX; s_ = c - T::PX;
   } else {
-    const int q = k - NTT, e = q / 5, r = q - e * 5, m = xc[e];
+    const int q = k - T::NTT, e = q / 5, r = q - e * 5, m = xc[e];
     const int dx = r == 1 ? -1 : r == 2 ? 1 : 0, dy = r == 3 ? -1 : r == 4 ? 1 : 0;
     i = m % Nx + dx; j = m / Nx + dy;
-    c = ext_prim(e, dx, dy);
+    c = ext_prim<T>(e, dx, dy);
     e_ = c + 1; w_ = c - 1; n_ = c + 5; s_ = c - 5;
   }
 }
 
-// vcell slot of cell (i, j) for the viscous faces: tile ring, or member e's 5 cells
-__device__ __forceinline__ int tile_vslot(int i, int j, int x0, int y0) { return (j - y0 + 1) * TW + (i - x0 + 1); }
-
-// --------------------------------------------------------------------------
-__global__ void __launch_bounds__(NT) k_physics(PhysArgs a, rn_params P) {
-  extern __shared__ float4 sm[];
-  __shared__ float red[NT / 32];
-  __shared__ int xc[MAXX];
-  const Grid g = a.g;
+// The viscous/wall/reaction split step on tile (bx, by).
+template <class T>
+__device__ __forceinline__ void physics_body(const PhysArgs& a, const rn_params& P, int bx, int by, int tileId,
+                                             float4* sm, float* red, int* xc) {
+  constexpr int TX = T::TX, NT = T::NT, PX = T::PX, TW = T::TW;
+  const Grid& g = a.g;
   const int Nx = g.Nx, Nr = g.Nr, W1 = Nx + 1;
   const int tid = threadIdx.x;
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const int x0 = bx * TX, y0 = by * T::TY;
   const float4 st = *a.st;
   const float dt = st.x, t = st.z;
-  const int tileId = blockIdx.y * gridDim.x + blockIdx.x;
   const int xb = a.xoff[tileId], xn = P.visc ? a.xoff[tileId + 1] - xb : 0;
-  const int NP = NPT + 25 * xn, NV = NTT + 5 * xn, NF = NXF + NRF + 4 * xn;
+  const int NP = T::NPT + 25 * xn, NV = T::NTT + 5 * xn, NF = T::NXF + T::NRF + 4 * xn;
   float4* sW = sm;
   float4* sWb = sW + NP;
   float4* sT1 = sWb + NP;
@@ -342,7 +367,7 @@ __global__ void __launch_bounds__(NT) k_physics(PhysArgs a, rn_params P) {
 
   for (int k = tid; k < NP; k += NT) {
     int i, j;
-    prim_slot(k, x0, y0, xc, Nx, i, j);
+    prim_slot<T>(k, x0, y0, xc, Nx, i, j);
     float4 W, Wb;
     if (i <= Nx + 1 && j <= Nr + 1) ghost_prim(g, a.A1, a.B1, i, j, t, P, W, Wb);
     else { W = make_float4(-1.f, 0.f, 0.f, 1.f); Wb = make_float4(0.f, 0.f, 0.f, 0.f); }
@@ -353,7 +378,7 @@ __global__ void __launch_bounds__(NT) k_physics(PhysArgs a, rn_params P) {
   // vcell over the tile + 1 ring and the members' cells
   for (int k = tid; k < NV; k += NT) {
     int i, j, c, e_, w_, n_, s_;
-    vcell_slot(k, x0, y0, xc, Nx, i, j, c, e_, w_, n_, s_);
+    vcell_slot<T>(k, x0, y0, xc, Nx, i, j, c, e_, w_, n_, s_);
     float4 T1 = make_float4(0.f, 0.f, 0.f, 0.f), T2 = T1;
     if (i >= 0 && i < Nx && j >= 0 && j < Nr)
       vcell(sW[c], sWb[c], sW[e_], sW[w_], sW[n_], sW[s_], i, j, g.geoM[j * Nx + i].w, dt, P, T1, T2);
@@ -366,25 +391,25 @@ __global__ void __launch_bounds__(NT) k_physics(PhysArgs a, rn_params P) {
       float4 F = make_float4(0.f, 0.f, 0.f, 0.f), FY = F;
       bool dirR, ok;
       int i, j, p1, p2, v1, v2;          // primitive and vcell slots of the cells behind (1) and at (2) the face
-      if (k < NXF) {
+      if (k < T::NXF) {
         const int ly = k / (TX + 1), lx = k - ly * (TX + 1);
         i = x0 + lx; j = y0 + ly; dirR = false;
         ok = i > 0 && i < Nx && j < Nr;
         p2 = (ly + 2) * PX + lx + 2; p1 = p2 - 1;
         v2 = (ly + 1) * TW + lx + 1; v1 = v2 - 1;
-      } else if (k < NXF + NRF) {
-        const int kk = k - NXF, ly = kk / TX, lx = kk - ly * TX;
+      } else if (k < T::NXF + T::NRF) {
+        const int kk = k - T::NXF, ly = kk / TX, lx = kk - ly * TX;
         i = x0 + lx; j = y0 + ly; dirR = true;
         ok = i < Nx && j > 0 && j < Nr;
         p2 = (ly + 2) * PX + lx + 2; p1 = p2 - PX;
         v2 = (ly + 1) * TW + lx + 1; v1 = v2 - TW;
       } else {
-        const int q = k - NXF - NRF, e = q >> 2, w = q & 3, m = xc[e];
-        const int mx = m % Nx, my = m / Nx, vb = NTT + 5 * e;
-        if (w == 0) { i = mx; j = my; dirR = false; p1 = ext_prim(e, -1, 0); p2 = ext_prim(e, 0, 0); v1 = vb + 1; v2 = vb; }
-        else if (w == 1) { i = mx + 1; j = my; dirR = false; p1 = ext_prim(e, 0, 0); p2 = ext_prim(e, 1, 0); v1 = vb; v2 = vb + 2; }
-        else if (w == 2) { i = mx; j = my; dirR = true; p1 = ext_prim(e, 0, -1); p2 = ext_prim(e, 0, 0); v1 = vb + 3; v2 = vb; }
-        else { i = mx; j = my + 1; dirR = true; p1 = ext_prim(e, 0, 0); p2 = ext_prim(e, 0, 1); v1 = vb; v2 = vb + 4; }
+        const int q = k - T::NXF - T::NRF, e = q >> 2, w = q & 3, m = xc[e];
+        const int mx = m % Nx, my = m / Nx, vb = T::NTT + 5 * e;
+        if (w == 0) { i = mx; j = my; dirR = false; p1 = ext_prim<T>(e, -1, 0); p2 = ext_prim<T>(e, 0, 0); v1 = vb + 1; v2 = vb; }
+        else if (w == 1) { i = mx + 1; j = my; dirR = false; p1 = ext_prim<T>(e, 0, 0); p2 = ext_prim<T>(e, 1, 0); v1 = vb; v2 = vb + 2; }
+        else if (w == 2) { i = mx; j = my; dirR = true; p1 = ext_prim<T>(e, 0, -1); p2 = ext_prim<T>(e, 0, 0); v1 = vb + 3; v2 = vb; }
+        else { i = mx; j = my + 1; dirR = true; p1 = ext_prim<T>(e, 0, 0); p2 = ext_prim<T>(e, 0, 1); v1 = vb; v2 = vb + 4; }
         ok = dirR ? (i < Nx && j > 0 && j < Nr) : (i > 0 && i < Nx && j < Nr);
       }
       if (ok) {
@@ -422,7 +447,7 @@ __global__ void __launch_bounds__(NT) k_physics(PhysArgs a, rn_params P) {
       float V = fmaxf(gg.x, 1e-6f);
       float Rm = rmix(q.s, P), Tg = p / (rho * Rm);
       float4 L = make_float4(0.f, 0.f, 0.f, 0.f), LY = L;
-      const int vh = tile_vslot(Hx, Hy, x0, y0);
+      const int vh = (Hy - y0 + 1) * TW + (Hx - x0 + 1);
       float4 T1h = sT1[vh], T2h = sT2[vh];
       if (P.visc) {
         const int sm_ = iround(g.geoM[kh].z);
@@ -436,7 +461,7 @@ __global__ void __launch_bounds__(NT) k_physics(PhysArgs a, rn_params P) {
           float aw = fabsf(gc.z), ae = fabsf(g.geoA[cy * W1 + cx + 1].z);
           float as_ = fabsf(gc.w), an = fabsf(g.geoA[(cy + 1) * W1 + cx].w);
           int fw, fe, fs, fn;
-          member_faces(cx, cy, x0, y0, xc, xn, Nx, fw, fe, fs, fn);
+          member_faces<T>(cx, cy, x0, y0, xc, xn, Nx, fw, fe, fs, fn);
           sub4(L, ae, sF[fe], aw, sF[fw]);
           sub4(L, an, sF[fn], as_, sF[fs]);
           sub4(LY, ae, sY[fe], aw, sY[fw]);
@@ -530,19 +555,93 @@ __global__ void __launch_bounds__(NT) k_physics(PhysArgs a, rn_params P) {
     a.oB[k] = oB;
     if (a.finalCfl && fluid) wcell = wave_speed(oA, oB);
   }
-  if (a.finalCfl) block_max_to(wcell, a.wOut, red);
+  if (a.finalCfl) block_max_to<NT>(wcell, a.wOut, red);
+}
+
+// --------------------------------------------------------------------------
+// Single-instance kernels: blockIdx = tile.
+template <class T, int STAGE>
+__global__ void __launch_bounds__(T::NT) k_stage(StageArgs a, rn_params P) {
+  extern __shared__ float4 sm[];
+  __shared__ float red[T::NT / 32];
+  __shared__ int xc[MAXX];
+  stage_body<T, STAGE>(a, P, blockIdx.x, blockIdx.y, blockIdx.y * gridDim.x + blockIdx.x, sm, red, xc);
+}
+template <class T>
+__global__ void __launch_bounds__(T::NT) k_physics(PhysArgs a, rn_params P) {
+  extern __shared__ float4 sm[];
+  __shared__ float red[T::NT / 32];
+  __shared__ int xc[MAXX];
+  physics_body<T>(a, P, blockIdx.x, blockIdx.y, blockIdx.y * gridDim.x + blockIdx.x, sm, red, xc);
+}
+
+// Batch kernels: block b belongs to instance blockInst[b]; its descriptor
+// (buffers, ring position, parameter block) is staged in shared memory.
+__device__ __forceinline__ void load_inst(const BatchInst* insts, const int* blockInst, BatchInst& d) {
+  __shared__ int di;
+  if (threadIdx.x == 0) di = blockInst[blockIdx.x];
+  __syncthreads();
+  const int* src = reinterpret_cast<const int*>(insts + di);
+  int* dst = reinterpret_cast<int*>(&d);
+  for (int q = threadIdx.x; q < int(sizeof(BatchInst) / sizeof(int)); q += blockDim.x) dst[q] = src[q];
+  __syncthreads();
+}
+template <class T, int STAGE>
+__global__ void __launch_bounds__(T::NT) k_stage_batch(const BatchInst* insts, const int* blockInst, BatchPhase ph) {
+  extern __shared__ float4 sm[];
+  __shared__ float red[T::NT / 32];
+  __shared__ int xc[MAXX];
+  __shared__ BatchInst d;
+  load_inst(insts, blockInst, d);
+  const int s0 = (d.cur0 + ph.shift) % 3, s1 = (s0 + 1) % 3, s2 = (s0 + 2) % 3;
+  const int si = d.stepIdx0 ^ ph.par, ws = d.wslot0 ^ ph.par;
+  StageArgs a;
+  a.g = d.g;
+  if (STAGE == 1) {
+    a.A = d.SA[s0]; a.B = d.SB[s0]; a.A0 = d.SA[s0]; a.B0 = d.SB[s0]; a.oA = d.SA[s1]; a.oB = d.SB[s1];
+  } else {
+    a.A = d.SA[s1]; a.B = d.SB[s1]; a.A0 = d.SA[s0]; a.B0 = d.SB[s0]; a.oA = d.SA[s2]; a.oB = d.SB[s2];
+  }
+  a.stPrev = d.stepTex + si;
+  a.stNew = d.stepTex + (1 - si);
+  a.wIn = d.wmax + ws;
+  a.wOut = d.wmax + (1 - ws);
+  a.finalCfl = ph.finalCfl;
+  a.xoff = d.xoff; a.xcell = d.xcell; a.maxX = ph.maxX;
+  const int local = blockIdx.x - d.firstBlock, by = local / d.tilesX, bx = local - by * d.tilesX;
+  stage_body<T, STAGE>(a, d.P, bx, by, local, sm, red, xc);
+}
+template <class T>
+__global__ void __launch_bounds__(T::NT) k_physics_batch(const BatchInst* insts, const int* blockInst, BatchPhase ph) {
+  extern __shared__ float4 sm[];
+  __shared__ float red[T::NT / 32];
+  __shared__ int xc[MAXX];
+  __shared__ BatchInst d;
+  load_inst(insts, blockInst, d);
+  const int s0 = (d.cur0 + ph.shift) % 3, s1 = (s0 + 1) % 3, s2 = (s0 + 2) % 3;
+  const int si = d.stepIdx0 ^ ph.par, ws = d.wslot0 ^ ph.par;
+  PhysArgs a;
+  a.g = d.g;
+  a.A1 = d.SA[s1]; a.B1 = d.SB[s1]; a.A2 = d.SA[s2]; a.B2 = d.SB[s2]; a.oA = d.SA[s0]; a.oB = d.SB[s0];
+  a.st = d.stepTex + (1 - si);
+  a.wOut = d.wmax + (1 - ws);
+  a.finalCfl = ph.finalCfl;
+  a.xoff = d.xoff; a.xcell = d.xcell; a.maxX = ph.maxX;
+  const int local = blockIdx.x - d.firstBlock, by = local / d.tilesX, bx = local - by * d.tilesX;
+  physics_body<T>(a, d.P, bx, by, local, sm, red, xc);
 }
 
 // --------------------------------------------------------------------------
 // stand-alone CFL reduction of a state (first step after setState/rescale)
-__global__ void __launch_bounds__(NT) k_reduce(Grid g, const float4* __restrict__ A, const float4* __restrict__ B,
-                                               unsigned* out) {
-  __shared__ float red[NT / 32];
+constexpr int RED_NT = 256;
+__global__ void __launch_bounds__(RED_NT) k_reduce(Grid g, const float4* __restrict__ A,
+                                                   const float4* __restrict__ B, unsigned* out) {
+  __shared__ float red[RED_NT / 32];
   const int N = g.Nx * g.Nr;
   float w = 0.0f;
-  for (int k = blockIdx.x * NT + threadIdx.x; k < N; k += gridDim.x * NT)
+  for (int k = blockIdx.x * RED_NT + threadIdx.x; k < N; k += gridDim.x * RED_NT)
     if (!g.mask[k]) w = fmaxf(w, wave_speed(A[k], B[k]));
-  block_max_to(w, out, red);
+  block_max_to<RED_NT>(w, out, red);
 }
 
 // FS_RESCALE (solver.js:418-437)
@@ -657,44 +756,59 @@ __global__ void k_integrals(Grid g, const float4* __restrict__ A, const float4* 
 }
 
 // --------------------------------------------------------------------------
-static dim3 tiles(const Grid& g) { return dim3((g.Nx + TX - 1) / TX, (g.Nr + TY - 1) / TY); }
-// dynamic shared memory for a largest per-tile member list of maxX cells
-size_t stage_smem(int maxX) {
-  return sizeof(float4) * (2 * (NPT + 25 * maxX) + 2 * (NXF + NRF + 4 * maxX)) + sizeof(float) * (NXF + NRF + 4 * maxX);
-}
-size_t physics_smem(int maxX) {
-  return sizeof(float4) * (2 * (NPT + 25 * maxX) + 2 * (NTT + 5 * maxX) + 2 * (NXF + NRF + 4 * maxX));
+// launchers
+template <class T>
+static dim3 tiles_of(const Grid& g) {
+  return dim3((g.Nx + T::TX - 1) / T::TX, (g.Nr + T::TY - 1) / T::TY);
 }
 
-// Raises the dynamic shared-memory limit of the stage and physics kernels to
-// what a member list of MAXX cells needs (a process-wide function attribute).
-int stage_kernels_init() {
-  if (cudaFuncSetAttribute(k_stage<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(stage_smem(MAXX))) !=
-      cudaSuccess)
+template <class T>
+static int init_tile() {
+  const int ss = int(stage_smem_t<T>(MAXX)), ps = int(physics_smem_t<T>(MAXX));
+  if (cudaFuncSetAttribute(k_stage<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss) != cudaSuccess) return -1;
+  if (cudaFuncSetAttribute(k_stage<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss) != cudaSuccess) return -1;
+  if (cudaFuncSetAttribute(k_physics<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps) != cudaSuccess) return -1;
+  if (cudaFuncSetAttribute(k_stage_batch<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss) != cudaSuccess)
     return -1;
-  if (cudaFuncSetAttribute(k_stage<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(stage_smem(MAXX))) !=
-      cudaSuccess)
+  if (cudaFuncSetAttribute(k_stage_batch<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss) != cudaSuccess)
     return -1;
-  if (cudaFuncSetAttribute(k_physics, cudaFuncAttributeMaxDynamicSharedMemorySize, int(physics_smem(MAXX))) !=
-      cudaSuccess)
+  if (cudaFuncSetAttribute(k_physics_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps) != cudaSuccess)
     return -1;
   return 0;
 }
+// Raises the dynamic shared-memory limits of the stage and physics kernels to
+// what a member list of MAXX cells needs (process-wide function attributes).
+int stage_kernels_init() { return (init_tile<Tile0>() == 0 && init_tile<Tile1>() == 0) ? 0 : -1; }
 
-void launch_stage1(const StageArgs& a, const rn_params& P, cudaStream_t s) {
-  k_stage<1><<<tiles(a.g), NT, stage_smem(a.maxX), s>>>(a, P);
+void launch_stage1(const StageArgs& a, const rn_params& P, int tile, cudaStream_t s) {
+  if (tile == 1) k_stage<Tile1, 1><<<tiles_of<Tile1>(a.g), Tile1::NT, stage_smem_t<Tile1>(a.maxX), s>>>(a, P);
+  else k_stage<Tile0, 1><<<tiles_of<Tile0>(a.g), Tile0::NT, stage_smem_t<Tile0>(a.maxX), s>>>(a, P);
 }
-void launch_stage2(const StageArgs& a, const rn_params& P, cudaStream_t s) {
-  k_stage<2><<<tiles(a.g), NT, stage_smem(a.maxX), s>>>(a, P);
+void launch_stage2(const StageArgs& a, const rn_params& P, int tile, cudaStream_t s) {
+  if (tile == 1) k_stage<Tile1, 2><<<tiles_of<Tile1>(a.g), Tile1::NT, stage_smem_t<Tile1>(a.maxX), s>>>(a, P);
+  else k_stage<Tile0, 2><<<tiles_of<Tile0>(a.g), Tile0::NT, stage_smem_t<Tile0>(a.maxX), s>>>(a, P);
 }
-void launch_physics(const PhysArgs& a, const rn_params& P, cudaStream_t s) {
-  k_physics<<<tiles(a.g), NT, physics_smem(a.maxX), s>>>(a, P);
+void launch_physics(const PhysArgs& a, const rn_params& P, int tile, cudaStream_t s) {
+  if (tile == 1) k_physics<Tile1><<<tiles_of<Tile1>(a.g), Tile1::NT, physics_smem_t<Tile1>(a.maxX), s>>>(a, P);
+  else k_physics<Tile0><<<tiles_of<Tile0>(a.g), Tile0::NT, physics_smem_t<Tile0>(a.maxX), s>>>(a, P);
+}
+void launch_batch_stage1(const BatchInst* d, const int* bi, int nb, BatchPhase ph, int tile, cudaStream_t s) {
+  if (tile == 1) k_stage_batch<Tile1, 1><<<nb, Tile1::NT, stage_smem_t<Tile1>(ph.maxX), s>>>(d, bi, ph);
+  else k_stage_batch<Tile0, 1><<<nb, Tile0::NT, stage_smem_t<Tile0>(ph.maxX), s>>>(d, bi, ph);
+}
+void launch_batch_stage2(const BatchInst* d, const int* bi, int nb, BatchPhase ph, int tile, cudaStream_t s) {
+  if (tile == 1) k_stage_batch<Tile1, 2><<<nb, Tile1::NT, stage_smem_t<Tile1>(ph.maxX), s>>>(d, bi, ph);
+  else k_stage_batch<Tile0, 2><<<nb, Tile0::NT, stage_smem_t<Tile0>(ph.maxX), s>>>(d, bi, ph);
+}
+void launch_batch_physics(const BatchInst* d, const int* bi, int nb, BatchPhase ph, int tile, cudaStream_t s) {
+  if (tile == 1) k_physics_batch<Tile1><<<nb, Tile1::NT, physics_smem_t<Tile1>(ph.maxX), s>>>(d, bi, ph);
+  else k_physics_batch<Tile0><<<nb, Tile0::NT, physics_smem_t<Tile0>(ph.maxX), s>>>(d, bi, ph);
 }
 void launch_reduce(const Grid& g, const float4* A, const float4* B, unsigned* w, cudaStream_t s) {
   int N = g.Nx * g.Nr;
-  int blocks = (N + NT - 1) / NT;
+  int blocks = (N + RED_NT - 1) / RED_NT;
   if (blocks > 148 * 8) blocks = 148 * 8;
-  k_reduce<<<blocks, NT, 0, s>>>(g, A, B, w);
+  k_reduce<<<blocks, RED_NT, 0, s>>>(g, A, B, w);
 }
 void launch_rescale(const Grid& g, const float4* A, const float4* B, float4* oA, float4* oB, float fp, float fT,
                     float du, const rn_params& P, cudaStream_t s) {

@@ -29,9 +29,13 @@ EXPORTS = ("rn_create", "rn_destroy", "rn_resize", "rn_set_mask", "rn_set_geomet
            "rn_read_step_info", "rn_request_async", "rn_poll_async", "rn_cancel_async", "rn_spray_set_injector",
            "rn_spray_reset", "rn_spray_stats", "rn_integrals", "rn_sync", "rn_wait", "rn_kernel_launches",
            "rn_set_precision", "rn_get_precision", "rn_get_stream", "rn_profile", "rn_profile_read",
-           "rn_integrals_static",
+           "rn_integrals_static", "rn_set_tile", "rn_get_tile", "rn_autotune", "rn_batch_create",
+           "rn_batch_destroy", "rn_batch_add", "rn_batch_remove", "rn_batch_set_params", "rn_batch_size",
+           "rn_batch_step", "rn_batch_sync", "rn_batch_set_tile", "rn_batch_autotune", "rn_batch_stream",
+           "rn_batch_kernel_launches",
            "rn_last_error")
 PRECISION = {"fast": 0, "exact": 1}
+TILES = {"16x16": 0, "16x8": 1}
 KERNEL_KINDS = ("reduce", "stage1", "stage2", "physics", "parcels", "apply", "other")
 
 
@@ -151,6 +155,21 @@ def lib():
     L.rn_get_precision.argtypes = [H, ctypes.POINTER(i)]
     L.rn_profile.argtypes = [H, i]
     L.rn_profile_read.argtypes = [H, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)]
+    L.rn_set_tile.argtypes = [H, i]
+    L.rn_get_tile.argtypes = [H, ctypes.POINTER(i)]
+    L.rn_autotune.argtypes = [H, ctypes.POINTER(RnParams), i, ctypes.POINTER(i)]
+    L.rn_batch_create.argtypes = [ctypes.POINTER(H)]
+    L.rn_batch_destroy.argtypes = [H]
+    L.rn_batch_add.argtypes = [H, H, ctypes.POINTER(RnParams), ctypes.POINTER(i)]
+    L.rn_batch_remove.argtypes = [H, H]
+    L.rn_batch_set_params.argtypes = [H, H, ctypes.POINTER(RnParams)]
+    L.rn_batch_size.argtypes = [H, ctypes.POINTER(i), ctypes.POINTER(ctypes.c_longlong)]
+    L.rn_batch_step.argtypes = [H, i]
+    L.rn_batch_sync.argtypes = [H]
+    L.rn_batch_set_tile.argtypes = [H, i]
+    L.rn_batch_autotune.argtypes = [H, i, ctypes.POINTER(i)]
+    L.rn_batch_stream.argtypes = [H, ctypes.POINTER(ctypes.c_void_p)]
+    L.rn_batch_kernel_launches.argtypes = [H, ctypes.POINTER(ctypes.c_longlong)]
     L.rn_last_error.restype = ctypes.c_char_p
     for n in EXPORTS[:-1]:
         getattr(L, n).restype = ctypes.c_int
@@ -354,6 +373,24 @@ class GPUSolver:
         _check(lib().rn_get_precision(self.h, ctypes.byref(v)))
         return {b: a for a, b in PRECISION.items()}[v.value]
 
+    def setTile(self, shape):
+        """Tile shape of the stage/physics kernels: '16x16' (default) or '16x8'."""
+        _check(lib().rn_set_tile(self.h, TILES[shape]))
+
+    @property
+    def tile(self):
+        v = ctypes.c_int()
+        _check(lib().rn_get_tile(self.h, ctypes.byref(v)))
+        return {b: a for a, b in TILES.items()}[v.value]
+
+    def autotune(self, P, steps=20):
+        """Time `steps` steps with each tile shape on the current state (which
+        is restored afterwards), keep the fastest and return its name."""
+        p = P if isinstance(P, RnParams) else params_from_P(P)
+        v = ctypes.c_int()
+        _check(lib().rn_autotune(self.h, ctypes.byref(p), int(steps), ctypes.byref(v)))
+        return {b: a for a, b in TILES.items()}[v.value]
+
     def stream(self):
         """The handle's CUDA stream as an integer handle (cudaStream_t)."""
         v = ctypes.c_void_p()
@@ -416,3 +453,81 @@ class GPUSpray:
         r = self.s._readRect
         return {"PA": r(RN_TEX_PARCEL_A, 0, 0, 256, 256), "PB": r(RN_TEX_PARCEL_B, 0, 0, 256, 256),
                 "PC": r(RN_TEX_PARCEL_C, 0, 0, 256, 256)}
+
+
+class SolverBatch:
+    """Steps many GPUSolver handles together: one launch per kernel kind per
+    step covers every tile of every member (no reference counterpart; the
+    reference runs one grid per page). Members share the physics flags and
+    the precision; each keeps its own grid, geometry, state, dt and P."""
+
+    def __init__(self):
+        self.b = ctypes.c_void_p()
+        _check(lib().rn_batch_create(ctypes.byref(self.b)))
+        self.members = []
+
+    def add(self, solver, P):
+        p = P if isinstance(P, RnParams) else params_from_P(P)
+        slot = ctypes.c_int()
+        _check(lib().rn_batch_add(self.b, solver.h, ctypes.byref(p), ctypes.byref(slot)))
+        self.members.append(solver)
+        return slot.value
+
+    def remove(self, solver):
+        _check(lib().rn_batch_remove(self.b, solver.h))
+        self.members.remove(solver)
+
+    def setParams(self, solver, P):
+        p = P if isinstance(P, RnParams) else params_from_P(P)
+        _check(lib().rn_batch_set_params(self.b, solver.h, ctypes.byref(p)))
+
+    def size(self):
+        """(members, cells)"""
+        m, c = ctypes.c_int(), ctypes.c_longlong()
+        _check(lib().rn_batch_size(self.b, ctypes.byref(m), ctypes.byref(c)))
+        return m.value, c.value
+
+    def step(self, n):
+        """n steps of every member, queued on the batch's stream."""
+        _check(lib().rn_batch_step(self.b, int(n)))
+        for s in self.members:
+            s.stepCount += int(n)
+
+    def sync(self):
+        _check(lib().rn_batch_sync(self.b))
+
+    def setTile(self, shape):
+        _check(lib().rn_batch_set_tile(self.b, TILES[shape]))
+
+    def autotune(self, steps=12):
+        """Time `steps` batch steps with each tile shape (member states are
+        restored afterwards), keep the fastest and return its name."""
+        v = ctypes.c_int()
+        _check(lib().rn_batch_autotune(self.b, int(steps), ctypes.byref(v)))
+        return {b: a for a, b in TILES.items()}[v.value]
+
+    @property
+    def tile(self):
+        return {b: a for a, b in TILES.items()}[self.members[0].tile] if self.members else None
+
+    def stream(self):
+        v = ctypes.c_void_p()
+        _check(lib().rn_batch_stream(self.b, ctypes.byref(v)))
+        return v.value or 0
+
+    def kernelLaunches(self):
+        v = ctypes.c_longlong()
+        _check(lib().rn_batch_kernel_launches(self.b, ctypes.byref(v)))
+        return v.value
+
+    def close(self):
+        if self.b.value:
+            lib().rn_batch_destroy(self.b)
+            self.b = ctypes.c_void_p()
+            self.members = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

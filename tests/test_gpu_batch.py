@@ -1,0 +1,206 @@
+"""Tile shapes, the tile autotuner and batched stepping, through librn.so.
+
+None of these change the arithmetic of a cell: every cell and cut-cell group
+computes the same float operations whatever tile or batch block it lands in.
+So in exact precision the results must be bit-identical to single-handle
+stepping with the default tile, and that to the CPU oracle (where the tests
+check it)."""
+import numpy as np
+import pytest
+
+from helpers import run_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def make(rn, s, precision="exact", tile=None):
+    g = rn.GPUSolver(s.Nx, s.Nr)
+    g.setPrecision(precision)
+    if tile:
+        g.setTile(tile)
+    g.setGeometry(s.geo)
+    init = s.initialState()
+    g.setState(init["A"], init["B"])
+    if s.injector is not None:
+        rn.GPUSpray(g).resize()
+        g.spray.setInjector(s.injector)
+    return g
+
+
+def identical(a, b):
+    return np.array_equal(a["A"], b["A"]) and np.array_equal(a["B"], b["B"])
+
+
+def setups(rn, kind, sizes):
+    from rocket_nozzle_cfd_solver_b200 import configs
+    f = {"plain": configs.plain_small, "viscous": configs.viscous_plume, "spray": configs.injector_spray}[kind]
+    return [rn.build_sim_setup(f(Nx, Nr)[0]) for Nx, Nr in sizes]
+
+
+@pytest.mark.parametrize("kind", ["plain", "viscous"])
+def test_tile_shapes_bit_identical(rn, oracle, kind):
+    s = setups(rn, kind, [(160, 60)])[0]
+    outs = []
+    for tile in ("16x16", "16x8"):
+        g = make(rn, s, tile=tile)
+        assert g.tile == tile
+        g.step(40, s.P)
+        outs.append((g.readAll(), g.readStepInfo()))
+        g.close()
+    assert identical(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+    assert identical(outs[0][0], run_oracle(oracle, s, 40).readAll())
+
+
+def test_fast_tile_shapes_agree(rn):
+    s = setups(rn, "viscous", [(256, 96)])[0]
+    outs = []
+    for tile in ("16x16", "16x8"):
+        g = make(rn, s, precision="fast", tile=tile)
+        g.step(60, s.P)
+        outs.append(g.readAll())
+        g.close()
+    assert identical(outs[0], outs[1])
+
+
+def test_autotune_restores_state(rn):
+    s = setups(rn, "spray", [(128, 48)])[0]
+    g = make(rn, s)
+    ref = make(rn, s)
+    g.step(12, s.P)
+    ref.step(12, s.P)
+    before, si = g.readAll(), g.readStepInfo()
+    launches = g.kernelLaunches()
+    chosen = g.autotune(s.P, steps=4)
+    assert chosen in ("16x16", "16x8") and g.tile == chosen
+    assert identical(g.readAll(), before) and np.array_equal(g.readStepInfo(), si)
+    assert g.kernelLaunches() == launches
+    g.step(9, s.P)
+    ref.step(9, s.P)
+    assert identical(g.readAll(), ref.readAll())
+    assert np.array_equal(g.spray.readParcels()["PA"], ref.spray.readParcels()["PA"])
+    g.close()
+    ref.close()
+
+
+@pytest.mark.parametrize("kind,sizes,calls", [
+    ("plain", [(96, 36), (160, 60), (256, 96)], [13, 5, 1, 6]),
+    ("viscous", [(128, 48), (200, 76)], [7, 6, 12]),
+    ("spray", [(128, 48), (96, 36)], [5, 4]),
+])
+def test_batch_matches_single_handles(rn, kind, sizes, calls):
+    """Members of uneven sizes, call lengths that start and end inside the
+    6-step graph period: every member ends bit-identical to a handle stepped
+    on its own."""
+    ss = setups(rn, kind, sizes)
+    batch = rn.SolverBatch()
+    members = [make(rn, s) for s in ss]
+    singles = [make(rn, s) for s in ss]
+    for g, s in zip(members, ss):
+        batch.add(g, s.P)
+    assert batch.size() == (len(ss), sum(s.Nx * s.Nr for s in ss))
+    for n in calls:
+        batch.step(n)
+        for g, s in zip(singles, ss):
+            g.step(n, s.P)
+        # reads in between go through the member handles
+        for g, h in zip(members, singles):
+            assert identical(g.readAll(), h.readAll())
+            assert np.array_equal(g.readStepInfo(), h.readStepInfo())
+    if kind == "spray":
+        for g, h in zip(members, singles):
+            assert np.array_equal(g.spray.readParcels()["PB"], h.spray.readParcels()["PB"])
+    batch.close()
+    for g in members + singles:
+        g.close()
+
+
+def test_batch_member_leaves_and_steps_alone(rn):
+    ss = setups(rn, "plain", [(96, 36), (128, 48)])
+    batch = rn.SolverBatch()
+    a, b = make(rn, ss[0]), make(rn, ss[1])
+    ref = make(rn, ss[1])
+    batch.add(a, ss[0].P)
+    batch.add(b, ss[1].P)
+    batch.step(8)
+    with pytest.raises(rn.RnError):
+        b.step(1, ss[1].P)                                  # stepped by the batch
+    batch.remove(b)
+    b.step(5, ss[1].P)
+    ref.step(13, ss[1].P)
+    assert identical(b.readAll(), ref.readAll())
+    # rescale a member between batch steps: the batch picks up its new ring slot
+    a2 = make(rn, ss[0])
+    a2.step(8, ss[0].P)
+    a.rescaleAmbient(0.9, 1.0, 0.0, ss[0].P)
+    a2.rescaleAmbient(0.9, 1.0, 0.0, ss[0].P)
+    batch.step(7)
+    a2.step(7, ss[0].P)
+    assert identical(a.readAll(), a2.readAll())
+    batch.close()
+    for g in (a, b, ref, a2):
+        g.close()
+
+
+def test_batch_rejects_mismatched_members(rn):
+    plain = setups(rn, "plain", [(96, 36)])[0]
+    visc = setups(rn, "viscous", [(96, 36)])[0]
+    batch = rn.SolverBatch()
+    a = make(rn, plain)
+    batch.add(a, plain.P)
+    v = make(rn, visc)
+    with pytest.raises(rn.RnError):
+        batch.add(v, visc.P)                                # flags differ
+    f = make(rn, plain, precision="fast")
+    with pytest.raises(rn.RnError):
+        batch.add(f, plain.P)                               # precision differs
+    with pytest.raises(rn.RnError):
+        batch.add(a, plain.P)                               # already a member
+    batch.close()
+    for g in (a, v, f):
+        g.close()
+
+
+def test_batch_launches_and_tile(rn, oracle):
+    ss = setups(rn, "plain", [(96, 36), (160, 60)])
+    batch = rn.SolverBatch()
+    gs = [make(rn, s) for s in ss]
+    for g, s in zip(gs, ss):
+        batch.add(g, s.P)
+    batch.setTile("16x8")
+    assert all(g.tile == "16x8" for g in gs)
+    n0 = batch.kernelLaunches()
+    batch.step(20)
+    batch.sync()
+    assert batch.kernelLaunches() - n0 == 2 * 20             # stage 1 + stage 2 for every member at once
+    for g, s in zip(gs, ss):
+        assert identical(g.readAll(), run_oracle(oracle, s, 20).readAll())
+    batch.close()
+    for g in gs:
+        g.close()
+
+
+def test_batch_autotune_restores_members(rn):
+    ss = setups(rn, "viscous", [(128, 48), (256, 96), (96, 36)])
+    batch = rn.SolverBatch()
+    members = [make(rn, s) for s in ss]
+    singles = [make(rn, s) for s in ss]
+    for g, s in zip(members, ss):
+        batch.add(g, s.P)
+    batch.step(5)
+    for g, s in zip(singles, ss):
+        g.step(5, s.P)
+    snaps = [(g.readAll(), g.readStepInfo()) for g in members]
+    n0 = batch.kernelLaunches()
+    chosen = batch.autotune(steps=6)
+    assert chosen in ("16x16", "16x8") and batch.tile == chosen
+    assert batch.kernelLaunches() == n0
+    for g, (st, si) in zip(members, snaps):
+        assert identical(g.readAll(), st) and np.array_equal(g.readStepInfo(), si)
+    batch.step(7)
+    for g, s in zip(singles, ss):
+        g.step(7, s.P)
+    for g, h in zip(members, singles):
+        assert identical(g.readAll(), h.readAll())
+    batch.close()
+    for g in members + singles:
+        g.close()
