@@ -283,9 +283,14 @@ def run_ours(args, rank, world, local_rank):
     g.close()
     del flush
     torch.cuda.empty_cache()
-    batched = None
+    batched = serving = large = None
+    if world == 1 and not args.no_large:
+        large = run_large_grid(args)
+        torch.cuda.empty_cache()
     if world == 1 and args.batch_instances > 0:
         batched = run_batched(args, local_rank)
+    if world == 1 and args.serve_requests > 0:
+        serving = run_serving(args)
 
     if rank != 0:
         return
@@ -305,7 +310,8 @@ def run_ours(args, rank, world, local_rank):
             "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "exit_thrust_N": perf["F"] if perf else None},
             "steady_state_value": steady,
-            "gpu_launches": launches, "clocks": clk.summary(), "batched": batched}
+            "gpu_launches": launches, "clocks": clk.summary(), "large_grid": large,
+            "batched": batched, "serving": serving}
     print(json.dumps(line), flush=True)
 
 
@@ -386,7 +392,11 @@ def run_batched(args, local_rank):
     sizes = {}
     for s in setups:
         sizes[f"{s.Nx}x{s.Nr}"] = sizes.get(f"{s.Nx}x{s.Nr}", 0) + 1
+    peak, src = measured_peak()
+    bpc = BYTES_PER_CELL["stage1"] + BYTES_PER_CELL["stage2"] + BYTES_PER_CELL["physics"]
     return {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "instances": len(setups),
+            "achieved_gbs": value * bpc / 1e9, "bytes_per_cell_step": bpc, "frac": value * bpc / 1e9 / peak,
+            "peak_source": src,
             "cells": cells, "grids": sizes, "solver_steps_per_bench_step": nsteps, "steps": args.steps,
             "ms_per_step": ms / args.steps, "tile": tile, "gpu_launches": launches,
             "launches_per_solver_step": launches / (nsteps * args.steps),
@@ -394,6 +404,125 @@ def run_batched(args, local_rank):
                               cells * nsteps * rounds / single_wall, "rounds": rounds},
             "speedup_vs_one_at_a_time": value / single, "fp64_readouts_finite": finite,
             "setup_s": t_setup, "l2": "state ~1 GB > L2: no flush"}
+
+
+def run_large_grid(args):
+    """HBM-resident sweep point: the plain cold-gas nozzle on a 4096 x 1536
+    grid (6.3 M cells; one state copy is 201 MB, beyond the 126 MB L2), two
+    kernels per step. Achieved GB/s = algorithmic bytes per cell-step (258 B:
+    stage 1 reads 32 + 49, writes 32; stage 2 reads 32 + 32 + 49, writes 32)
+    x cell-steps/s, device time from CUDA events."""
+    import torch
+    rn = ge.load_package()
+    from rocket_nozzle_cfd_solver_b200.configs import plain_small
+    s = rn.build_sim_setup(plain_small(4096, 1536)[0])
+    g = rn.GPUSolver(s.Nx, s.Nr)
+    g.setGeometry(s.geo)
+    init = s.initialState()
+    g.setState(init["A"], init["B"])
+    p = rn.params_from_P(s.P)
+    stream = torch.cuda.ExternalStream(g.stream())
+    n = 20
+    for _ in range(max(args.warmup, 1)):
+        g.step(n, p)
+    g.sync()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    g.profile(True)
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            evs[k][0].record(stream)
+        g.step(n, p)
+        with torch.cuda.stream(stream):
+            evs[k][1].record(stream)
+    g.sync()
+    prof = g.profileRead()
+    g.profile(False)
+    ms = sum(a.elapsed_time(b) for a, b in evs)
+    cells = s.Nx * s.Nr
+    rate = cells * n * args.steps / (ms * 1e-3)
+    peak, src = measured_peak()
+    bpc = BYTES_PER_CELL["stage1"] + BYTES_PER_CELL["stage2"]
+    kern = {}
+    for k in ("stage1", "stage2"):
+        kms, kn = prof[k]
+        if kn:
+            gbs = BYTES_PER_CELL[k] * cells / (kms / kn * 1e-3) / 1e9
+            kern[k] = {"avg_launch_us": 1e3 * kms / kn, "achieved_gbs": gbs, "frac": gbs / peak}
+    g.close()
+    return {"workload": "plain cold-gas nozzle 4096x1536 (inviscid, 2 kernels per step)", "cells": cells,
+            "value": rate, "unit": "cell-updates/s", "bytes_per_cell_step": bpc,
+            "achieved_gbs": rate * bpc / 1e9, "peak_gbs": peak, "peak_source": src,
+            "frac": rate * bpc / 1e9 / peak, "kernels": kern}
+
+
+def serving_requests(rn, count, seed=7, spray_frac=0.2):
+    """Seeded serving workload: nozzles drawn as in the batched workload; a
+    fraction are injector chambers with the spray (their parcel ring spawns
+    from the injector, 4 parcels per step, as the reference does)."""
+    from rocket_nozzle_cfd_solver_b200 import configs
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        if rng.uniform() < spray_frac:
+            Nx, Nr = configs.BATCH_SIZES[int(rng.integers(len(configs.BATCH_SIZES)))]
+            out.append(("spray", rn.build_sim_setup(configs.injector_spray(Nx, Nr)[0])))
+        else:
+            out.append(("nozzle", rn.build_sim_setup(configs.batched_instance(rng))))
+    return out
+
+
+def serve_once(rn, reqs, arrivals, max_active, check_every, drop, t_end_s):
+    """Submits reqs at their arrival times (s) to a SolveServer; returns the results."""
+    srv = rn.SolveServer(max_active=max_active, check_every=check_every)
+    ids = []
+    t0 = time.perf_counter()
+    for (kind, s), ta in zip(reqs, arrivals):
+        delay = ta - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        ids.append(srv.submit(s, drop=drop, t_end_s=t_end_s))
+    res = [srv.wait(i, timeout_s=1800) for i in ids]
+    st = srv.stats()
+    srv.close()
+    return res, st
+
+
+def latency_summary(res):
+    lat = np.array([r["latency_ms"] for r in res])
+    span = max(r["done_ms"] for r in res) - min(r["submit_ms"] for r in res)
+    return {"solves_per_s": len(res) / (span * 1e-3), "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "makespan_s": span * 1e-3}
+
+
+def run_serving(args):
+    """Serving: Poisson arrivals of whole solves (stop at a density-residual
+    drop of 1e-4 or 2 ms of simulated time) into the continuous-batching
+    SolveServer, against the same arrivals served one solve at a time
+    (max_active=1, the plain form)."""
+    rn = ge.load_package()
+    t0 = time.perf_counter()
+    reqs = serving_requests(rn, args.serve_requests)
+    t_setup = time.perf_counter() - t0
+    rng = np.random.default_rng(11)
+    rate = args.serve_rate
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
+    arrivals -= arrivals[0]
+    K, drop, t_end = 60, 1e-4, 2e-3
+    served, st = serve_once(rn, reqs, arrivals, 0, K, drop, t_end)
+    plain, _ = serve_once(rn, reqs, arrivals, 1, K, drop, t_end)
+    same = all(a["integrals"] == b["integrals"] and a["steps"] == b["steps"] for a, b in zip(served, plain))
+    status = {}
+    for r in served:
+        status[r["status"]] = status.get(r["status"], 0) + 1
+    cells = sum(s.Nx * s.Nr * r["steps"] for (_, s), r in zip(reqs, served))
+    sv, pl = latency_summary(served), latency_summary(plain)
+    return {"metric": "solves/s", "value": sv["solves_per_s"], "unit": "solves/s", "rate_per_s": rate,
+            "requests": len(reqs), "spray_requests": sum(1 for k, _ in reqs if k == "spray"),
+            "stop": "density residual drop 1e-4 or 2 ms simulated", "check_every": K,
+            "p50_ms": sv["p50_ms"], "p99_ms": sv["p99_ms"], "makespan_s": sv["makespan_s"],
+            "cell_updates_per_s": cells / sv["makespan_s"], "status": status, "ticks": st["ticks"],
+            "one_at_a_time": pl, "speedup_solves_per_s": sv["solves_per_s"] / pl["solves_per_s"],
+            "results_identical_in_mix_and_alone": same, "setup_s": t_setup}
 
 
 def main():
@@ -406,6 +535,9 @@ def main():
     ap.add_argument("--batch-instances", type=int, default=64,
                     help="instances of the batched workload measured after the main line's (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=30, help="time steps per batched bench step")
+    ap.add_argument("--no-large", action="store_true", help="skip the 4096x1536 HBM-resident sweep point")
+    ap.add_argument("--serve-requests", type=int, default=24, help="requests of the serving leg (0: skip)")
+    ap.add_argument("--serve-rate", type=float, default=5.0, help="Poisson arrival rate of the serving leg (1/s)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

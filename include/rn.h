@@ -205,6 +205,85 @@ int rn_batch_stream(rn_batch b, void** stream);
 /* number of kernels the batch has launched (graph replays included) */
 int rn_batch_kernel_launches(rn_batch b, long long* out);
 
+/* Steady-state residual (no reference counterpart: the reference has no
+ * convergence measure). rn_residual_mark snapshots the current A plane and
+ * step info on the device (allocating the snapshot on first use);
+ * rn_residual returns in FP64, for each component c of A = (rho, rho u,
+ * rho v, E), the RMS over fluid cells of (A_c - A_c at the mark) / (t - t_mark):
+ * out[0..3], with out[4] = t - t_mark and out[5] = the fluid-cell count. With
+ * one step between the two calls this is the L2 norm of dU/dt of that step.
+ * Deterministic (fixed reduction order); blocks until out is filled. */
+int rn_residual_mark(rn_handle h);
+int rn_residual(rn_handle h, double out[6]);
+
+/* Solve server: continuous batching of whole solves on one GPU (no
+ * reference counterpart; the reference runs one interactive solve per page).
+ * rn_serve_submit copies a request (grid, geometry, initial state, P, stop
+ * criteria) into the arrival queue and returns its id at once. A worker thread
+ * admits queued requests in arrival order while their device bytes
+ * (rn_solve_bytes) fit in the budget, adds each to the batch of its physics
+ * class (visc, chem, inj; classes run on separate streams and overlap), steps
+ * every batch check_every steps per tick, and evaluates each solve's FP64
+ * density residual (rn_residual over the tick's last step) and time after the
+ * tick. A solve whose residual fell to drop x its first value, whose time
+ * reached t_end or whose steps reached max_steps (tested in that order, at
+ * tick granularity) gets its FP64 read-outs and final state copied out and
+ * frees its memory, which admits later arrivals. A solve's result does not
+ * depend on what else is in the mix. */
+typedef struct rn_server_t* rn_server;
+typedef struct {
+  size_t hbm_budget;   /* device bytes admitted solves may hold; 0 = 80 % of the free memory at creation */
+  int max_active;      /* most solves on the device at once; 0 = limited by the budget only */
+  int check_every;     /* steps per tick (>= 2) */
+  int precision;       /* RN_PRECISION_* of every solve */
+  int tile;            /* RN_TILE_* of the class batches */
+} rn_server_opts;
+typedef struct {
+  int Nx, Nr;
+  const uint8_t* mask;              /* as rn_set_geometry */
+  const float* geoA;
+  const float* geoG;
+  const float* geoM;
+  const float* jWall;               /* or NULL */
+  const float* A;                   /* initial state, as rn_set_state */
+  const float* B;
+  const float* injTab;              /* 256 x 3 float4 when P.inj, else NULL */
+  rn_params P;
+  rn_integral_spec spec;            /* read-out columns for the result */
+  double drop;                      /* density-residual drop that ends the solve (0: off) */
+  double t_end;                     /* normalised time that ends the solve (0: off) */
+  long long max_steps;              /* step count that ends the solve (0: off) */
+} rn_solve_request;
+#define RN_SOLVE_CONVERGED 0
+#define RN_SOLVE_TIME 1
+#define RN_SOLVE_MAX_STEPS 2
+#define RN_SOLVE_REJECTED (-1)      /* needs more than the whole budget */
+#define RN_SOLVE_FAILED (-2)
+typedef struct {
+  int status;                       /* RN_SOLVE_* */
+  int pad_;
+  long long steps;
+  double t, residual0, residual;    /* final normalised time; first and last density residual */
+  double submit_ms, admit_ms, done_ms;   /* server clock, ms since rn_server_create */
+  rn_integrals_out integrals;       /* FP64 read-outs of the final state */
+} rn_solve_result;
+typedef struct {
+  long long queued, active, finished, bytes_used, bytes_budget, ticks, admitted, failed;
+} rn_serve_status;
+int rn_server_default_opts(rn_server_opts* opts);
+int rn_server_create(const rn_server_opts* opts, rn_server* out);
+/* stops the worker after its current tick; unfinished solves are dropped */
+int rn_server_destroy(rn_server s);
+int rn_serve_submit(rn_server s, const rn_solve_request* req, long long* id);
+/* RN_NOT_READY until request id has finished; then fills res and, if not
+ * NULL, the final state planes (Nx*Nr*4 floats each), and forgets the id */
+int rn_serve_poll(rn_server s, long long id, rn_solve_result* res, float* A, float* B);
+/* rn_serve_poll after waiting up to timeout_ms for the request to finish */
+int rn_serve_wait(rn_server s, long long id, int timeout_ms, rn_solve_result* res, float* A, float* B);
+int rn_serve_stats(rn_server s, rn_serve_status* out);
+/* device bytes the server charges a solve of an Nx x Nr grid against its budget */
+int rn_solve_bytes(int Nx, int Nr, long long* bytes);
+
 /* the handle's CUDA stream (a cudaStream_t), so a caller can order its own
  * work (timing events, cache flushes) with the handle's kernels */
 int rn_get_stream(rn_handle h, void** stream);

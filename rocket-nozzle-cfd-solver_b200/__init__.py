@@ -7,4 +7,4 @@ library ``librn.so`` (declared in ``include/rn.h``). ``GPUSolver`` and
 """
 from . import physics, cutcell, simsetup  # noqa: F401
 from .simsetup import build_sim_setup, compute_params, exit_performance, cell_prim_si  # noqa: F401
-from .solver import GPUSolver, GPUSpray, SolverBatch, RnError, params_from_P  # noqa: F401
+from .solver import GPUSolver, GPUSpray, SolverBatch, SolveServer, RnError, params_from_P  # noqa: F401

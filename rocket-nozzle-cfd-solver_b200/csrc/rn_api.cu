@@ -15,6 +15,7 @@
 #include <string>
 #include <thread>
 #include <algorithm>
+#include <mutex>
 #include <vector>
 #include "rn.h"
 #include "rn_internal.h"
@@ -58,6 +59,9 @@ void free_buffers(rn_solver* h) {
   cudaFree(h->src); cudaFree(h->tab); cudaFree(h->dep); cudaFree(h->key); cudaFree(h->sortTemp);
   cudaFree(h->xoff); cudaFree(h->xcell);
   h->xoff = h->xcell = nullptr;
+  cudaFree(h->mark); cudaFree(h->dRes);
+  h->mark = h->markSt = nullptr;
+  h->dRes = nullptr;
   h->maxX = 1;
   h->geoA = h->geoG = h->geoM = h->jw = h->wallRow = nullptr;
   h->mask = nullptr; h->stepTex = nullptr; h->wmax = nullptr; h->dInt = nullptr;
@@ -261,15 +265,21 @@ int rn_create(int Nx, int Nr, rn_handle* out) {
   if (e != cudaSuccess) { delete h; return cuda_fail(e, "cudaStreamCreate"); }
   e = cudaEventCreateWithFlags(&h->asyncEv, cudaEventDisableTiming);
   if (e != cudaSuccess) { cudaStreamDestroy(h->stream); delete h; return cuda_fail(e, "cudaEventCreate"); }
-  static bool kernels_ready = false;
-  if (!kernels_ready) {
-    if (kernels_exact.init() != 0 || kernels_fast.init() != 0) {
-      cudaEventDestroy(h->asyncEv);
-      cudaStreamDestroy(h->stream);
-      delete h;
-      return fail(RN_ERR_CUDA, "rn_create: cannot size the stage kernels' shared memory");
+  {
+    // process-wide kernel attributes, once (the solve server creates handles
+    // on its worker thread while callers may create their own)
+    static std::mutex initMu;
+    static bool kernels_ready = false;
+    std::lock_guard<std::mutex> lk(initMu);
+    if (!kernels_ready) {
+      if (kernels_exact.init() != 0 || kernels_fast.init() != 0) {
+        cudaEventDestroy(h->asyncEv);
+        cudaStreamDestroy(h->stream);
+        delete h;
+        return fail(RN_ERR_CUDA, "rn_create: cannot size the stage kernels' shared memory");
+      }
+      kernels_ready = true;
     }
-    kernels_ready = true;
   }
   int rc = alloc_buffers(h, Nx, Nr);
   if (rc != RN_OK) {

@@ -54,6 +54,10 @@ struct rn_solver {
   std::vector<float> hostGeoM;
   // kernels of the selected precision (rn_set_precision)
   const rn::KernelSet* K = &rn::kernels_fast;
+  // residual snapshot (A plane + step info) and FP64 scratch (rn_readout.cu)
+  float4* mark = nullptr;
+  float4* markSt = nullptr;
+  double* dRes = nullptr;
   // the batch this handle is stepped by, if any (rn_batch.cu)
   struct rn_batch_t* batch = nullptr;
 
@@ -69,6 +73,11 @@ int rn_build_member_lists(rn_solver* h);
 int rn_ensure_wave_speed(rn_solver* h);
 // Takes h out of its batch, if any (rn_batch.cu).
 void rn_batch_detach(rn_solver* h);
+// Residual of the current state against the mark, into h->dRes[0..5], and the
+// mark itself, queued on `stream` (rn_readout.cu); device bytes they hold.
+int rn_residual_launch(rn_solver* h, cudaStream_t stream);
+int rn_residual_mark_on(rn_solver* h, cudaStream_t stream);
+size_t rn_residual_bytes(int Nx, int Nr);
 
 #define RN_CK(call)                                            \
   do {                                                         \

@@ -32,7 +32,9 @@ EXPORTS = ("rn_create", "rn_destroy", "rn_resize", "rn_set_mask", "rn_set_geomet
            "rn_integrals_static", "rn_set_tile", "rn_get_tile", "rn_autotune", "rn_batch_create",
            "rn_batch_destroy", "rn_batch_add", "rn_batch_remove", "rn_batch_set_params", "rn_batch_size",
            "rn_batch_step", "rn_batch_sync", "rn_batch_set_tile", "rn_batch_autotune", "rn_batch_stream",
-           "rn_batch_kernel_launches",
+           "rn_batch_kernel_launches", "rn_residual_mark", "rn_residual", "rn_server_default_opts",
+           "rn_server_create", "rn_server_destroy", "rn_serve_submit", "rn_serve_poll", "rn_serve_wait",
+           "rn_serve_stats", "rn_solve_bytes",
            "rn_last_error")
 PRECISION = {"fast": 0, "exact": 1}
 TILES = {"16x16": 0, "16x8": 1}
@@ -78,6 +80,49 @@ class RnIntegralSpec(ctypes.Structure):
 class RnIntegralsOut(ctypes.Structure):
     _fields_ = [(n, ctypes.c_double) for n in ("F", "mdot", "Mw", "pw", "A", "throat_mdot", "throat_mO",
                                                "throat_mF", "chamber_p", "chamber_T", "dt", "t")]
+
+
+class RnServerOpts(ctypes.Structure):
+    _fields_ = [("hbm_budget", ctypes.c_size_t), ("max_active", ctypes.c_int), ("check_every", ctypes.c_int),
+                ("precision", ctypes.c_int), ("tile", ctypes.c_int)]
+
+
+class RnSolveRequest(ctypes.Structure):
+    _fields_ = [("Nx", ctypes.c_int), ("Nr", ctypes.c_int), ("mask", ctypes.c_void_p), ("geoA", ctypes.c_void_p),
+                ("geoG", ctypes.c_void_p), ("geoM", ctypes.c_void_p), ("jWall", ctypes.c_void_p),
+                ("A", ctypes.c_void_p), ("B", ctypes.c_void_p), ("injTab", ctypes.c_void_p), ("P", RnParams),
+                ("spec", RnIntegralSpec), ("drop", ctypes.c_double), ("t_end", ctypes.c_double),
+                ("max_steps", ctypes.c_longlong)]
+
+
+class RnSolveResult(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("pad_", ctypes.c_int), ("steps", ctypes.c_longlong),
+                ("t", ctypes.c_double), ("residual0", ctypes.c_double), ("residual", ctypes.c_double),
+                ("submit_ms", ctypes.c_double), ("admit_ms", ctypes.c_double), ("done_ms", ctypes.c_double),
+                ("integrals", RnIntegralsOut)]
+
+
+class RnServeStatus(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_longlong) for n in ("queued", "active", "finished", "bytes_used", "bytes_budget",
+                                                  "ticks", "admitted", "failed")]
+
+
+SOLVE_STATUS = {0: "converged", 1: "time", 2: "max_steps", -1: "rejected", -2: "failed"}
+
+
+def integral_spec(setup):
+    """rn_integral_spec of a setup from build_sim_setup: the exit and throat
+    columns, the chamber probe and the gas constants of the read-outs."""
+    P = setup["P"]
+    s = RnIntegralSpec()
+    s.iExit, s.jExit, s.iThroat, s.iChamber = setup["iExit"], setup["jExit"], setup["iThroat"], setup["iChamber"]
+    s.dx = setup["dx"]
+    s.pAmb = P["amb"][3]
+    for k in range(3):
+        s.Rs[k] = P["Rs"][k]
+    s.RaN = P["RaN"]
+    s.inj = 1 if P["inj"] else 0
+    return s
 
 
 def params_from_P(P):
@@ -170,6 +215,18 @@ def lib():
     L.rn_batch_autotune.argtypes = [H, i, ctypes.POINTER(i)]
     L.rn_batch_stream.argtypes = [H, ctypes.POINTER(ctypes.c_void_p)]
     L.rn_batch_kernel_launches.argtypes = [H, ctypes.POINTER(ctypes.c_longlong)]
+    L.rn_residual_mark.argtypes = [H]
+    L.rn_residual.argtypes = [H, ctypes.POINTER(ctypes.c_double)]
+    L.rn_server_default_opts.argtypes = [ctypes.POINTER(RnServerOpts)]
+    L.rn_server_create.argtypes = [ctypes.POINTER(RnServerOpts), ctypes.POINTER(H)]
+    L.rn_server_destroy.argtypes = [H]
+    L.rn_serve_submit.argtypes = [H, ctypes.POINTER(RnSolveRequest), ctypes.POINTER(ctypes.c_longlong)]
+    L.rn_serve_poll.argtypes = [H, ctypes.c_longlong, ctypes.POINTER(RnSolveResult), ctypes.c_void_p,
+                                ctypes.c_void_p]
+    L.rn_serve_wait.argtypes = [H, ctypes.c_longlong, i, ctypes.POINTER(RnSolveResult), ctypes.c_void_p,
+                                ctypes.c_void_p]
+    L.rn_serve_stats.argtypes = [H, ctypes.POINTER(RnServeStatus)]
+    L.rn_solve_bytes.argtypes = [i, i, ctypes.POINTER(ctypes.c_longlong)]
     L.rn_last_error.restype = ctypes.c_char_p
     for n in EXPORTS[:-1]:
         getattr(L, n).restype = ctypes.c_int
@@ -341,18 +398,20 @@ class GPUSolver:
     def integrals(self, setup):
         """FP64 exit/throat/chamber read-outs (rn_integrals) in the reference's
         normalised units, for ``setup`` from build_sim_setup."""
-        P = setup["P"]
-        s = RnIntegralSpec()
-        s.iExit, s.jExit, s.iThroat, s.iChamber = setup["iExit"], setup["jExit"], setup["iThroat"], setup["iChamber"]
-        s.dx = setup["dx"]
-        s.pAmb = P["amb"][3]
-        for k in range(3):
-            s.Rs[k] = P["Rs"][k]
-        s.RaN = P["RaN"]
-        s.inj = 1 if P["inj"] else 0
         o = RnIntegralsOut()
-        _check(lib().rn_integrals(self.h, ctypes.byref(s), ctypes.byref(o)))
+        _check(lib().rn_integrals(self.h, ctypes.byref(integral_spec(setup)), ctypes.byref(o)))
         return {n: getattr(o, n) for n, _ in RnIntegralsOut._fields_}
+
+    def residualMark(self):
+        """Snapshot the current state for residual()."""
+        _check(lib().rn_residual_mark(self.h))
+
+    def residual(self):
+        """FP64 RMS of dU/dt since residualMark() over fluid cells:
+        {rho, rhou, rhov, E, span, cells}."""
+        out = (ctypes.c_double * 6)()
+        _check(lib().rn_residual(self.h, out))
+        return dict(zip(("rho", "rhou", "rhov", "E", "span", "cells"), list(out)))
 
     def sync(self):
         _check(lib().rn_sync(self.h))
@@ -508,7 +567,7 @@ class SolverBatch:
 
     @property
     def tile(self):
-        return {b: a for a, b in TILES.items()}[self.members[0].tile] if self.members else None
+        return self.members[0].tile if self.members else None
 
     def stream(self):
         v = ctypes.c_void_p()
@@ -525,6 +584,111 @@ class SolverBatch:
             lib().rn_batch_destroy(self.b)
             self.b = ctypes.c_void_p()
             self.members = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SolveServer:
+    """Continuous batching of whole solves on one GPU (rn_server_*): submit
+    setups from build_sim_setup with stop criteria, collect results with their
+    FP64 read-outs, latencies and (optionally) final states. No reference
+    counterpart: the reference runs one interactive solve per page."""
+
+    def __init__(self, budget_bytes=0, max_active=0, check_every=60, precision="fast", tile="16x16"):
+        o = RnServerOpts()
+        _check(lib().rn_server_default_opts(ctypes.byref(o)))
+        o.hbm_budget = int(budget_bytes)
+        o.max_active = int(max_active)
+        o.check_every = int(check_every)
+        o.precision = PRECISION[precision]
+        o.tile = TILES[tile]
+        self.s = ctypes.c_void_p()
+        _check(lib().rn_server_create(ctypes.byref(o), ctypes.byref(self.s)))
+        self.shapes = {}
+
+    @staticmethod
+    def solve_bytes(Nx, Nr):
+        v = ctypes.c_longlong()
+        _check(lib().rn_solve_bytes(int(Nx), int(Nr), ctypes.byref(v)))
+        return v.value
+
+    def submit(self, setup, drop=1e-4, t_end_s=2e-3, max_steps=0, state=None):
+        """Queue a solve of ``setup`` from its initial state (or ``state``);
+        stop at a density-residual drop of ``drop``, ``t_end_s`` seconds of
+        simulated time or ``max_steps`` steps. Returns the request id."""
+        s = setup
+        N, NF = s.Nx * s.Nr, (s.Nx + 1) * (s.Nr + 1)
+        geo = s.geo
+        keep = [np.ascontiguousarray(geo["mask"], dtype=np.uint8), _f32(geo["geoA"], NF * 4),
+                _f32(geo["geoG"], N * 4), _f32(geo["geoM"], N * 4)]
+        jw = geo.get("jWall")
+        keep.append(_f32(jw, s.Nx * 4) if jw is not None else None)
+        init = state if state is not None else s.initialState()
+        keep += [_f32(init["A"], N * 4), _f32(init["B"], N * 4)]
+        tab = None
+        if s.P["inj"]:
+            tab = _f32(s.injector["tab"], 256 * 3 * 4)
+        keep.append(tab)
+        r = RnSolveRequest()
+        r.Nx, r.Nr = s.Nx, s.Nr
+        for name, a in zip(("mask", "geoA", "geoG", "geoM", "jWall", "A", "B", "injTab"), keep):
+            setattr(r, name, a.ctypes.data if a is not None else None)
+        r.P = params_from_P(s.P)
+        r.spec = integral_spec(s)
+        r.drop = float(drop or 0.0)
+        r.t_end = float(t_end_s) / float(s.tScale) if t_end_s else 0.0
+        r.max_steps = int(max_steps or 0)
+        rid = ctypes.c_longlong()
+        _check(lib().rn_serve_submit(self.s, ctypes.byref(r), ctypes.byref(rid)))
+        self.shapes[rid.value] = (s.Nx, s.Nr)
+        return rid.value
+
+    def _result(self, rid, res, A, B, state):
+        out = {"id": rid, "status": SOLVE_STATUS.get(res.status, res.status), "steps": res.steps, "t": res.t,
+               "residual0": res.residual0, "residual": res.residual, "submit_ms": res.submit_ms,
+               "admit_ms": res.admit_ms, "done_ms": res.done_ms,
+               "latency_ms": res.done_ms - res.submit_ms,
+               "integrals": {n: getattr(res.integrals, n) for n, _ in RnIntegralsOut._fields_}}
+        if state:
+            out["A"], out["B"] = A, B
+        self.shapes.pop(rid, None)
+        return out
+
+    def _bufs(self, rid, state):
+        if not state:
+            return None, None
+        Nx, Nr = self.shapes[rid]
+        return np.empty(Nx * Nr * 4, np.float32), np.empty(Nx * Nr * 4, np.float32)
+
+    def poll(self, rid, state=False):
+        """The result of request ``rid`` once it has finished, else None."""
+        A, B = self._bufs(rid, state)
+        res = RnSolveResult()
+        rc = _check(lib().rn_serve_poll(self.s, int(rid), ctypes.byref(res), A.ctypes.data if state else None,
+                                        B.ctypes.data if state else None), (RN_OK, RN_NOT_READY))
+        return None if rc == RN_NOT_READY else self._result(rid, res, A, B, state)
+
+    def wait(self, rid, timeout_s=600.0, state=False):
+        A, B = self._bufs(rid, state)
+        res = RnSolveResult()
+        rc = _check(lib().rn_serve_wait(self.s, int(rid), int(timeout_s * 1000), ctypes.byref(res),
+                                        A.ctypes.data if state else None, B.ctypes.data if state else None),
+                    (RN_OK, RN_NOT_READY))
+        return None if rc == RN_NOT_READY else self._result(rid, res, A, B, state)
+
+    def stats(self):
+        st = RnServeStatus()
+        _check(lib().rn_serve_stats(self.s, ctypes.byref(st)))
+        return {n: getattr(st, n) for n, _ in RnServeStatus._fields_}
+
+    def close(self):
+        if self.s.value:
+            lib().rn_server_destroy(self.s)
+            self.s = ctypes.c_void_p()
 
     def __del__(self):
         try:

@@ -46,6 +46,11 @@ int main(void) {
   F(rn_params, amb) F(rn_params, bar) F(rn_params, Tw) F(rn_params, RcCells) F(rn_params, order2)
   F(rn_params, chem) F(rn_params, mhat) F(rn_params, fuel) F(rn_params, ox) F(rn_params, fan)
   F(rn_integral_spec, dx) F(rn_integral_spec, Rs) F(rn_integral_spec, inj) F(rn_integrals_out, t)
+  printf("rn_server_opts %zu\nrn_solve_request %zu\nrn_solve_result %zu\nrn_serve_status %zu\n",
+         sizeof(rn_server_opts), sizeof(rn_solve_request), sizeof(rn_solve_result), sizeof(rn_serve_status));
+  F(rn_server_opts, max_active) F(rn_server_opts, tile) F(rn_solve_request, mask) F(rn_solve_request, injTab)
+  F(rn_solve_request, P) F(rn_solve_request, spec) F(rn_solve_request, drop) F(rn_solve_request, max_steps)
+  F(rn_solve_result, steps) F(rn_solve_result, done_ms) F(rn_solve_result, integrals) F(rn_serve_status, failed)
   return 0;
 }
 """
@@ -65,11 +70,16 @@ def test_struct_layout_matches_header(rn):
     assert c["rn_read_req"] == ctypes.sizeof(solver.RnReadReq)
     assert c["rn_integral_spec"] == ctypes.sizeof(solver.RnIntegralSpec)
     assert c["rn_integrals_out"] == ctypes.sizeof(solver.RnIntegralsOut)
+    classes = {"rn_params": solver.RnParams, "rn_integral_spec": solver.RnIntegralSpec,
+               "rn_integrals_out": solver.RnIntegralsOut, "rn_server_opts": solver.RnServerOpts,
+               "rn_solve_request": solver.RnSolveRequest, "rn_solve_result": solver.RnSolveResult,
+               "rn_serve_status": solver.RnServeStatus}
+    for t in ("rn_server_opts", "rn_solve_request", "rn_solve_result", "rn_serve_status"):
+        assert c[t] == ctypes.sizeof(classes[t]), t
     for key, v in c.items():
         if "." in key:
             t, m = key.split(".")
-            cls = {"rn_params": solver.RnParams, "rn_integral_spec": solver.RnIntegralSpec,
-                   "rn_integrals_out": solver.RnIntegralsOut}[t]
+            cls = classes[t]
             assert getattr(cls, m).offset == v, key
 
 
