@@ -35,9 +35,20 @@
 namespace rn {
 namespace RN_VARIANT {
 
+// Resident warps per SM the step kernels are compiled for: 32 caps them at 64
+// registers (4 blocks of 256 threads per SM). Measured on B200 (fast
+// precision, G cell-updates/s, caps of 8 / 24 / 32 / 40 warps): 64 batched
+// instances 2.24 / 3.05 / 3.44 / 3.04, plain 4096x1536 3.33 / 4.55 / 5.52 /
+// 5.65, viscous 512x192 1.71 / 2.24 / 2.18 / 1.89. Results are bit-identical
+// across caps.
+#ifndef RN_MIN_WARPS
+#define RN_MIN_WARPS 32
+#endif
+
 template <int TX_, int TY_>
 struct TileT {
   static constexpr int TX = TX_, TY = TY_, NT = TX * TY;
+  static constexpr int MINB = RN_MIN_WARPS / (NT / 32) > 0 ? RN_MIN_WARPS / (NT / 32) : 1;
   static constexpr int PX = TX + 4, PY = TY + 4, NPT = PX * PY;   // primitives with a 2-cell halo
   static constexpr int NXF = TY * (TX + 1), NRF = (TY + 1) * TX;  // x- and r-faces of a tile
   static constexpr int TW = TX + 2, NTT = (TX + 2) * (TY + 2);    // vcell ring (tile + 1)
@@ -561,14 +572,14 @@ __device__ __forceinline__ void physics_body(const PhysArgs& a, const rn_params&
 // --------------------------------------------------------------------------
 // Single-instance kernels: blockIdx = tile.
 template <class T, int STAGE>
-__global__ void __launch_bounds__(T::NT) k_stage(StageArgs a, rn_params P) {
+__global__ void __launch_bounds__(T::NT, T::MINB) k_stage(StageArgs a, rn_params P) {
   extern __shared__ float4 sm[];
   __shared__ float red[T::NT / 32];
   __shared__ int xc[MAXX];
   stage_body<T, STAGE>(a, P, blockIdx.x, blockIdx.y, blockIdx.y * gridDim.x + blockIdx.x, sm, red, xc);
 }
 template <class T>
-__global__ void __launch_bounds__(T::NT) k_physics(PhysArgs a, rn_params P) {
+__global__ void __launch_bounds__(T::NT, T::MINB) k_physics(PhysArgs a, rn_params P) {
   extern __shared__ float4 sm[];
   __shared__ float red[T::NT / 32];
   __shared__ int xc[MAXX];
@@ -587,7 +598,7 @@ __device__ __forceinline__ void load_inst(const BatchInst* insts, const int* blo
   __syncthreads();
 }
 template <class T, int STAGE>
-__global__ void __launch_bounds__(T::NT) k_stage_batch(const BatchInst* insts, const int* blockInst, BatchPhase ph) {
+__global__ void __launch_bounds__(T::NT, T::MINB) k_stage_batch(const BatchInst* insts, const int* blockInst, BatchPhase ph) {
   extern __shared__ float4 sm[];
   __shared__ float red[T::NT / 32];
   __shared__ int xc[MAXX];
@@ -612,7 +623,7 @@ __global__ void __launch_bounds__(T::NT) k_stage_batch(const BatchInst* insts, c
   stage_body<T, STAGE>(a, d.P, bx, by, local, sm, red, xc);
 }
 template <class T>
-__global__ void __launch_bounds__(T::NT) k_physics_batch(const BatchInst* insts, const int* blockInst, BatchPhase ph) {
+__global__ void __launch_bounds__(T::NT, T::MINB) k_physics_batch(const BatchInst* insts, const int* blockInst, BatchPhase ph) {
   extern __shared__ float4 sm[];
   __shared__ float red[T::NT / 32];
   __shared__ int xc[MAXX];
