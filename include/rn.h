@@ -299,7 +299,8 @@ int rn_get_stream(rn_handle h, void** stream);
 #define RN_K_PARCELS 4   /* parcel update + deposit sort + segment sums */
 #define RN_K_APPLY 5
 #define RN_K_OTHER 6     /* rescale, wall row, integrals */
-#define RN_NKERNELS 7
+#define RN_K_STAGE2_PHYSICS 7   /* stage 2 fused with the viscous/wall/reaction split step */
+#define RN_NKERNELS 8
 int rn_profile(rn_handle h, int enable);
 int rn_profile_read(rn_handle h, double ms[RN_NKERNELS], long long launches[RN_NKERNELS]);
 

@@ -6,8 +6,8 @@
 // geometry planes geoA ((Nx+1) x (Nr+1) float4), geoG and geoM (float4 per
 // cell), the mask (1 byte per cell), two step-info float4s and two wave-speed
 // slots; the spray ring is 2 x 3 planes of 65,536 float4 plus the deposit
-// records. rn_step queues 2 kernels per step for the inviscid scheme (stage 1,
-// stage 2), 3 with the viscous/reaction split step and 3 more with sprays.
+// records. rn_step queues 2 kernels per step (stage 1, then stage 2 or stage 2
+// fused with the viscous/reaction split step) and 3 more with sprays.
 #include <cuda_runtime.h>
 #include <chrono>
 #include <cmath>
@@ -434,26 +434,22 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
     b.A = h->SA[s1]; b.B = h->SB[s1]; b.A0 = h->SA[s0]; b.B0 = h->SB[s0];
     b.oA = h->SA[s2]; b.oB = h->SB[s2];
     b.finalCfl = (!phys && !inj) ? 1 : 0;
-    {
+    if (phys) {
+      // stage 2 + split step in one kernel; its output replaces the stage-2 slot
+      PhysArgs p;
+      p.g = g;
+      p.A1 = h->SA[s1]; p.B1 = h->SB[s1]; p.A2 = h->SA[s2]; p.B2 = h->SB[s2];
+      p.oA = h->SA[s2]; p.oB = h->SB[s2];
+      p.st = stNew; p.wOut = wOut; p.finalCfl = inj ? 0 : 1;
+      p.xoff = h->xoff; p.xcell = h->xcell; p.maxX = h->maxX;
+      ProfScope ps(h, RN_K_STAGE2_PHYSICS);
+      h->K->stage2phys(b, p, *P, h->tile, h->stream);
+    } else {
       ProfScope ps(h, RN_K_STAGE2);
       h->K->stage2(b, *P, h->tile, h->stream);
     }
     h->launches++;
     h->cur = s2;
-    if (phys) {
-      PhysArgs p;
-      p.g = g;
-      p.A1 = h->SA[s1]; p.B1 = h->SB[s1]; p.A2 = h->SA[s2]; p.B2 = h->SB[s2];
-      p.oA = h->SA[s0]; p.oB = h->SB[s0];
-      p.st = stNew; p.wOut = wOut; p.finalCfl = inj ? 0 : 1;
-      p.xoff = h->xoff; p.xcell = h->xcell; p.maxX = h->maxX;
-      {
-        ProfScope ps(h, RN_K_PHYSICS);
-        h->K->physics(p, *P, h->tile, h->stream);
-      }
-      h->launches++;
-      h->cur = s0;
-    }
     if (inj) {
       const int out = (h->cur + 1) % 3;
       ApplyArgs ap;

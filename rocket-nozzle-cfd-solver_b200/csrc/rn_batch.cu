@@ -4,7 +4,7 @@
 // (solver.js:849-891 steps it). A batch is the serving form of the same step:
 // every tile of every member is one block of a single 1-D launch per kernel
 // kind, so small grids share the 148 SMs instead of each leaving most of them
-// idle, and a step of the whole batch costs 2-3 launches instead of 2-3 per
+// idle, and a step of the whole batch costs 2 launches instead of 2 per
 // member.
 //
 // Each block finds its member in a block->member table and that member's
@@ -31,15 +31,10 @@ constexpr int SPRAY_N = 65536;
 struct Flags {
   int visc = 0, chem = 0, inj = 0;
   bool phys() const { return visc || chem; }
-  // how far the state ring turns per step (rn_step's slot bookkeeping):
-  // 2 kernels write s1 then s2; physics writes s0 back; the spray apply
-  // writes the slot after the current one
-  int delta() const {
-    int d = 2;
-    if (phys()) d = 0;
-    if (inj) d = (d + 1) % 3;
-    return d;
-  }
+  // how far the state ring turns per step (rn_step's slot bookkeeping): the
+  // step's kernels write s1, then s2 (stage 2, or stage 2 fused with the
+  // split step); the spray apply writes the slot after s2
+  int delta() const { return inj ? 0 : 2; }
   bool operator==(const Flags& o) const { return visc == o.visc && chem == o.chem && inj == o.inj; }
 };
 Flags flags_of(const rn_params& P) {
@@ -234,20 +229,16 @@ int launch_step(rn_batch_t* b, int c, bool withSpray) {
       b->launches += launched;
     }
   }
-  ph.finalCfl = (!f.phys() && !f.inj) ? 1 : 0;
-  b->K->batchStage2(b->dInst, b->dBlock, nb, ph, b->tile, b->stream);
+  ph.finalCfl = f.inj ? 0 : 1;
+  if (f.phys()) b->K->batchStage2Phys(b->dInst, b->dBlock, nb, ph, b->tile, b->stream);
+  else b->K->batchStage2(b->dInst, b->dBlock, nb, ph, b->tile, b->stream);
   b->launches++;
-  if (f.phys()) {
-    ph.finalCfl = f.inj ? 0 : 1;
-    b->K->batchPhysics(b->dInst, b->dBlock, nb, ph, b->tile, b->stream);
-    b->launches++;
-  }
   if (f.inj && withSpray) {
     for (size_t m = 0; m < b->members.size(); m++) {
       rn_solver* h = b->members[m];
       const BatchInst& d = b->uploaded[m];
       const int s0 = (d.cur0 + ph.shift) % 3;
-      const int cur = f.phys() ? s0 : (s0 + 2) % 3, out = (cur + 1) % 3;
+      const int cur = (s0 + 2) % 3, out = (cur + 1) % 3;
       const int ws = d.wslot0 ^ ph.par;
       ApplyArgs ap;
       ap.g = h->grid();
@@ -293,7 +284,7 @@ int build_graph(rn_batch_t* b) {
   return RN_OK;
 }
 
-int launches_per_step(const rn_batch_t* b) { return 2 + (b->flags.phys() ? 1 : 0); }
+int launches_per_step(const rn_batch_t*) { return 2; }
 
 }  // namespace
 

@@ -35,7 +35,7 @@ struct StageArgs {
 struct PhysArgs {
   Grid g;
   const float4* A1; const float4* B1;   // stage-1 result (its primitives feed the viscous terms)
-  const float4* A2; const float4* B2;   // stage-2 result (updated here)
+  const float4* A2; const float4* B2;   // stage-2 result (slot; the fused kernel keeps it on chip)
   float4* oA; float4* oB;
   const float4* st;
   unsigned* wOut;
@@ -102,11 +102,12 @@ struct KernelSet {
   const char* name;
   void (*stage1)(const StageArgs& a, const rn_params& P, int tile, cudaStream_t s);
   void (*stage2)(const StageArgs& a, const rn_params& P, int tile, cudaStream_t s);
-  void (*physics)(const PhysArgs& a, const rn_params& P, int tile, cudaStream_t s);
+  // stage 2 + the viscous/wall/reaction split step in one kernel
+  void (*stage2phys)(const StageArgs& a, const PhysArgs& p, const rn_params& P, int tile, cudaStream_t s);
   void (*batchStage1)(const BatchInst* d, const int* blockInst, int nblocks, BatchPhase ph, int tile, cudaStream_t s);
   void (*batchStage2)(const BatchInst* d, const int* blockInst, int nblocks, BatchPhase ph, int tile, cudaStream_t s);
-  void (*batchPhysics)(const BatchInst* d, const int* blockInst, int nblocks, BatchPhase ph, int tile,
-                       cudaStream_t s);
+  void (*batchStage2Phys)(const BatchInst* d, const int* blockInst, int nblocks, BatchPhase ph, int tile,
+                          cudaStream_t s);
   void (*reduce)(const Grid& g, const float4* A, const float4* B, unsigned* w, cudaStream_t s);
   void (*rescale)(const Grid& g, const float4* A, const float4* B, float4* oA, float4* oB, float fp, float fT,
                   float du, const rn_params& P, cudaStream_t s);

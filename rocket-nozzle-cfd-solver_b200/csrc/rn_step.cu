@@ -21,9 +21,13 @@
 // stores the step info (FS_STEPINFO, solver.js:398-411). dt never leaves the
 // device.
 //
-// The viscous/wall/reaction split step is ONE kernel (k_physics): vcell
-// (FS_VCELL), the viscous face fluxes (makeViscFluxShader) and FS_SOURCE fused
-// per tile, reading the stage-1 primitives (solver.js:940-941).
+// With the viscous/wall/reaction split step, stage 2 and the split step are
+// ONE kernel (k_stage2phys): the stage-2 ghost primitives are the ones the
+// split step reads (solver.js:940-941), so the block stages them once, keeps
+// its stage-2 results in shared memory and runs vcell (FS_VCELL), the viscous
+// face fluxes (makeViscFluxShader) and FS_SOURCE on them. Its output goes to
+// the ring slot stage 2 alone would write, so no block overwrites the state
+// another block's stage-2 update still reads.
 //
 // Every body is a device function templated on the tile shape; a
 // single-instance kernel maps blockIdx to a tile, a batch kernel maps its 1-D
@@ -169,9 +173,138 @@ __host__ __device__ constexpr size_t stage_smem_t(int maxX) {
   return sizeof(float4) * (2 * (T::NPT + 25 * maxX) + 2 * (T::NXF + T::NRF + 4 * maxX)) +
          sizeof(float) * (T::NXF + T::NRF + 4 * maxX);
 }
+// --------------------------------------------------------------------------
+// Phases shared by the stage, physics and fused kernels. Each loops its slots
+// over the block's threads; the caller puts the barriers between phases.
+
+// FS_PRIM: ghost-cell primitives of the tile + 2-cell halo, then the listed
+// members' 5x5 blocks.
 template <class T>
-__host__ __device__ constexpr size_t physics_smem_t(int maxX) {
-  return sizeof(float4) * (2 * (T::NPT + 25 * maxX) + 2 * (T::NTT + 5 * maxX) + 2 * (T::NXF + T::NRF + 4 * maxX));
+__device__ __forceinline__ void load_prims(const Grid& g, const float4* __restrict__ A, const float4* __restrict__ B,
+                                           float t, const rn_params& P, int x0, int y0, const int* xc, int NP,
+                                           float4* sW, float4* sWb) {
+  const int Nx = g.Nx, Nr = g.Nr;
+  for (int k = threadIdx.x; k < NP; k += T::NT) {
+    int i, j;
+    prim_slot<T>(k, x0, y0, xc, Nx, i, j);
+    float4 W, Wb;
+    if (i <= Nx + 1 && j <= Nr + 1) ghost_prim(g, A, B, i, j, t, P, W, Wb);
+    else { W = make_float4(-1.f, 0.f, 0.f, 1.f); Wb = make_float4(0.f, 0.f, 0.f, 0.f); }
+    sW[k] = W;
+    sWb[k] = Wb;
+  }
+}
+
+// FS_FLUX_X/R: tile x-faces, tile r-faces, members' faces.
+template <class T>
+__device__ __forceinline__ void inviscid_faces(const Grid& g, const rn_params& P, int x0, int y0, const int* xc,
+                                               int NF, const float4* sW, const float4* sWb, float4* sF, float4* sY,
+                                               float* sO) {
+  const int Nx = g.Nx, Nr = g.Nr, W1 = Nx + 1;
+  for (int k = threadIdx.x; k < NF; k += T::NT) {
+    const FaceSlot s = face_slot<T>(k, x0, y0, xc, Nx, Nr);
+    Flux f;
+    f.F = make_float4(0.f, 0.f, 0.f, 0.f); f.Y = f.F; f.O = 0.f;
+    if (s.valid) {
+      float4 geo = g.geoA[s.j * W1 + s.i];
+      float area = s.dirR ? geo.w : geo.z;
+      if (area != 0.0f)
+        f = face_flux(s.dirR, area, sW[s.c[0]], sWb[s.c[0]], sW[s.c[1]], sWb[s.c[1]], sW[s.c[2]], sWb[s.c[2]],
+                      sW[s.c[3]], sWb[s.c[3]], sW[s.s[0]], sW[s.s[1]], sW[s.s[2]], sW[s.s[3]], P);
+    }
+    sF[k] = f.F; sY[k] = f.Y; sO[k] = f.O;
+  }
+}
+
+// FS_UPDATE of cell (i, j) inside the grid: the RK update of its host's
+// cut-cell group. Returns whether the cell is fluid.
+template <class T, int STAGE>
+__device__ __forceinline__ bool update_cell(const StageArgs& a, const rn_params& P, int i, int j, float dt, float t,
+                                            int x0, int y0, const int* xc, int xn, const float4* sF,
+                                            const float4* sY, const float* sO, float4& oA, float4& oB) {
+  const Grid& g = a.g;
+  const int Nx = g.Nx, W1 = Nx + 1;
+  const int k = j * Nx + i;
+  if (g.mask[k]) {
+    oA = make_float4(P.ambCons[0], P.ambCons[1], P.ambCons[2], P.ambCons[3]);
+    oB = make_float4(P.ambB[0], P.ambB[1], P.ambB[2], P.ambB[3]);
+    return false;
+  }
+  float4 gm = g.geoM[k];
+  const int Hx = i + iround(gm.x), Hy = j + iround(gm.y), kh = Hy * Nx + Hx;
+  float4 gg = g.geoG[k];
+  float4 A = a.A[kh], B = a.B[kh];
+  Prim q = to_prim(A, B);
+  float4 L = make_float4(0.f, 0.f, 0.f, 0.f), LY = L;
+  float LO = 0.0f;
+  const int sm_ = iround(g.geoM[kh].z);
+  for (int m = 0; m < 5; m++) {
+    int cx = Hx, cy = Hy;
+    if (m == 1) { if (!(sm_ & 1)) continue; cx -= 1; }
+    else if (m == 2) { if (!(sm_ & 2)) continue; cx += 1; }
+    else if (m == 3) { if (!(sm_ & 4)) continue; cy -= 1; }
+    else if (m == 4) { if (!(sm_ & 8)) continue; cy += 1; }
+    float4 gc = g.geoA[cy * W1 + cx];
+    float aw = fabsf(gc.z), ae = fabsf(g.geoA[cy * W1 + cx + 1].z);
+    float as_ = fabsf(gc.w), an = fabsf(g.geoA[(cy + 1) * W1 + cx].w);
+    int fw, fe, fs, fn;
+    member_faces<T>(cx, cy, x0, y0, xc, xn, Nx, fw, fe, fs, fn);
+    sub4(L, ae, sF[fe], aw, sF[fw]);
+    sub4(L, an, sF[fn], as_, sF[fs]);
+    sub4(LY, ae, sY[fe], aw, sY[fw]);
+    sub4(LY, an, sY[fn], as_, sY[fs]);
+    if (P.inj) {
+      LO -= ae * sO[fe] - aw * sO[fw];
+      LO -= an * sO[fn] - as_ * sO[fs];
+    }
+  }
+  // embedded wall: pressure force along the r-weighted wall vector
+  float wl = len2(gg.z, gg.w);
+  if (wl > 1e-6f) {
+    float nx = gg.z / wl, nr = gg.w / wl;
+    float pw = wall_pressure(q, q.w.y * nx + q.w.z * nr);
+    L.y -= gg.z * pw;
+    L.z -= gg.w * pw;
+  }
+  L.z += q.w.w * gg.y;                       // axisymmetric source p Am
+  float invV = 1.0f / fmaxf(gg.x, 1e-6f);
+  float4 LB = make_float4(LY.x, LY.y, LY.z - q.s.z * LY.w, LO);
+  float f = dt * invV;
+  float4 U, UY;
+  if (STAGE == 1) {
+    U = make_float4(A.x + f * L.x, A.y + f * L.y, A.z + f * L.z, A.w + f * L.w);
+    UY = make_float4(B.x + f * LB.x, B.y + f * LB.y, B.z + f * LB.z, B.w + f * LB.w);
+  } else {
+    float4 A0 = a.A0[kh], B0 = a.B0[kh];
+    U = make_float4(0.5f * (A0.x + A.x + f * L.x), 0.5f * (A0.y + A.y + f * L.y), 0.5f * (A0.z + A.z + f * L.z),
+                    0.5f * (A0.w + A.w + f * L.w));
+    UY = make_float4(0.5f * (B0.x + B.x + f * LB.x), 0.5f * (B0.y + B.y + f * LB.y),
+                     0.5f * (B0.z + B.z + f * LB.z), 0.5f * (B0.w + B.w + f * LB.w));
+  }
+  float rho = fmaxf(U.x, RHO_MIN);
+  float den = fmaxf(U.x, RHO_MIN);
+  float vx = U.y / den, vy = U.z / den;
+  float sp = len2(vx, vy);
+  if (sp > P.vMax) { float s = P.vMax / sp; vx *= s; vy *= s; }
+  if (!(rho < 1e30f) || !(vx < 1e30f && vx > -1e30f)) {   // NaN guard
+    oA = make_float4(P.ambCons[0], P.ambCons[1], P.ambCons[2], P.ambCons[3]);
+    oB = make_float4(P.ambB[0], P.ambB[1], P.ambB[2], P.ambB[3]);
+  } else {
+    float ke = 0.5f * rho * (vx * vx + vy * vy);
+    float Gn = clampf(UY.z, P.gamR[0], P.gamR[1]);
+    float E = fmaxf(U.w, P_MIN * Gn + ke);
+    float Zn = clampf(UY.x, 0.0f, rho);
+    oA = make_float4(rho, rho * vx, rho * vy, E);
+    float ubar = 0.0f;
+    if (P.inj) ubar = clampf(UY.w, 0.0f, rho);
+    else if (i == 0) {
+      float u0 = a.B[k].w;
+      bool on = STAGE == 2 && t > P.bar[2];
+      ubar = on ? fminf(u0 + fminf(dt * P.bar[0], 1.0f) * (vx - u0), P.bar[1]) : u0;
+    }
+    oB = make_float4(Zn, clampf(UY.y, 0.0f, Zn), Gn, ubar);
+  }
+  return true;
 }
 
 // --------------------------------------------------------------------------
@@ -181,7 +314,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const rn_params& 
                                            float4* sm, float* red, int* xc) {
   constexpr int TX = T::TX, NT = T::NT;
   const Grid& g = a.g;
-  const int Nx = g.Nx, Nr = g.Nr, W1 = Nx + 1;
+  const int Nx = g.Nx, Nr = g.Nr;
   const int tid = threadIdx.x;
   const int x0 = bx * TX, y0 = by * T::TY;
   const int xb = a.xoff[tileId], xn = a.xoff[tileId + 1] - xb;
@@ -210,122 +343,17 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const rn_params& 
     t = st.z;                                     // inlet ramp at t_new
   }
   __syncthreads();
-
-  // ---- ghost-cell primitives: tile + 2-cell halo, then the members' blocks
-  for (int k = tid; k < NP; k += NT) {
-    int i, j;
-    prim_slot<T>(k, x0, y0, xc, Nx, i, j);
-    float4 W, Wb;
-    if (i <= Nx + 1 && j <= Nr + 1) ghost_prim(g, a.A, a.B, i, j, t, P, W, Wb);
-    else { W = make_float4(-1.f, 0.f, 0.f, 1.f); Wb = make_float4(0.f, 0.f, 0.f, 0.f); }
-    sW[k] = W;
-    sWb[k] = Wb;
-  }
+  load_prims<T>(g, a.A, a.B, t, P, x0, y0, xc, NP, sW, sWb);
+  __syncthreads();
+  inviscid_faces<T>(g, P, x0, y0, xc, NF, sW, sWb, sF, sY, sO);
   __syncthreads();
 
-  // ---- face fluxes: tile x-faces, tile r-faces, members' faces
-  for (int k = tid; k < NF; k += NT) {
-    const FaceSlot s = face_slot<T>(k, x0, y0, xc, Nx, Nr);
-    Flux f;
-    f.F = make_float4(0.f, 0.f, 0.f, 0.f); f.Y = f.F; f.O = 0.f;
-    if (s.valid) {
-      float4 geo = g.geoA[s.j * W1 + s.i];
-      float area = s.dirR ? geo.w : geo.z;
-      if (area != 0.0f)
-        f = face_flux(s.dirR, area, sW[s.c[0]], sWb[s.c[0]], sW[s.c[1]], sWb[s.c[1]], sW[s.c[2]], sWb[s.c[2]],
-                      sW[s.c[3]], sWb[s.c[3]], sW[s.s[0]], sW[s.s[1]], sW[s.s[2]], sW[s.s[3]], P);
-    }
-    sF[k] = f.F; sY[k] = f.Y; sO[k] = f.O;
-  }
-  __syncthreads();
-
-  // ---- cut-cell group update (FS_UPDATE)
-  const int lx = tid % TX, ly = tid / TX;
-  const int i = x0 + lx, j = y0 + ly;
+  const int i = x0 + tid % TX, j = y0 + tid / TX;
   float wcell = 0.0f;
   if (i < Nx && j < Nr) {
-    const int k = j * Nx + i;
     float4 oA, oB;
-    bool fluid = !g.mask[k];
-    if (!fluid) {
-      oA = make_float4(P.ambCons[0], P.ambCons[1], P.ambCons[2], P.ambCons[3]);
-      oB = make_float4(P.ambB[0], P.ambB[1], P.ambB[2], P.ambB[3]);
-    } else {
-      float4 gm = g.geoM[k];
-      const int Hx = i + iround(gm.x), Hy = j + iround(gm.y), kh = Hy * Nx + Hx;
-      float4 gg = g.geoG[k];
-      float4 A = a.A[kh], B = a.B[kh];
-      Prim q = to_prim(A, B);
-      float4 L = make_float4(0.f, 0.f, 0.f, 0.f), LY = L;
-      float LO = 0.0f;
-      const int sm_ = iround(g.geoM[kh].z);
-      for (int m = 0; m < 5; m++) {
-        int cx = Hx, cy = Hy;
-        if (m == 1) { if (!(sm_ & 1)) continue; cx -= 1; }
-        else if (m == 2) { if (!(sm_ & 2)) continue; cx += 1; }
-        else if (m == 3) { if (!(sm_ & 4)) continue; cy -= 1; }
-        else if (m == 4) { if (!(sm_ & 8)) continue; cy += 1; }
-        float4 gc = g.geoA[cy * W1 + cx];
-        float aw = fabsf(gc.z), ae = fabsf(g.geoA[cy * W1 + cx + 1].z);
-        float as_ = fabsf(gc.w), an = fabsf(g.geoA[(cy + 1) * W1 + cx].w);
-        int fw, fe, fs, fn;
-        member_faces<T>(cx, cy, x0, y0, xc, xn, Nx, fw, fe, fs, fn);
-        sub4(L, ae, sF[fe], aw, sF[fw]);
-        sub4(L, an, sF[fn], as_, sF[fs]);
-        sub4(LY, ae, sY[fe], aw, sY[fw]);
-        sub4(LY, an, sY[fn], as_, sY[fs]);
-        if (P.inj) {
-          LO -= ae * sO[fe] - aw * sO[fw];
-          LO -= an * sO[fn] - as_ * sO[fs];
-        }
-      }
-      // embedded wall: pressure force along the r-weighted wall vector
-      float wl = len2(gg.z, gg.w);
-      if (wl > 1e-6f) {
-        float nx = gg.z / wl, nr = gg.w / wl;
-        float pw = wall_pressure(q, q.w.y * nx + q.w.z * nr);
-        L.y -= gg.z * pw;
-        L.z -= gg.w * pw;
-      }
-      L.z += q.w.w * gg.y;                       // axisymmetric source p Am
-      float invV = 1.0f / fmaxf(gg.x, 1e-6f);
-      float4 LB = make_float4(LY.x, LY.y, LY.z - q.s.z * LY.w, LO);
-      float f = dt * invV;
-      float4 U, UY;
-      if (STAGE == 1) {
-        U = make_float4(A.x + f * L.x, A.y + f * L.y, A.z + f * L.z, A.w + f * L.w);
-        UY = make_float4(B.x + f * LB.x, B.y + f * LB.y, B.z + f * LB.z, B.w + f * LB.w);
-      } else {
-        float4 A0 = a.A0[kh], B0 = a.B0[kh];
-        U = make_float4(0.5f * (A0.x + A.x + f * L.x), 0.5f * (A0.y + A.y + f * L.y), 0.5f * (A0.z + A.z + f * L.z),
-                        0.5f * (A0.w + A.w + f * L.w));
-        UY = make_float4(0.5f * (B0.x + B.x + f * LB.x), 0.5f * (B0.y + B.y + f * LB.y),
-                         0.5f * (B0.z + B.z + f * LB.z), 0.5f * (B0.w + B.w + f * LB.w));
-      }
-      float rho = fmaxf(U.x, RHO_MIN);
-      float den = fmaxf(U.x, RHO_MIN);
-      float vx = U.y / den, vy = U.z / den;
-      float sp = len2(vx, vy);
-      if (sp > P.vMax) { float s = P.vMax / sp; vx *= s; vy *= s; }
-      if (!(rho < 1e30f) || !(vx < 1e30f && vx > -1e30f)) {   // NaN guard
-        oA = make_float4(P.ambCons[0], P.ambCons[1], P.ambCons[2], P.ambCons[3]);
-        oB = make_float4(P.ambB[0], P.ambB[1], P.ambB[2], P.ambB[3]);
-      } else {
-        float ke = 0.5f * rho * (vx * vx + vy * vy);
-        float Gn = clampf(UY.z, P.gamR[0], P.gamR[1]);
-        float E = fmaxf(U.w, P_MIN * Gn + ke);
-        float Zn = clampf(UY.x, 0.0f, rho);
-        oA = make_float4(rho, rho * vx, rho * vy, E);
-        float ubar = 0.0f;
-        if (P.inj) ubar = clampf(UY.w, 0.0f, rho);
-        else if (i == 0) {
-          float u0 = a.B[k].w;
-          bool on = STAGE == 2 && t > P.bar[2];
-          ubar = on ? fminf(u0 + fminf(dt * P.bar[0], 1.0f) * (vx - u0), P.bar[1]) : u0;
-        }
-        oB = make_float4(Zn, clampf(UY.y, 0.0f, Zn), Gn, ubar);
-      }
-    }
+    const bool fluid = update_cell<T, STAGE>(a, P, i, j, dt, t, x0, y0, xc, xn, sF, sY, sO, oA, oB);
+    const int k = j * Nx + i;
     a.oA[k] = oA;
     a.oB[k] = oB;
     if (a.finalCfl && fluid) wcell = wave_speed(oA, oB);
@@ -354,40 +382,12 @@ __device__ __forceinline__ void vcell_slot(int k, int x0, int y0, const int* xc,
   }
 }
 
-// The viscous/wall/reaction split step on tile (bx, by).
+// FS_VCELL over the tile + 1 ring and the members' cells.
 template <class T>
-__device__ __forceinline__ void physics_body(const PhysArgs& a, const rn_params& P, int bx, int by, int tileId,
-                                             float4* sm, float* red, int* xc) {
-  constexpr int TX = T::TX, NT = T::NT, PX = T::PX, TW = T::TW;
-  const Grid& g = a.g;
-  const int Nx = g.Nx, Nr = g.Nr, W1 = Nx + 1;
-  const int tid = threadIdx.x;
-  const int x0 = bx * TX, y0 = by * T::TY;
-  const float4 st = *a.st;
-  const float dt = st.x, t = st.z;
-  const int xb = a.xoff[tileId], xn = P.visc ? a.xoff[tileId + 1] - xb : 0;
-  const int NP = T::NPT + 25 * xn, NV = T::NTT + 5 * xn, NF = T::NXF + T::NRF + 4 * xn;
-  float4* sW = sm;
-  float4* sWb = sW + NP;
-  float4* sT1 = sWb + NP;
-  float4* sT2 = sT1 + NV;
-  float4* sF = sT2 + NV;
-  float4* sY = sF + NF;
-  for (int q = tid; q < xn; q += NT) xc[q] = a.xcell[xb + q];
-  __syncthreads();
-
-  for (int k = tid; k < NP; k += NT) {
-    int i, j;
-    prim_slot<T>(k, x0, y0, xc, Nx, i, j);
-    float4 W, Wb;
-    if (i <= Nx + 1 && j <= Nr + 1) ghost_prim(g, a.A1, a.B1, i, j, t, P, W, Wb);
-    else { W = make_float4(-1.f, 0.f, 0.f, 1.f); Wb = make_float4(0.f, 0.f, 0.f, 0.f); }
-    sW[k] = W;
-    sWb[k] = Wb;
-  }
-  __syncthreads();
-  // vcell over the tile + 1 ring and the members' cells
-  for (int k = tid; k < NV; k += NT) {
+__device__ __forceinline__ void vcells(const Grid& g, const rn_params& P, float dt, int x0, int y0, const int* xc,
+                                       int NV, const float4* sW, const float4* sWb, float4* sT1, float4* sT2) {
+  const int Nx = g.Nx, Nr = g.Nr;
+  for (int k = threadIdx.x; k < NV; k += T::NT) {
     int i, j, c, e_, w_, n_, s_;
     vcell_slot<T>(k, x0, y0, xc, Nx, i, j, c, e_, w_, n_, s_);
     float4 T1 = make_float4(0.f, 0.f, 0.f, 0.f), T2 = T1;
@@ -396,177 +396,284 @@ __device__ __forceinline__ void physics_body(const PhysArgs& a, const rn_params&
     sT1[k] = T1;
     sT2[k] = T2;
   }
-  __syncthreads();
+}
+
+// FS_VFLUX_X/R: viscous faces of the tile and of the members.
+template <class T>
+__device__ __forceinline__ void viscous_faces(const Grid& g, int x0, int y0, const int* xc, int NF, const float4* sW,
+                                              const float4* sWb, const float4* sT1, const float4* sT2, float4* sF,
+                                              float4* sY) {
+  constexpr int TX = T::TX, PX = T::PX, TW = T::TW;
+  const int Nx = g.Nx, Nr = g.Nr, W1 = Nx + 1;
+  for (int k = threadIdx.x; k < NF; k += T::NT) {
+    float4 F = make_float4(0.f, 0.f, 0.f, 0.f), FY = F;
+    bool dirR, ok;
+    int i, j, p1, p2, v1, v2;          // primitive and vcell slots of the cells behind (1) and at (2) the face
+    if (k < T::NXF) {
+      const int ly = k / (TX + 1), lx = k - ly * (TX + 1);
+      i = x0 + lx; j = y0 + ly; dirR = false;
+      ok = i > 0 && i < Nx && j < Nr;
+      p2 = (ly + 2) * PX + lx + 2; p1 = p2 - 1;
+      v2 = (ly + 1) * TW + lx + 1; v1 = v2 - 1;
+    } else if (k < T::NXF + T::NRF) {
+      const int kk = k - T::NXF, ly = kk / TX, lx = kk - ly * TX;
+      i = x0 + lx; j = y0 + ly; dirR = true;
+      ok = i < Nx && j > 0 && j < Nr;
+      p2 = (ly + 2) * PX + lx + 2; p1 = p2 - PX;
+      v2 = (ly + 1) * TW + lx + 1; v1 = v2 - TW;
+    } else {
+      const int q = k - T::NXF - T::NRF, e = q >> 2, w = q & 3, m = xc[e];
+      const int mx = m % Nx, my = m / Nx, vb = T::NTT + 5 * e;
+      if (w == 0) { i = mx; j = my; dirR = false; p1 = ext_prim<T>(e, -1, 0); p2 = ext_prim<T>(e, 0, 0); v1 = vb + 1; v2 = vb; }
+      else if (w == 1) { i = mx + 1; j = my; dirR = false; p1 = ext_prim<T>(e, 0, 0); p2 = ext_prim<T>(e, 1, 0); v1 = vb; v2 = vb + 2; }
+      else if (w == 2) { i = mx; j = my; dirR = true; p1 = ext_prim<T>(e, 0, -1); p2 = ext_prim<T>(e, 0, 0); v1 = vb + 3; v2 = vb; }
+      else { i = mx; j = my + 1; dirR = true; p1 = ext_prim<T>(e, 0, 0); p2 = ext_prim<T>(e, 0, 1); v1 = vb; v2 = vb + 4; }
+      ok = dirR ? (i < Nx && j > 0 && j < Nr) : (i > 0 && i < Nx && j < Nr);
+    }
+    if (ok) {
+      float4 geo = g.geoA[j * W1 + i];
+      float area = dirR ? geo.w : geo.z;
+      float4 w1 = sW[p1], w2 = sW[p2];
+      if (area != 0.0f && !(w1.x < 0.0f || w2.x < 0.0f))
+        visc_flux(dirR, w1, sWb[p1], sT1[v1], sT2[v1], w2, sWb[p2], sT1[v2], sT2[v2], j, F, FY);
+    }
+    sF[k] = F;
+    sY[k] = FY;
+  }
+}
+
+// FS_SOURCE of cell (i, j) inside the grid. A, B = the stage-2 state of the
+// cell's group host; Bw = the cell's own stage-2 B.w. A1/B1 (global) feed
+// the separation samples. Returns whether the cell is fluid.
+template <class T>
+__device__ __forceinline__ bool source_cell(const Grid& g, const float4* __restrict__ A1,
+                                            const float4* __restrict__ B1, const rn_params& P, int i, int j,
+                                            float dt, int x0, int y0, const int* xc, int xn, const float4* sF,
+                                            const float4* sY, const float4* sT1, const float4* sT2, float4 A,
+                                            float4 B, float Bw, float4& oA, float4& oB) {
+  constexpr int TW = T::TW;
+  const int Nx = g.Nx, Nr = g.Nr, W1 = Nx + 1;
+  const int k = j * Nx + i;
+  if (g.mask[k]) {
+    oA = make_float4(P.ambCons[0], P.ambCons[1], P.ambCons[2], P.ambCons[3]);
+    oB = make_float4(P.ambB[0], P.ambB[1], P.ambB[2], P.ambB[3]);
+    return false;
+  }
+  float4 gmij = g.geoM[k];
+  const int Hx = i + iround(gmij.x), Hy = j + iround(gmij.y), kh = Hy * Nx + Hx;
+  float4 gg = g.geoG[k];
+  Prim q = to_prim(A, B);
+  float rho = q.w.x, p = q.w.w, G = q.s.z;
+  float velx = q.w.y, vely = q.w.z;
+  float V = fmaxf(gg.x, 1e-6f);
+  float Rm = rmix(q.s, P), Tg = p / (rho * Rm);
+  float4 L = make_float4(0.f, 0.f, 0.f, 0.f), LY = L;
+  const int vh = (Hy - y0 + 1) * TW + (Hx - x0 + 1);
+  float4 T1h = sT1[vh], T2h = sT2[vh];
   if (P.visc) {
-    for (int k = tid; k < NF; k += NT) {
-      float4 F = make_float4(0.f, 0.f, 0.f, 0.f), FY = F;
-      bool dirR, ok;
-      int i, j, p1, p2, v1, v2;          // primitive and vcell slots of the cells behind (1) and at (2) the face
-      if (k < T::NXF) {
-        const int ly = k / (TX + 1), lx = k - ly * (TX + 1);
-        i = x0 + lx; j = y0 + ly; dirR = false;
-        ok = i > 0 && i < Nx && j < Nr;
-        p2 = (ly + 2) * PX + lx + 2; p1 = p2 - 1;
-        v2 = (ly + 1) * TW + lx + 1; v1 = v2 - 1;
-      } else if (k < T::NXF + T::NRF) {
-        const int kk = k - T::NXF, ly = kk / TX, lx = kk - ly * TX;
-        i = x0 + lx; j = y0 + ly; dirR = true;
-        ok = i < Nx && j > 0 && j < Nr;
-        p2 = (ly + 2) * PX + lx + 2; p1 = p2 - PX;
-        v2 = (ly + 1) * TW + lx + 1; v1 = v2 - TW;
-      } else {
-        const int q = k - T::NXF - T::NRF, e = q >> 2, w = q & 3, m = xc[e];
-        const int mx = m % Nx, my = m / Nx, vb = T::NTT + 5 * e;
-        if (w == 0) { i = mx; j = my; dirR = false; p1 = ext_prim<T>(e, -1, 0); p2 = ext_prim<T>(e, 0, 0); v1 = vb + 1; v2 = vb; }
-        else if (w == 1) { i = mx + 1; j = my; dirR = false; p1 = ext_prim<T>(e, 0, 0); p2 = ext_prim<T>(e, 1, 0); v1 = vb; v2 = vb + 2; }
-        else if (w == 2) { i = mx; j = my; dirR = true; p1 = ext_prim<T>(e, 0, -1); p2 = ext_prim<T>(e, 0, 0); v1 = vb + 3; v2 = vb; }
-        else { i = mx; j = my + 1; dirR = true; p1 = ext_prim<T>(e, 0, 0); p2 = ext_prim<T>(e, 0, 1); v1 = vb; v2 = vb + 4; }
-        ok = dirR ? (i < Nx && j > 0 && j < Nr) : (i > 0 && i < Nx && j < Nr);
+    const int sm_ = iround(g.geoM[kh].z);
+    for (int m = 0; m < 5; m++) {
+      int cx = Hx, cy = Hy;
+      if (m == 1) { if (!(sm_ & 1)) continue; cx -= 1; }
+      else if (m == 2) { if (!(sm_ & 2)) continue; cx += 1; }
+      else if (m == 3) { if (!(sm_ & 4)) continue; cy -= 1; }
+      else if (m == 4) { if (!(sm_ & 8)) continue; cy += 1; }
+      float4 gc = g.geoA[cy * W1 + cx];
+      float aw = fabsf(gc.z), ae = fabsf(g.geoA[cy * W1 + cx + 1].z);
+      float as_ = fabsf(gc.w), an = fabsf(g.geoA[(cy + 1) * W1 + cx].w);
+      int fw, fe, fs, fn;
+      member_faces<T>(cx, cy, x0, y0, xc, xn, Nx, fw, fe, fs, fn);
+      sub4(L, ae, sF[fe], aw, sF[fw]);
+      sub4(L, an, sF[fn], as_, sF[fs]);
+      sub4(LY, ae, sY[fe], aw, sY[fw]);
+      sub4(LY, an, sY[fn], as_, sY[fs]);
+    }
+    // axisymmetric hoop stress
+    float r = V / fmaxf(gg.y, 1e-6f), vor = vely / r;
+    L.z -= T2h.x * (2.0f * vor - 0.6666667f * (T1h.x + T1h.w + vor)) * gg.y;
+    // Werner-Wengle wall shear and Reynolds-analogy heat flux
+    float wl = len2(gg.z, gg.w);
+    if (wl > 1e-6f) {
+      float nx = gg.z / wl, nr = gg.w / wl;
+      float dn = velx * nx + vely * nr;
+      float utx = velx - dn * nx, uty = vely - dn * nr;
+      float up = len2(utx, uty);
+      float cp = Rm * (G + 1.0f);
+      float Taw = Tg + 0.89f * up * up / (2.0f * cp);
+      float Ts = fmaxf(Tg + 0.5f * (P.Tw - Tg) + 0.22f * (Taw - Tg), 1e-3f);
+      float rs = p / (Rm * Ts), mus = sutherland(Ts * P.gas[2], P);
+      float dz = 2.0f * clampf(0.5f * V / wl, 0.25f, 1.0f);
+      float nz = mus / (rs * dz);
+      float tw = up <= 69.7f * nz ? 2.0f * mus * up / dz
+                                  : rs * powf(7.187f * powf(nz, 1.142857f) + 0.13769f * powf(nz, 0.142857f) * up, 1.75f);
+      tw = fminf(tw, 0.3f * rho * up * V / fmaxf(wl * dt, 1e-9f));
+      if (up > 1e-6f) { L.y -= tw * wl * utx / up; L.z -= tw * wl * uty / up; }
+      float qw = tw / fmaxf(up, 1e-4f) * cp * (Taw - P.Tw) * 1.24f;
+      float qmax = 0.3f * p * G * V / fmaxf(wl * dt, 1e-9f);
+      L.w -= clampf(qw, -qmax, qmax) * wl;
+    }
+    // shock / boundary-layer interaction on the bit-16 band
+    if (sm_ & 16) {
+      float up = len2(velx, vely), Mn = up / sqrtf((1.0f + 1.0f / G) * p / rho);
+      if (Mn > 1.0f) {
+        float shx = velx / up, shy = vely / up;
+        float pd = 0.0f;
+        for (int n = 4; n <= 6; n += 2)
+          for (int mm = 0; mm <= 1; mm++) {
+            int Dx = Hx + int(rintf(float(n) * shx));
+            int Dy = Hy + int(floorf(float(n) * shy)) + mm;
+            Dx = min(max(Dx, 0), Nx - 1);
+            Dy = min(max(Dy, 0), Nr - 1);
+            float4 wd, sd;
+            interior_prim(g, A1, B1, Dx, Dy, wd, sd);
+            if (wd.x > 0.0f) pd = fmaxf(pd, wd.w);
+          }
+        float crit = 1.0f + 0.5f * Mn;
+        float fsep = smoothstepf(crit, 1.2f * crit, pd / p) * V * rho * up;
+        L.y -= fsep * velx;
+        L.z -= fsep * vely;
+      } else if (velx > 0.0f && p < 1.3f * P.chemK[3]) {
+        float fsep = 0.5f * V * rho * up;
+        L.y -= fsep * velx;
+        L.z -= fsep * vely;
       }
-      if (ok) {
-        float4 geo = g.geoA[j * W1 + i];
-        float area = dirR ? geo.w : geo.z;
-        float4 w1 = sW[p1], w2 = sW[p2];
-        if (area != 0.0f && !(w1.x < 0.0f || w2.x < 0.0f))
-          visc_flux(dirR, w1, sWb[p1], sT1[v1], sT2[v1], w2, sWb[p2], sT1[v2], sT2[v2], j, F, FY);
-      }
-      sF[k] = F;
-      sY[k] = FY;
+    }
+  }
+  float invV = dt / V;
+  float dO = invV * L.x;
+  L.x = 0.0f;
+  float4 U = make_float4(A.x + invV * L.x, A.y + invV * L.y, A.z + invV * L.z, A.w + invV * L.w);
+  float4 UY = make_float4(B.x + invV * LY.x / 1.0f, B.y + invV * LY.y / 1.0f, B.z + invV * LY.z / rho,
+                          B.w + invV * 0.0f / 1.0f);
+  if (P.inj) UY.w += dO;
+  if (P.chem) {
+    float Z = q.s.x, F = q.s.y, O = q.s.w, s = P.chemK[1];
+    float avail = P.inj ? fminf(F, (O + 0.233f * fmaxf(1.0f - Z, 0.0f)) / s)
+                        : fminf(F, fmaxf(1.0f - Z - s * (Z - F), 0.0f) / s);
+    if (avail > 1e-5f) {
+      float TK = Tg * P.gas[2];
+      float kin = P.chemK[2] * p * expf(-9000.0f / TK) * (1.0f - smoothstepf(P.cap[0], P.cap[1], TK));
+      float mixr = P.inj ? fmaxf(T2h.z, 4.0f * T2h.x / rho) : T2h.z;
+      float burn = avail * fminf(fminf(mixr, kin) * dt, 0.5f);
+      UY.y -= rho * burn;
+      if (P.inj) UY.w = fmaxf(UY.w - rho * burn * s, 0.0f);
+      U.w += rho * burn * P.chemK[0];
+    }
+  }
+  float rn = fmaxf(U.x, RHO_MIN);
+  float vnx = U.y / rn, vny = U.z / rn;
+  if (!(rn < 1e30f) || !(vnx < 1e30f && vnx > -1e30f)) {
+    oA = make_float4(P.ambCons[0], P.ambCons[1], P.ambCons[2], P.ambCons[3]);
+    oB = make_float4(P.ambB[0], P.ambB[1], P.ambB[2], P.ambB[3]);
+  } else {
+    float Gn = clampf(UY.z, P.gamR[0], P.gamR[1]);
+    float Zn = clampf(UY.x, 0.0f, rn);
+    oA = make_float4(rn, rn * vnx, rn * vny, fmaxf(U.w, P_MIN * Gn + 0.5f * rn * (vnx * vnx + vny * vny)));
+    oB = make_float4(Zn, clampf(UY.y, 0.0f, Zn), Gn, P.inj ? clampf(UY.w, 0.0f, rn) : Bw);
+  }
+  return true;
+}
+
+// Stage 2 and the split step fused on tile (bx, by): the stage-2 input
+// primitives (the stage-1 state at t_new) are exactly what the split step
+// reads (solver.js:940-941), so they are staged once; the stage-2 results of
+// the tile's cells and of its listed members (every out-of-tile group host a
+// tile cell can have) stay in shared memory and feed FS_SOURCE directly.
+template <class T>
+__host__ __device__ constexpr size_t fused_region_t(int maxX) {
+  // float4 slots of the region that holds first the inviscid faces, then
+  // the vcell ring and the viscous faces
+  return (2 * (T::NXF + T::NRF + 4 * maxX) + ((T::NXF + T::NRF + 4 * maxX) + 3) / 4) >
+                 (2 * (T::NTT + 5 * maxX) + 2 * (T::NXF + T::NRF + 4 * maxX))
+             ? (2 * (T::NXF + T::NRF + 4 * maxX) + ((T::NXF + T::NRF + 4 * maxX) + 3) / 4)
+             : (2 * (T::NTT + 5 * maxX) + 2 * (T::NXF + T::NRF + 4 * maxX));
+}
+template <class T>
+__host__ __device__ constexpr size_t fused_smem_t(int maxX) {
+  return sizeof(float4) * (2 * (T::NPT + 25 * maxX) + fused_region_t<T>(maxX) + 2 * (T::NT + maxX));
+}
+template <class T>
+__device__ __forceinline__ void stage2_physics_body(const StageArgs& a, const PhysArgs& p, const rn_params& P, int bx,
+                                                    int by, int tileId, float4* sm, float* red, int* xc) {
+  constexpr int TX = T::TX, NT = T::NT;
+  const Grid& g = a.g;
+  const int Nx = g.Nx, Nr = g.Nr;
+  const int tid = threadIdx.x;
+  const int x0 = bx * TX, y0 = by * T::TY;
+  const int xb = a.xoff[tileId], xn = a.xoff[tileId + 1] - xb, xnP = P.visc ? xn : 0;
+  const int NP = T::NPT + 25 * xn, NF = T::NXF + T::NRF + 4 * xn;
+  const int NV = T::NTT + 5 * xnP, NFV = T::NXF + T::NRF + 4 * xnP;
+  float4* sW = sm;
+  float4* sWb = sW + NP;
+  float4* R = sWb + NP;
+  float4* sA2 = R + fused_region_t<T>(xn);
+  float4* sB2 = sA2 + NT + xn;
+  for (int q = tid; q < xn; q += NT) xc[q] = a.xcell[xb + q];
+  const float4 st = *a.stNew;
+  const float dt = st.x, t = st.z;
+  __syncthreads();
+  load_prims<T>(g, a.A, a.B, t, P, x0, y0, xc, NP, sW, sWb);
+  __syncthreads();
+  {
+    float4* sF = R;
+    float4* sY = sF + NF;
+    float* sO = reinterpret_cast<float*>(sY + NF);
+    inviscid_faces<T>(g, P, x0, y0, xc, NF, sW, sWb, sF, sY, sO);
+    __syncthreads();
+    const int i = x0 + tid % TX, j = y0 + tid / TX;
+    if (i < Nx && j < Nr) {
+      float4 oA, oB;
+      update_cell<T, 2>(a, P, i, j, dt, t, x0, y0, xc, xn, sF, sY, sO, oA, oB);
+      sA2[tid] = oA;
+      sB2[tid] = oB;
+    }
+    for (int q = tid; q < xn; q += NT) {
+      const int m = xc[q];
+      float4 oA, oB;
+      update_cell<T, 2>(a, P, m % Nx, m / Nx, dt, t, x0, y0, xc, xn, sF, sY, sO, oA, oB);
+      sA2[NT + q] = oA;
+      sB2[NT + q] = oB;
     }
   }
   __syncthreads();
+  float4* sT1 = R;
+  float4* sT2 = sT1 + NV;
+  float4* sF = sT2 + NV;
+  float4* sY = sF + NFV;
+  vcells<T>(g, P, dt, x0, y0, xc, NV, sW, sWb, sT1, sT2);
+  __syncthreads();
+  if (P.visc) viscous_faces<T>(g, x0, y0, xc, NFV, sW, sWb, sT1, sT2, sF, sY);
+  __syncthreads();
 
-  // ---- FS_SOURCE
-  const int lx = tid % TX, ly = tid / TX;
-  const int i = x0 + lx, j = y0 + ly;
+  const int i = x0 + tid % TX, j = y0 + tid / TX;
   float wcell = 0.0f;
   if (i < Nx && j < Nr) {
     const int k = j * Nx + i;
-    float4 oA, oB;
-    bool fluid = !g.mask[k];
-    if (!fluid) {
-      oA = make_float4(P.ambCons[0], P.ambCons[1], P.ambCons[2], P.ambCons[3]);
-      oB = make_float4(P.ambB[0], P.ambB[1], P.ambB[2], P.ambB[3]);
-    } else {
-      float4 gmij = g.geoM[k];
-      const int Hx = i + iround(gmij.x), Hy = j + iround(gmij.y), kh = Hy * Nx + Hx;
-      float4 gg = g.geoG[k];
-      float4 A = a.A2[kh], B = a.B2[kh];
-      Prim q = to_prim(A, B);
-      float rho = q.w.x, p = q.w.w, G = q.s.z;
-      float velx = q.w.y, vely = q.w.z;
-      float V = fmaxf(gg.x, 1e-6f);
-      float Rm = rmix(q.s, P), Tg = p / (rho * Rm);
-      float4 L = make_float4(0.f, 0.f, 0.f, 0.f), LY = L;
-      const int vh = (Hy - y0 + 1) * TW + (Hx - x0 + 1);
-      float4 T1h = sT1[vh], T2h = sT2[vh];
-      if (P.visc) {
-        const int sm_ = iround(g.geoM[kh].z);
-        for (int m = 0; m < 5; m++) {
-          int cx = Hx, cy = Hy;
-          if (m == 1) { if (!(sm_ & 1)) continue; cx -= 1; }
-          else if (m == 2) { if (!(sm_ & 2)) continue; cx += 1; }
-          else if (m == 3) { if (!(sm_ & 4)) continue; cy -= 1; }
-          else if (m == 4) { if (!(sm_ & 8)) continue; cy += 1; }
-          float4 gc = g.geoA[cy * W1 + cx];
-          float aw = fabsf(gc.z), ae = fabsf(g.geoA[cy * W1 + cx + 1].z);
-          float as_ = fabsf(gc.w), an = fabsf(g.geoA[(cy + 1) * W1 + cx].w);
-          int fw, fe, fs, fn;
-          member_faces<T>(cx, cy, x0, y0, xc, xn, Nx, fw, fe, fs, fn);
-          sub4(L, ae, sF[fe], aw, sF[fw]);
-          sub4(L, an, sF[fn], as_, sF[fs]);
-          sub4(LY, ae, sY[fe], aw, sY[fw]);
-          sub4(LY, an, sY[fn], as_, sY[fs]);
-        }
-        // axisymmetric hoop stress
-        float r = V / fmaxf(gg.y, 1e-6f), vor = vely / r;
-        L.z -= T2h.x * (2.0f * vor - 0.6666667f * (T1h.x + T1h.w + vor)) * gg.y;
-        // Werner-Wengle wall shear and Reynolds-analogy heat flux
-        float wl = len2(gg.z, gg.w);
-        if (wl > 1e-6f) {
-          float nx = gg.z / wl, nr = gg.w / wl;
-          float dn = velx * nx + vely * nr;
-          float utx = velx - dn * nx, uty = vely - dn * nr;
-          float up = len2(utx, uty);
-          float cp = Rm * (G + 1.0f);
-          float Taw = Tg + 0.89f * up * up / (2.0f * cp);
-          float Ts = fmaxf(Tg + 0.5f * (P.Tw - Tg) + 0.22f * (Taw - Tg), 1e-3f);
-          float rs = p / (Rm * Ts), mus = sutherland(Ts * P.gas[2], P);
-          float dz = 2.0f * clampf(0.5f * V / wl, 0.25f, 1.0f);
-          float nz = mus / (rs * dz);
-          float tw = up <= 69.7f * nz ? 2.0f * mus * up / dz
-                                      : rs * powf(7.187f * powf(nz, 1.142857f) + 0.13769f * powf(nz, 0.142857f) * up, 1.75f);
-          tw = fminf(tw, 0.3f * rho * up * V / fmaxf(wl * dt, 1e-9f));
-          if (up > 1e-6f) { L.y -= tw * wl * utx / up; L.z -= tw * wl * uty / up; }
-          float qw = tw / fmaxf(up, 1e-4f) * cp * (Taw - P.Tw) * 1.24f;
-          float qmax = 0.3f * p * G * V / fmaxf(wl * dt, 1e-9f);
-          L.w -= clampf(qw, -qmax, qmax) * wl;
-        }
-        // shock / boundary-layer interaction on the bit-16 band
-        if (sm_ & 16) {
-          float up = len2(velx, vely), Mn = up / sqrtf((1.0f + 1.0f / G) * p / rho);
-          if (Mn > 1.0f) {
-            float shx = velx / up, shy = vely / up;
-            float pd = 0.0f;
-            for (int n = 4; n <= 6; n += 2)
-              for (int mm = 0; mm <= 1; mm++) {
-                int Dx = Hx + int(rintf(float(n) * shx));
-                int Dy = Hy + int(floorf(float(n) * shy)) + mm;
-                Dx = min(max(Dx, 0), Nx - 1);
-                Dy = min(max(Dy, 0), Nr - 1);
-                float4 wd, sd;
-                interior_prim(g, a.A1, a.B1, Dx, Dy, wd, sd);
-                if (wd.x > 0.0f) pd = fmaxf(pd, wd.w);
-              }
-            float crit = 1.0f + 0.5f * Mn;
-            float fsep = smoothstepf(crit, 1.2f * crit, pd / p) * V * rho * up;
-            L.y -= fsep * velx;
-            L.z -= fsep * vely;
-          } else if (velx > 0.0f && p < 1.3f * P.chemK[3]) {
-            float fsep = 0.5f * V * rho * up;
-            L.y -= fsep * velx;
-            L.z -= fsep * vely;
-          }
-        }
-      }
-      float invV = dt / V;
-      float dO = invV * L.x;
-      L.x = 0.0f;
-      float4 U = make_float4(A.x + invV * L.x, A.y + invV * L.y, A.z + invV * L.z, A.w + invV * L.w);
-      float4 UY = make_float4(B.x + invV * LY.x / 1.0f, B.y + invV * LY.y / 1.0f, B.z + invV * LY.z / rho,
-                              B.w + invV * 0.0f / 1.0f);
-      if (P.inj) UY.w += dO;
-      if (P.chem) {
-        float Z = q.s.x, F = q.s.y, O = q.s.w, s = P.chemK[1];
-        float avail = P.inj ? fminf(F, (O + 0.233f * fmaxf(1.0f - Z, 0.0f)) / s)
-                            : fminf(F, fmaxf(1.0f - Z - s * (Z - F), 0.0f) / s);
-        if (avail > 1e-5f) {
-          float TK = Tg * P.gas[2];
-          float kin = P.chemK[2] * p * expf(-9000.0f / TK) * (1.0f - smoothstepf(P.cap[0], P.cap[1], TK));
-          float mixr = P.inj ? fmaxf(T2h.z, 4.0f * T2h.x / rho) : T2h.z;
-          float burn = avail * fminf(fminf(mixr, kin) * dt, 0.5f);
-          UY.y -= rho * burn;
-          if (P.inj) UY.w = fmaxf(UY.w - rho * burn * s, 0.0f);
-          U.w += rho * burn * P.chemK[0];
-        }
-      }
-      float rn = fmaxf(U.x, RHO_MIN);
-      float vnx = U.y / rn, vny = U.z / rn;
-      if (!(rn < 1e30f) || !(vnx < 1e30f && vnx > -1e30f)) {
-        oA = make_float4(P.ambCons[0], P.ambCons[1], P.ambCons[2], P.ambCons[3]);
-        oB = make_float4(P.ambB[0], P.ambB[1], P.ambB[2], P.ambB[3]);
+    float4 oA, oB, A = make_float4(0.f, 0.f, 0.f, 0.f), B = A;
+    float Bw = 0.0f;
+    if (!g.mask[k]) {
+      float4 gm = g.geoM[k];
+      const int Hx = i + iround(gm.x), Hy = j + iround(gm.y);
+      const int hx = Hx - x0, hy = Hy - y0;
+      int s;
+      if (hx >= 0 && hx < TX && hy >= 0 && hy < T::TY) {
+        s = hy * TX + hx;
       } else {
-        float Gn = clampf(UY.z, P.gamR[0], P.gamR[1]);
-        float Zn = clampf(UY.x, 0.0f, rn);
-        oA = make_float4(rn, rn * vnx, rn * vny, fmaxf(U.w, P_MIN * Gn + 0.5f * rn * (vnx * vnx + vny * vny)));
-        oB = make_float4(Zn, clampf(UY.y, 0.0f, Zn), Gn, P.inj ? clampf(UY.w, 0.0f, rn) : a.B2[k].w);
+        const int kh = Hy * Nx + Hx;
+        int e = 0;
+        while (e < xn - 1 && xc[e] != kh) e++;
+        s = NT + e;
       }
+      A = sA2[s];
+      B = sB2[s];
+      Bw = sB2[tid].w;
     }
-    a.oA[k] = oA;
-    a.oB[k] = oB;
-    if (a.finalCfl && fluid) wcell = wave_speed(oA, oB);
+    const bool fluid = source_cell<T>(g, p.A1, p.B1, P, i, j, dt, x0, y0, xc, xnP, sF, sY, sT1, sT2, A, B, Bw, oA, oB);
+    p.oA[k] = oA;
+    p.oB[k] = oB;
+    if (p.finalCfl && fluid) wcell = wave_speed(oA, oB);
   }
-  if (a.finalCfl) block_max_to<NT>(wcell, a.wOut, red);
+  if (p.finalCfl) block_max_to<NT>(wcell, p.wOut, red);
 }
 
 // --------------------------------------------------------------------------
@@ -579,11 +686,11 @@ __global__ void __launch_bounds__(T::NT, T::MINB) k_stage(StageArgs a, rn_params
   stage_body<T, STAGE>(a, P, blockIdx.x, blockIdx.y, blockIdx.y * gridDim.x + blockIdx.x, sm, red, xc);
 }
 template <class T>
-__global__ void __launch_bounds__(T::NT, T::MINB) k_physics(PhysArgs a, rn_params P) {
+__global__ void __launch_bounds__(T::NT, T::MINB) k_stage2phys(StageArgs a, PhysArgs p, rn_params P) {
   extern __shared__ float4 sm[];
   __shared__ float red[T::NT / 32];
   __shared__ int xc[MAXX];
-  physics_body<T>(a, P, blockIdx.x, blockIdx.y, blockIdx.y * gridDim.x + blockIdx.x, sm, red, xc);
+  stage2_physics_body<T>(a, p, P, blockIdx.x, blockIdx.y, blockIdx.y * gridDim.x + blockIdx.x, sm, red, xc);
 }
 
 // Batch kernels: block b belongs to instance blockInst[b]; its descriptor
@@ -623,7 +730,8 @@ __global__ void __launch_bounds__(T::NT, T::MINB) k_stage_batch(const BatchInst*
   stage_body<T, STAGE>(a, d.P, bx, by, local, sm, red, xc);
 }
 template <class T>
-__global__ void __launch_bounds__(T::NT, T::MINB) k_physics_batch(const BatchInst* insts, const int* blockInst, BatchPhase ph) {
+__global__ void __launch_bounds__(T::NT, T::MINB) k_stage2phys_batch(const BatchInst* insts, const int* blockInst,
+                                                                     BatchPhase ph) {
   extern __shared__ float4 sm[];
   __shared__ float red[T::NT / 32];
   __shared__ int xc[MAXX];
@@ -631,15 +739,24 @@ __global__ void __launch_bounds__(T::NT, T::MINB) k_physics_batch(const BatchIns
   load_inst(insts, blockInst, d);
   const int s0 = (d.cur0 + ph.shift) % 3, s1 = (s0 + 1) % 3, s2 = (s0 + 2) % 3;
   const int si = d.stepIdx0 ^ ph.par, ws = d.wslot0 ^ ph.par;
-  PhysArgs a;
+  StageArgs a;
   a.g = d.g;
-  a.A1 = d.SA[s1]; a.B1 = d.SB[s1]; a.A2 = d.SA[s2]; a.B2 = d.SB[s2]; a.oA = d.SA[s0]; a.oB = d.SB[s0];
-  a.st = d.stepTex + (1 - si);
+  a.A = d.SA[s1]; a.B = d.SB[s1]; a.A0 = d.SA[s0]; a.B0 = d.SB[s0]; a.oA = d.SA[s2]; a.oB = d.SB[s2];
+  a.stPrev = d.stepTex + si;
+  a.stNew = d.stepTex + (1 - si);
+  a.wIn = d.wmax + ws;
   a.wOut = d.wmax + (1 - ws);
-  a.finalCfl = ph.finalCfl;
+  a.finalCfl = 0;
   a.xoff = d.xoff; a.xcell = d.xcell; a.maxX = ph.maxX;
+  PhysArgs p;
+  p.g = d.g;
+  p.A1 = d.SA[s1]; p.B1 = d.SB[s1]; p.A2 = d.SA[s2]; p.B2 = d.SB[s2]; p.oA = d.SA[s2]; p.oB = d.SB[s2];
+  p.st = d.stepTex + (1 - si);
+  p.wOut = d.wmax + (1 - ws);
+  p.finalCfl = ph.finalCfl;
+  p.xoff = d.xoff; p.xcell = d.xcell; p.maxX = ph.maxX;
   const int local = blockIdx.x - d.firstBlock, by = local / d.tilesX, bx = local - by * d.tilesX;
-  physics_body<T>(a, d.P, bx, by, local, sm, red, xc);
+  stage2_physics_body<T>(a, p, d.P, bx, by, local, sm, red, xc);
 }
 
 // --------------------------------------------------------------------------
@@ -775,15 +892,15 @@ static dim3 tiles_of(const Grid& g) {
 
 template <class T>
 static int init_tile() {
-  const int ss = int(stage_smem_t<T>(MAXX)), ps = int(physics_smem_t<T>(MAXX));
+  const int ss = int(stage_smem_t<T>(MAXX)), ps = int(fused_smem_t<T>(MAXX));
   if (cudaFuncSetAttribute(k_stage<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss) != cudaSuccess) return -1;
   if (cudaFuncSetAttribute(k_stage<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss) != cudaSuccess) return -1;
-  if (cudaFuncSetAttribute(k_physics<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps) != cudaSuccess) return -1;
+  if (cudaFuncSetAttribute(k_stage2phys<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps) != cudaSuccess) return -1;
   if (cudaFuncSetAttribute(k_stage_batch<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss) != cudaSuccess)
     return -1;
   if (cudaFuncSetAttribute(k_stage_batch<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss) != cudaSuccess)
     return -1;
-  if (cudaFuncSetAttribute(k_physics_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps) != cudaSuccess)
+  if (cudaFuncSetAttribute(k_stage2phys_batch<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, ps) != cudaSuccess)
     return -1;
   return 0;
 }
@@ -799,9 +916,11 @@ void launch_stage2(const StageArgs& a, const rn_params& P, int tile, cudaStream_
   if (tile == 1) k_stage<Tile1, 2><<<tiles_of<Tile1>(a.g), Tile1::NT, stage_smem_t<Tile1>(a.maxX), s>>>(a, P);
   else k_stage<Tile0, 2><<<tiles_of<Tile0>(a.g), Tile0::NT, stage_smem_t<Tile0>(a.maxX), s>>>(a, P);
 }
-void launch_physics(const PhysArgs& a, const rn_params& P, int tile, cudaStream_t s) {
-  if (tile == 1) k_physics<Tile1><<<tiles_of<Tile1>(a.g), Tile1::NT, physics_smem_t<Tile1>(a.maxX), s>>>(a, P);
-  else k_physics<Tile0><<<tiles_of<Tile0>(a.g), Tile0::NT, physics_smem_t<Tile0>(a.maxX), s>>>(a, P);
+void launch_stage2phys(const StageArgs& a, const PhysArgs& p, const rn_params& P, int tile, cudaStream_t s) {
+  if (tile == 1)
+    k_stage2phys<Tile1><<<tiles_of<Tile1>(a.g), Tile1::NT, fused_smem_t<Tile1>(a.maxX), s>>>(a, p, P);
+  else
+    k_stage2phys<Tile0><<<tiles_of<Tile0>(a.g), Tile0::NT, fused_smem_t<Tile0>(a.maxX), s>>>(a, p, P);
 }
 void launch_batch_stage1(const BatchInst* d, const int* bi, int nb, BatchPhase ph, int tile, cudaStream_t s) {
   if (tile == 1) k_stage_batch<Tile1, 1><<<nb, Tile1::NT, stage_smem_t<Tile1>(ph.maxX), s>>>(d, bi, ph);
@@ -811,9 +930,9 @@ void launch_batch_stage2(const BatchInst* d, const int* bi, int nb, BatchPhase p
   if (tile == 1) k_stage_batch<Tile1, 2><<<nb, Tile1::NT, stage_smem_t<Tile1>(ph.maxX), s>>>(d, bi, ph);
   else k_stage_batch<Tile0, 2><<<nb, Tile0::NT, stage_smem_t<Tile0>(ph.maxX), s>>>(d, bi, ph);
 }
-void launch_batch_physics(const BatchInst* d, const int* bi, int nb, BatchPhase ph, int tile, cudaStream_t s) {
-  if (tile == 1) k_physics_batch<Tile1><<<nb, Tile1::NT, physics_smem_t<Tile1>(ph.maxX), s>>>(d, bi, ph);
-  else k_physics_batch<Tile0><<<nb, Tile0::NT, physics_smem_t<Tile0>(ph.maxX), s>>>(d, bi, ph);
+void launch_batch_stage2phys(const BatchInst* d, const int* bi, int nb, BatchPhase ph, int tile, cudaStream_t s) {
+  if (tile == 1) k_stage2phys_batch<Tile1><<<nb, Tile1::NT, fused_smem_t<Tile1>(ph.maxX), s>>>(d, bi, ph);
+  else k_stage2phys_batch<Tile0><<<nb, Tile0::NT, fused_smem_t<Tile0>(ph.maxX), s>>>(d, bi, ph);
 }
 void launch_reduce(const Grid& g, const float4* A, const float4* B, unsigned* w, cudaStream_t s) {
   int N = g.Nx * g.Nr;

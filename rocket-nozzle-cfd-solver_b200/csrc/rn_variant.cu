@@ -20,10 +20,10 @@ const KernelSet RN_CAT(kernels_, RN_VARIANT) = {
     RN_STR(RN_VARIANT),
     RN_VARIANT::launch_stage1,
     RN_VARIANT::launch_stage2,
-    RN_VARIANT::launch_physics,
+    RN_VARIANT::launch_stage2phys,
     RN_VARIANT::launch_batch_stage1,
     RN_VARIANT::launch_batch_stage2,
-    RN_VARIANT::launch_batch_physics,
+    RN_VARIANT::launch_batch_stage2phys,
     RN_VARIANT::launch_reduce,
     RN_VARIANT::launch_rescale,
     RN_VARIANT::launch_wallrow,

@@ -38,7 +38,7 @@ EXPORTS = ("rn_create", "rn_destroy", "rn_resize", "rn_set_mask", "rn_set_geomet
            "rn_last_error")
 PRECISION = {"fast": 0, "exact": 1}
 TILES = {"16x16": 0, "16x8": 1}
-KERNEL_KINDS = ("reduce", "stage1", "stage2", "physics", "parcels", "apply", "other")
+KERNEL_KINDS = ("reduce", "stage1", "stage2", "physics", "parcels", "apply", "other", "stage2_physics")
 
 
 class RnError(RuntimeError):

@@ -259,10 +259,10 @@ def test_kernel_launch_accounting(rn):
     n0 = g.kernelLaunches()
     g.step(10, s.P)
     g.sync()
-    assert g.kernelLaunches() - n0 == 1 + 3 * 10         # first-step CFL reduction + 3 kernels per step
+    assert g.kernelLaunches() - n0 == 1 + 2 * 10         # first-step CFL reduction + 2 kernels per step
     g.profile(True)
     g.step(5, s.P)
     prof = g.profileRead()
-    assert prof["stage1"][1] == 5 and prof["stage2"][1] == 5 and prof["physics"][1] == 5
+    assert prof["stage1"][1] == 5 and prof["stage2_physics"][1] == 5 and prof["stage2"][1] == 0
     assert all(v[0] > 0 for k, v in prof.items() if v[1])
     g.close()
