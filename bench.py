@@ -118,9 +118,12 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+GRID = (512, 192)
+
+
 def make_setup(rn):
     from rocket_nozzle_cfd_solver_b200.configs import viscous_plume
-    cfg, _ = viscous_plume(Nx=512, Nr=192)
+    cfg, _ = viscous_plume(Nx=GRID[0], Nr=GRID[1])
     return rn.build_sim_setup(cfg)
 
 
@@ -526,6 +529,7 @@ def run_serving(args):
 
 
 def main():
+    global GRID, SOLVER_STEPS, WORKLOAD
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=50)
@@ -535,10 +539,18 @@ def main():
     ap.add_argument("--batch-instances", type=int, default=64,
                     help="instances of the batched workload measured after the main line's (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=30, help="time steps per batched bench step")
+    ap.add_argument("--grid", default="512x192",
+                    help="grid of the main viscous-plume leg (other sizes are for profiling; the bench line's "
+                         "workload is 512x192)")
+    ap.add_argument("--solver-steps", type=int, default=SOLVER_STEPS, help="time steps per bench step")
     ap.add_argument("--no-large", action="store_true", help="skip the 4096x1536 HBM-resident sweep point")
     ap.add_argument("--serve-requests", type=int, default=24, help="requests of the serving leg (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=5.0, help="Poisson arrival rate of the serving leg (1/s)")
     args = ap.parse_args()
+    GRID = tuple(int(v) for v in args.grid.lower().split("x"))
+    SOLVER_STEPS = args.solver_steps
+    if GRID != (512, 192):
+        WORKLOAD = WORKLOAD.replace("512x192", f"{GRID[0]}x{GRID[1]}")
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
