@@ -216,6 +216,48 @@ int rn_batch_kernel_launches(rn_batch b, long long* out);
 int rn_residual_mark(rn_handle h);
 int rn_residual(rn_handle h, double out[6]);
 
+/* Flow-separation read-out on the device (wallSeparation, simsetup.js:352-373):
+ * walks the near-wall row (the FS_WALLROW values, solver.js:665-674, built on
+ * the fly from the current state and jWall) upstream from iExit and returns
+ * the separation column with its FP64 read-outs; only these scalars reach the
+ * host. rn_set_wall_profile uploads, per column i (x = (i + 0.5) dx), the wall
+ * slope (R(x + dx/2) - R(x - dx/2)) / dx, hypot(1, slope) and R(x), in metres,
+ * once per geometry. found = 0 where the reference returns null. */
+typedef struct {
+  int iThroat, iExit;
+  double dx, xt, xe, Rt;   /* metres */
+  double paSi, pRef;       /* ambient pressure (Pa) and the pressure unit P_REF (Pa) */
+} rn_separation_spec;
+typedef struct {
+  int found, last;         /* last = separation column (or -1) */
+  double x, frac, eps, pRatio, Msep;
+} rn_separation_out;
+int rn_set_wall_profile(rn_handle h, const double* slope, const double* hyp, const double* radius);
+int rn_wall_separation(rn_handle h, const rn_separation_spec* spec, rn_separation_out* out);
+
+/* Derived display fields into a headless device buffer (FS_DERIVED,
+ * render.js:60-134): per cell (t, Z, normalised T, Mach) with t the selected
+ * field mapped to its display range, (0, 0, 0, -1) in walls. field is the
+ * reference's uField: 0 temperature, 1 Mach, 2 schlieren, 3 log10 p, 4 log10
+ * rho, 5 speed, 6 vorticity, 7 exhaust fraction, 9 log10 eddy/laminar
+ * viscosity, 10 unburnt fraction, 11 fuel vapour, 12 oxidiser, 13 burning rate.
+ * The spec carries the shader's uniforms. Fields 9 and 13 need P (the
+ * step's parameter block) and read the split step's T2, recomputed from the
+ * last step's stage-1 state (0 if no step ran since the state was set). The
+ * buffer (Nx*Nr float4) belongs to the handle (rn_derived_buffer gives its
+ * device address); `out` (Nx*Nr*4 floats) may be NULL. No reference
+ * counterpart for the buffer: the reference draws it to the screen. */
+typedef struct {
+  int field;
+  float range[2];           /* uRange */
+  float RaN, Rs[3];         /* uRaN, uRs */
+  float chemV[4];           /* uChemV */
+  float Tscale[4];          /* uTscale: (T_REF, Tc K, Ta K, unused) */
+  float schlGain, velScale, dx;
+} rn_derived_spec;
+int rn_derived(rn_handle h, const rn_derived_spec* spec, const rn_params* P, float* out);
+int rn_derived_buffer(rn_handle h, void** dev);
+
 /* Solve server: continuous batching of whole solves on one GPU (no
  * reference counterpart; the reference runs one interactive solve per page).
  * rn_serve_submit copies a request (grid, geometry, initial state, P, stop

@@ -80,6 +80,7 @@ def lib():
         L.rno_get_state.argtypes = [vp, dptr, dptr]
         L.rno_get_step_info.argtypes = [vp, dptr]
         L.rno_get_wall_row.argtypes = [vp, dptr]
+        L.rno_get_t2.argtypes = [vp, dptr]
         L.rno_get_parcels.argtypes = [vp, dptr, dptr, dptr]
         L.rno_get_spray_counters.argtypes = [vp, np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")]
         L.rno_get_src.argtypes = [vp, dptr]
@@ -149,6 +150,12 @@ class OracleSolver:
     def readWallRow(self):
         o = np.empty(self.Nx * 4)
         lib().rno_get_wall_row(self.h, o)
+        return o
+
+    def readT2(self):
+        """T2 of the last physics pass (effective viscosity, h, strain, laminar viscosity)."""
+        o = np.empty(self.Nx * self.Nr * 4)
+        lib().rno_get_t2(self.h, o)
         return o
 
     def readParcels(self):

@@ -1018,6 +1018,11 @@ void rno_get_wall_row(void* hp, double* out) {
   Handle* h = static_cast<Handle*>(hp);
   if (h->fp64) { h->d.drawWallRow(); copy_out(h->d.wallRow, out); } else { h->f.drawWallRow(); copy_out(h->f.wallRow, out); }
 }
+// the split step's cell data T2 of the last physics pass (solver.js:458-488), N x 4
+void rno_get_t2(void* hp, double* out) {
+  Handle* h = static_cast<Handle*>(hp);
+  if (h->fp64) copy_out(h->d.T2, out); else copy_out(h->f.T2, out);
+}
 // parcels of the current parcel slot: PA, PB (each 65536 x 4) and PC of that slot
 void rno_get_parcels(void* hp, double* PA, double* PB, double* PC) {
   Handle* h = static_cast<Handle*>(hp);

@@ -59,9 +59,12 @@ void free_buffers(rn_solver* h) {
   cudaFree(h->src); cudaFree(h->tab); cudaFree(h->dep); cudaFree(h->key); cudaFree(h->sortTemp);
   cudaFree(h->xoff); cudaFree(h->xcell);
   h->xoff = h->xcell = nullptr;
-  cudaFree(h->mark); cudaFree(h->dRes);
+  cudaFree(h->mark); cudaFree(h->dRes); cudaFree(h->wallProf); cudaFree(h->derived);
   h->mark = h->markSt = nullptr;
   h->dRes = nullptr;
+  h->wallProf = nullptr;
+  h->derived = nullptr;
+  h->s1last = -1;
   h->maxX = 1;
   h->geoA = h->geoG = h->geoM = h->jw = h->wallRow = nullptr;
   h->mask = nullptr; h->stepTex = nullptr; h->wmax = nullptr; h->dInt = nullptr;
@@ -375,7 +378,7 @@ int rn_set_state(rn_handle h, const float* A, const float* B) {
     CK(cudaMemcpyAsync(h->SB[s], B, sizeof(float4) * N, cudaMemcpyHostToDevice, h->stream));
   }
   CK(cudaMemsetAsync(h->stepTex, 0, sizeof(float4) * 2, h->stream));
-  h->cur = 0; h->stepIdx = 0; h->stepCount = 0; h->wvalid = false;
+  h->cur = 0; h->stepIdx = 0; h->stepCount = 0; h->wvalid = false; h->s1last = -1;
   return spray_reset_dev(h);
 }
 
@@ -470,6 +473,7 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
     h->stepIdx = 1 - h->stepIdx;
     h->wslot = 1 - h->wslot;
     h->wvalid = true;
+    h->s1last = s1;
     h->stepCount++;
   }
   cudaError_t e = cudaGetLastError();
@@ -487,6 +491,7 @@ int rn_rescale_ambient(rn_handle h, float fp, float fT, float du, const rn_param
   h->launches++;
   h->cur = s1;
   h->wvalid = false;
+  h->s1last = -1;
   CK(cudaGetLastError());
   return RN_OK;
 }

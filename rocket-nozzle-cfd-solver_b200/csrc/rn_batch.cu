@@ -479,6 +479,7 @@ int rn_batch_step(rn_batch b, int n) {
       h->wslot = 1 - h->wslot;
     }
     h->wvalid = true;
+    h->s1last = f.inj ? (h->cur + 1) % 3 : (h->cur + 2) % 3;   // the last step's stage-1 slot
     h->stepCount += n;
   }
   // later work of each member waits for the batch

@@ -58,6 +58,12 @@ struct rn_solver {
   float4* mark = nullptr;
   float4* markSt = nullptr;
   double* dRes = nullptr;
+  // per-column wall slope, hypot(1, slope) and radius for rn_wall_separation
+  double* wallProf = nullptr;
+  // derived-field buffer (rn_derived) and the ring slot of the last step's
+  // stage-1 state (-1 when no step has run since the state was set)
+  float4* derived = nullptr;
+  int s1last = -1;
   // the batch this handle is stepped by, if any (rn_batch.cu)
   struct rn_batch_t* batch = nullptr;
 

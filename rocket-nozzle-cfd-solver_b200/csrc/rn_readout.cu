@@ -1,4 +1,5 @@
-// rn_readout.cu -- steady-state residual of a solver handle (declared in rn.h).
+// rn_readout.cu -- device read-outs of a solver handle (declared in rn.h):
+// the steady-state residual and the flow-separation point.
 //
 // No reference counterpart: the reference has no convergence measure (its
 // frame loop runs until the user stops it). The residual is the RMS over fluid
@@ -10,7 +11,9 @@
 // Neumaier sums in a fixed cell order, a fixed shared-memory tree per block and
 // an in-order sum of the block partials.
 #include <cuda_runtime.h>
+#include <math.h>
 #include <string>
+#include <vector>
 #include "rn.h"
 #include "rn_internal.h"
 
@@ -122,6 +125,99 @@ int rn_residual(rn_handle h, double out[6]) {
   if (rc != RN_OK) return rc;
   RN_CK(cudaMemcpyAsync(out, h->dRes, sizeof(double) * 6, cudaMemcpyDeviceToHost, h->stream));
   RN_CK(cudaStreamSynchronize(h->stream));
+  return RN_OK;
+}
+
+}  // extern "C"
+
+// --------------------------------------------------------------------------
+// Flow-separation read-out on the device (wallSeparation, simsetup.js:352-373):
+// one thread walks the near-wall row upstream from the exit, building each
+// row entry exactly as FS_WALLROW does (solver.js:665-674), and returns the
+// separation column, its pressure ratio and Mach number in FP64. Only the
+// scalars cross to the host, not the wall row.
+namespace {
+
+__device__ float4 wall_row_entry(const rn::Grid& g, const float4* __restrict__ A, const float4* __restrict__ B,
+                                 const float4* __restrict__ jw, int i) {
+  int cj = int(jw[i].x);
+  cj = min(max(cj, 0), g.Nr - 1);
+  rn::Prim q = rn::to_prim(A[cj * g.Nx + i], B[cj * g.Nx + i]);
+  return make_float4(q.w.y, q.w.z, q.w.w, rn::sound_speed(q));
+}
+
+// prof: per column (slope, hypot(1, slope), R(x_i)); out: found, last, x, frac, eps, pRatio, Msep
+__global__ void k_separation(rn::Grid g, const float4* __restrict__ A, const float4* __restrict__ B,
+                             const float4* __restrict__ jw, const double* __restrict__ prof,
+                             rn_separation_spec sp, double* out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  int i = sp.iExit, gaps = 0, last = -1;
+  for (; i > sp.iThroat + 2 && gaps <= 2; i--) {
+    const float4 r = wall_row_entry(g, A, B, jw, i);
+    const double u = r.x, v = r.y, c = r.w;
+    const double ut = (u + prof[3 * i] * v) / prof[3 * i + 1];
+    if (ut < 0.0 || sqrt(u * u + v * v) < 0.6 * c) { last = i; gaps = 0; }
+    else if (last >= 0 || sp.iExit - i > 2) gaps++;
+  }
+  for (int q = 0; q < 8; q++) out[q] = 0.0;
+  out[1] = double(last);
+  if (last < 0 || sp.iExit - last < 3) return;
+  double pSep = INFINITY;
+  int kS = last;
+  for (int q = last; q >= max(sp.iThroat + 1, last - 30); q--) {
+    const double p = wall_row_entry(g, A, B, jw, q).z;
+    if (p < pSep) { pSep = p; kS = q; }
+  }
+  const float4 rs = wall_row_entry(g, A, B, jw, kS);
+  const double us = rs.x, vs = rs.y;
+  const double Msep = sqrt(us * us + vs * vs) / fmax(double(rs.w), 1e-6);
+  out[6] = Msep;
+  if (Msep < 1.05) return;
+  const double x = (last + 0.5) * sp.dx, R = prof[3 * last + 2];
+  out[0] = 1.0;
+  out[2] = x;
+  out[3] = (x - sp.xt) / (sp.xe - sp.xt);
+  out[4] = (R * R) / (sp.Rt * sp.Rt);
+  out[5] = pSep * sp.pRef / fmax(sp.paSi, 1e-6);
+}
+
+}  // namespace
+
+extern "C" {
+
+int rn_set_wall_profile(rn_handle h, const double* slope, const double* hyp, const double* radius) {
+  if (!h || !h->SA[0] || !slope || !hyp || !radius) return rn_record_error(RN_ERR_ARG, "rn_set_wall_profile: bad argument");
+  std::vector<double> prof(size_t(h->Nx) * 3);
+  for (int i = 0; i < h->Nx; i++) {
+    prof[3 * i] = slope[i];
+    prof[3 * i + 1] = hyp[i];
+    prof[3 * i + 2] = radius[i];
+  }
+  if (!h->wallProf) RN_CK(cudaMalloc(&h->wallProf, sizeof(double) * prof.size()));
+  RN_CK(cudaMemcpyAsync(h->wallProf, prof.data(), sizeof(double) * prof.size(), cudaMemcpyHostToDevice, h->stream));
+  RN_CK(cudaStreamSynchronize(h->stream));
+  return RN_OK;
+}
+
+int rn_wall_separation(rn_handle h, const rn_separation_spec* spec, rn_separation_out* out) {
+  if (!h || !h->SA[0] || !spec || !out) return rn_record_error(RN_ERR_ARG, "rn_wall_separation: bad argument");
+  if (!h->wallProf) return rn_record_error(RN_ERR_STATE, "rn_wall_separation: no wall profile (rn_set_wall_profile)");
+  if (spec->iExit < 0 || spec->iExit >= h->Nx || spec->iThroat < -1 || spec->iThroat >= h->Nx)
+    return rn_record_error(RN_ERR_ARG, "rn_wall_separation: column out of range");
+  if (!h->dRes) RN_CK(cudaMalloc(&h->dRes, sizeof(double) * (8 + RES_BLOCKS * RES_Q)));
+  k_separation<<<1, 32, 0, h->stream>>>(h->grid(), h->SA[h->cur], h->SB[h->cur], h->jw, h->wallProf, *spec, h->dRes);
+  h->launches++;
+  RN_CK(cudaGetLastError());
+  double r[8];
+  RN_CK(cudaMemcpyAsync(r, h->dRes, sizeof(r), cudaMemcpyDeviceToHost, h->stream));
+  RN_CK(cudaStreamSynchronize(h->stream));
+  out->found = r[0] != 0.0;
+  out->last = int(r[1]);
+  out->x = r[2];
+  out->frac = r[3];
+  out->eps = r[4];
+  out->pRatio = r[5];
+  out->Msep = r[6];
   return RN_OK;
 }
 

@@ -34,7 +34,8 @@ EXPORTS = ("rn_create", "rn_destroy", "rn_resize", "rn_set_mask", "rn_set_geomet
            "rn_batch_step", "rn_batch_sync", "rn_batch_set_tile", "rn_batch_autotune", "rn_batch_stream",
            "rn_batch_kernel_launches", "rn_residual_mark", "rn_residual", "rn_server_default_opts",
            "rn_server_create", "rn_server_destroy", "rn_serve_submit", "rn_serve_poll", "rn_serve_wait",
-           "rn_serve_stats", "rn_solve_bytes",
+           "rn_serve_stats", "rn_solve_bytes", "rn_set_wall_profile", "rn_wall_separation", "rn_derived",
+           "rn_derived_buffer",
            "rn_last_error")
 PRECISION = {"fast": 0, "exact": 1}
 TILES = {"16x16": 0, "16x8": 1}
@@ -105,6 +106,39 @@ class RnSolveResult(ctypes.Structure):
 class RnServeStatus(ctypes.Structure):
     _fields_ = [(n, ctypes.c_longlong) for n in ("queued", "active", "finished", "bytes_used", "bytes_budget",
                                                   "ticks", "admitted", "failed")]
+
+
+class RnSeparationSpec(ctypes.Structure):
+    _fields_ = [("iThroat", ctypes.c_int), ("iExit", ctypes.c_int)] + \
+               [(n, ctypes.c_double) for n in ("dx", "xt", "xe", "Rt", "paSi", "pRef")]
+
+
+class RnSeparationOut(ctypes.Structure):
+    _fields_ = [("found", ctypes.c_int), ("last", ctypes.c_int)] + \
+               [(n, ctypes.c_double) for n in ("x", "frac", "eps", "pRatio", "Msep")]
+
+
+class RnDerivedSpec(ctypes.Structure):
+    _fields_ = [("field", ctypes.c_int), ("range", ctypes.c_float * 2), ("RaN", ctypes.c_float),
+                ("Rs", ctypes.c_float * 3), ("chemV", ctypes.c_float * 4), ("Tscale", ctypes.c_float * 4),
+                ("schlGain", ctypes.c_float), ("velScale", ctypes.c_float), ("dx", ctypes.c_float)]
+
+
+# the reference's display fields in uField order (render.js:8-23)
+FIELDS = ("temp", "mach", "schl", "pres", "dens", "vel", "vort", "exh", "flame", "turb", "burn", "fuel", "ox",
+          "heat")
+
+
+def derived_spec(setup, field, value_range=(0.0, 1.0), schl_gain=10.0, Tc=None):
+    """Uniforms of the derived-field pass as app.js sets them (app.js:376-383,
+    render.js:427-434): gas constants and chemistry of P, (T_REF, Tc, Ta),
+    the schlieren gain, U_REF and dx. ``field`` is a FIELDS name or index."""
+    from .physics import T_REF, U_REF
+    P = setup["P"]
+    return {"field": FIELDS.index(field) if isinstance(field, str) else int(field),
+            "range": tuple(value_range), "RaN": P["RaN"], "Rs": tuple(P["Rs"]), "chemV": tuple(P["chemK"]),
+            "Tscale": (T_REF, Tc if Tc is not None else setup["cfg"]["Tc"], P["Ta"], 0.0),
+            "schlGain": schl_gain, "velScale": U_REF, "dx": setup["dx"]}
 
 
 SOLVE_STATUS = {0: "converged", 1: "time", 2: "max_steps", -1: "rejected", -2: "failed"}
@@ -227,6 +261,11 @@ def lib():
                                 ctypes.c_void_p]
     L.rn_serve_stats.argtypes = [H, ctypes.POINTER(RnServeStatus)]
     L.rn_solve_bytes.argtypes = [i, i, ctypes.POINTER(ctypes.c_longlong)]
+    dp = ctypes.POINTER(ctypes.c_double)
+    L.rn_set_wall_profile.argtypes = [H, dp, dp, dp]
+    L.rn_wall_separation.argtypes = [H, ctypes.POINTER(RnSeparationSpec), ctypes.POINTER(RnSeparationOut)]
+    L.rn_derived.argtypes = [H, ctypes.POINTER(RnDerivedSpec), ctypes.POINTER(RnParams), ctypes.c_void_p]
+    L.rn_derived_buffer.argtypes = [H, ctypes.POINTER(ctypes.c_void_p)]
     L.rn_last_error.restype = ctypes.c_char_p
     for n in EXPORTS[:-1]:
         getattr(L, n).restype = ctypes.c_int
@@ -401,6 +440,62 @@ class GPUSolver:
         o = RnIntegralsOut()
         _check(lib().rn_integrals(self.h, ctypes.byref(integral_spec(setup)), ctypes.byref(o)))
         return {n: getattr(o, n) for n, _ in RnIntegralsOut._fields_}
+
+    def wallSeparation(self, setup, paSi):
+        """Separation point of the current state, evaluated on the device
+        (wallSeparation, simsetup.js:352-373): None where the reference returns
+        null, else {x, frac, eps, pRatio, Msep}. The wall profile of ``setup``
+        is uploaded on first use."""
+        from .physics import P_REF
+        c, dx, Nx = setup["contour"], setup["dx"], self.Nx
+        if getattr(self, "_wall_profile_of", None) is not setup:
+            slope = np.empty(Nx)
+            hyp = np.empty(Nx)
+            rad = np.empty(Nx)
+            for i in range(Nx):
+                x = (i + 0.5) * dx
+                slope[i] = (c.radiusAt(x + 0.5 * dx) - c.radiusAt(x - 0.5 * dx)) / dx
+                hyp[i] = math.hypot(1, slope[i])
+                rad[i] = c.radiusAt(x)
+            dp = ctypes.POINTER(ctypes.c_double)
+            _check(lib().rn_set_wall_profile(self.h, slope.ctypes.data_as(dp), hyp.ctypes.data_as(dp),
+                                             rad.ctypes.data_as(dp)))
+            self._wall_profile_of = setup
+        sp = RnSeparationSpec()
+        sp.iThroat, sp.iExit = setup["iThroat"], setup["iExit"]
+        sp.dx, sp.xt, sp.xe, sp.Rt = dx, c.xt, c.xe, c.Rt
+        sp.paSi, sp.pRef = float(paSi), float(P_REF)
+        o = RnSeparationOut()
+        _check(lib().rn_wall_separation(self.h, ctypes.byref(sp), ctypes.byref(o)))
+        if not o.found:
+            return None
+        return {"x": o.x, "frac": o.frac, "eps": o.eps, "pRatio": o.pRatio, "Msep": o.Msep}
+
+    def derived(self, spec, P=None, read=True):
+        """Derived display field (FS_DERIVED, render.js:60-134) into the
+        handle's device buffer; returns it as Nx*Nr*4 float32 (t, Z, Tn, M)
+        when ``read``. ``spec`` from derived_spec(); fields 'turb' and 'heat'
+        need the step's parameter block P."""
+        sp = RnDerivedSpec()
+        sp.field = int(spec["field"])
+        sp.range[0], sp.range[1] = spec["range"]
+        sp.RaN = spec["RaN"]
+        for k in range(3):
+            sp.Rs[k] = spec["Rs"][k]
+        for k in range(4):
+            sp.chemV[k] = spec["chemV"][k]
+            sp.Tscale[k] = spec["Tscale"][k]
+        sp.schlGain, sp.velScale, sp.dx = spec["schlGain"], spec["velScale"], spec["dx"]
+        p = None if P is None else ctypes.byref(P if isinstance(P, RnParams) else params_from_P(P))
+        out = np.empty(self.Nx * self.Nr * 4, np.float32) if read else None
+        _check(lib().rn_derived(self.h, ctypes.byref(sp), p, out.ctypes.data if read else None))
+        return out
+
+    def derivedBuffer(self):
+        """Device address of the derived-field buffer (0 before the first derived())."""
+        v = ctypes.c_void_p()
+        _check(lib().rn_derived_buffer(self.h, ctypes.byref(v)))
+        return v.value or 0
 
     def residualMark(self):
         """Snapshot the current state for residual()."""

@@ -51,6 +51,10 @@ int main(void) {
   F(rn_server_opts, max_active) F(rn_server_opts, tile) F(rn_solve_request, mask) F(rn_solve_request, injTab)
   F(rn_solve_request, P) F(rn_solve_request, spec) F(rn_solve_request, drop) F(rn_solve_request, max_steps)
   F(rn_solve_result, steps) F(rn_solve_result, done_ms) F(rn_solve_result, integrals) F(rn_serve_status, failed)
+  printf("rn_separation_spec %zu\nrn_separation_out %zu\n", sizeof(rn_separation_spec), sizeof(rn_separation_out));
+  F(rn_separation_spec, dx) F(rn_separation_spec, pRef) F(rn_separation_out, x) F(rn_separation_out, Msep)
+  printf("rn_derived_spec %zu\n", sizeof(rn_derived_spec));
+  F(rn_derived_spec, range) F(rn_derived_spec, chemV) F(rn_derived_spec, Tscale) F(rn_derived_spec, dx)
   return 0;
 }
 """
@@ -73,8 +77,10 @@ def test_struct_layout_matches_header(rn):
     classes = {"rn_params": solver.RnParams, "rn_integral_spec": solver.RnIntegralSpec,
                "rn_integrals_out": solver.RnIntegralsOut, "rn_server_opts": solver.RnServerOpts,
                "rn_solve_request": solver.RnSolveRequest, "rn_solve_result": solver.RnSolveResult,
-               "rn_serve_status": solver.RnServeStatus}
-    for t in ("rn_server_opts", "rn_solve_request", "rn_solve_result", "rn_serve_status"):
+               "rn_serve_status": solver.RnServeStatus, "rn_separation_spec": solver.RnSeparationSpec,
+               "rn_separation_out": solver.RnSeparationOut, "rn_derived_spec": solver.RnDerivedSpec}
+    for t in ("rn_server_opts", "rn_solve_request", "rn_solve_result", "rn_serve_status", "rn_separation_spec",
+              "rn_separation_out", "rn_derived_spec"):
         assert c[t] == ctypes.sizeof(classes[t]), t
     for key, v in c.items():
         if "." in key:

@@ -133,3 +133,29 @@ def test_cold_gas_thrust_near_one_d_theory(rn, oracle):
     assert perf["F"] == pytest.approx(th["F"], rel=0.10)
     ch = rn.cell_prim_si(s, A[0, s.iChamber], B[0, s.iChamber])
     assert abs(ch["p"] - 20e5) / 20e5 < 0.25                # the reference self-test's chamber criterion
+
+
+def test_derived_restatement_on_a_uniform_state():
+    """oracle/derived.py (FS_DERIVED restatement) on a uniform gas at rest and
+    in motion: temperature, Mach, speed and zero vorticity / schlieren."""
+    import importlib.util
+    path = os.path.join(os.path.dirname(HERE), "oracle", "derived.py")
+    spec = importlib.util.spec_from_file_location("oracle_derived", path)
+    D = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(D)
+    Nx, Nr = 6, 4
+    rho, u, p, G = 1.0, 0.5, 1.0, 2.5
+    A = np.tile(np.float32([rho, rho * u, 0.0, p * G + 0.5 * rho * u * u]), Nx * Nr)
+    B = np.tile(np.float32([0.0, 0.0, G, 0.0]), Nx * Nr)
+    mask = np.zeros(Nx * Nr, np.uint8)
+    mask[0] = 1
+    base = {"range": (0.0, 1.0), "RaN": 1.0, "Rs": (1.0, 1.0, 1.0), "chemV": (0, 1, 1, 0),
+            "Tscale": (300.0, 3000.0, 300.0, 0.0), "schlGain": 10.0, "velScale": 100.0, "dx": 0.01}
+    c = np.sqrt(1.4 * p / rho)
+    out = {F: D.derived(A, B, mask, Nx, Nr, dict(base, field=F)).reshape(Nr, Nx, 4) for F in (0, 1, 2, 5, 6)}
+    assert np.allclose(out[0][1:, 1:, 0], 300.0)                   # T = p/(rho R) T_REF, mapped with range (0, 1)
+    assert np.allclose(out[1][1:, 1:, 0], u / c, rtol=1e-6)
+    assert np.allclose(out[2][1:, 1:, 0], 0.0)
+    assert np.allclose(out[5][1:, 1:, 0], u * 100.0)
+    assert np.allclose(out[6][1:, 1:, 0], 0.0)
+    assert np.all(out[0][0, 0] == (0, 0, 0, -1))
