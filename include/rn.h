@@ -258,6 +258,41 @@ typedef struct {
 int rn_derived(rn_handle h, const rn_derived_spec* spec, const rn_params* P, float* out);
 int rn_derived_buffer(rn_handle h, void** dev);
 
+/* Cut-cell geometry builder on the device (buildCutGeometry, cutcell.js:14-186,
+ * plus buildSimSetup's geoM turbulence length and boundary-layer band,
+ * simsetup.js:51-63, and the near-wall row jWall): builds the handle's mask,
+ * geoA, geoG, geoM and jWall in place of rn_set_geometry, bit-identical to the
+ * host builder. Lengths in cells unless stated. The wall enters as the
+ * reference's Float32Array radius table Rtab (Nx*8+1 entries, cutcell.js:22)
+ * and as RinAt(x) at the abscissae the builder samples, per column i
+ * (RN_CUT_SAMPLES doubles): x = i, i + 0.5, i + (a + 0.5)/8 (a < 8),
+ * i + (b + 0.5)/12 (b < 12), i + 1; each entry is read only where
+ * x <= xeC. rinCol is the setup's Float32Array of the wall radius at the column
+ * centres in metres (+inf beyond the exit). No reference counterpart for the
+ * device placement (the reference builds on the CPU). */
+#define RN_CUT_SAMPLES 23
+typedef struct {
+  int Nx, Nr;
+  int cut;                  /* wallModel 'cut' (1) or 'stair' (0) */
+  int base;                 /* base / boat-tail body present */
+  int nSolids;              /* chamber hardware blocks (at most 64) */
+  int iExit;                /* jWall is set for columns 0..iExit */
+  double xeC, twC, xBaseC, bodyC;
+  double dx, xt, xe, Rt;    /* metres */
+  const float* Rtab;
+  const double* rin;        /* Nx * RN_CUT_SAMPLES */
+  const double* solids;     /* nSolids * (x0, x1, r0, r1) */
+  const float* rinCol;      /* Nx */
+} rn_cut_spec;
+typedef struct {
+  int nCut, nMerged;        /* fluid cells with kappa < 0.98; merged slivers */
+} rn_cut_stats;
+int rn_build_geometry(rn_handle h, const rn_cut_spec* spec, rn_cut_stats* stats);
+/* the handle's geometry planes back on the host (any pointer may be NULL);
+ * sizes as rn_set_geometry's, jWall Nx float4. No reference counterpart (the
+ * reference keeps its geometry on the host). */
+int rn_get_geometry(rn_handle h, uint8_t* mask, float* geoA, float* geoG, float* geoM, float* jWall);
+
 /* Solve server: continuous batching of whole solves on one GPU (no
  * reference counterpart; the reference runs one interactive solve per page).
  * rn_serve_submit copies a request (grid, geometry, initial state, P, stop

@@ -370,6 +370,18 @@ int rn_set_geometry(rn_handle h, const uint8_t* mask, const float* geoA, const f
   return RN_OK;
 }
 
+int rn_get_geometry(rn_handle h, uint8_t* mask, float* geoA, float* geoG, float* geoM, float* jWall) {
+  if (!valid(h)) return fail(RN_ERR_ARG, "rn_get_geometry: bad handle");
+  const size_t N = size_t(h->Nx) * h->Nr, NF = size_t(h->Nx + 1) * (h->Nr + 1);
+  if (mask) CK(cudaMemcpyAsync(mask, h->mask, N, cudaMemcpyDeviceToHost, h->stream));
+  if (geoA) CK(cudaMemcpyAsync(geoA, h->geoA, sizeof(float4) * NF, cudaMemcpyDeviceToHost, h->stream));
+  if (geoG) CK(cudaMemcpyAsync(geoG, h->geoG, sizeof(float4) * N, cudaMemcpyDeviceToHost, h->stream));
+  if (geoM) CK(cudaMemcpyAsync(geoM, h->geoM, sizeof(float4) * N, cudaMemcpyDeviceToHost, h->stream));
+  if (jWall) CK(cudaMemcpyAsync(jWall, h->jw, sizeof(float4) * h->Nx, cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return RN_OK;
+}
+
 int rn_set_state(rn_handle h, const float* A, const float* B) {
   if (!valid(h) || !A || !B) return fail(RN_ERR_ARG, "rn_set_state: bad argument");
   const size_t N = size_t(h->Nx) * h->Nr;

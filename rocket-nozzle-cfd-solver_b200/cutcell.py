@@ -85,6 +85,32 @@ class _Walls:
         return ok
 
 
+CUT_SAMPLES = 23     # RinAt abscissae per column handed to the device builder (rn.h RN_CUT_SAMPLES)
+
+
+def sample_abscissae(i):
+    """The x (cells) at which the builder evaluates RinAt in column i: the
+    x-face, the centre, the 8 volume and 12 r-face sub-samples, the next x-face."""
+    return ([float(i), i + 0.5] + [i + (a + 0.5) / NC for a in range(NC)] +
+            [i + (b + 0.5) / NF for b in range(NF)] + [float(i + 1)])
+
+
+def device_inputs(o):
+    """Inputs of the device builder (rn_build_geometry) for the same ``o`` as
+    build_cut_geometry: the float32 radius table, RinAt at every sampled
+    abscissa (-1e9 beyond the exit, where it is not read), solids in cells."""
+    w = _Walls(o)
+    Nx = o["Nx"]
+    rin = np.full((Nx, CUT_SAMPLES), -1e9, dtype=np.float64)
+    for i in range(Nx):
+        for s, xc in enumerate(sample_abscissae(i)):
+            if xc <= w.xeC:
+                rin[i, s] = w.RinAt(xc)
+    solids = np.array([[s["x0"], s["x1"], s["r0"], s["r1"]] for s in w.solids], dtype=np.float64).reshape(-1, 4)
+    return {"Rtab": w.Rtab, "rin": rin, "solids": solids, "xeC": w.xeC, "twC": w.twC, "xBaseC": w.xBaseC,
+            "bodyC": w.bodyC, "base": w.base, "cut": o.get("mode") != "stair"}
+
+
 def build_cut_geometry(o):
     """Cut-cell geometry (cutcell.js:14-186).
 
@@ -199,7 +225,8 @@ def build_cut_geometry(o):
 
     # classification (cutcell.js:107-120)
     kap = (V.astype(np.float64) / rc_mid[:, None]).astype(f32)
-    solid = (kap < 0.02).astype(np.uint8)
+    kap64 = kap.astype(np.float64)               # Float32Array values compared as doubles
+    solid = (kap64 < 0.02).astype(np.uint8)
 
     def zero_solid_faces():
         js, is_ = np.nonzero(solid)
@@ -238,7 +265,7 @@ def build_cut_geometry(o):
     zero_solid_faces()
 
     # first-order flag for faces next to cut cells: store the area negated (cutcell.js:145-153)
-    partial = (solid == 0) & ((kap < 0.98) | (host >= 0))
+    partial = (solid == 0) & ((kap64 < 0.98) | (host >= 0))
     pp = np.zeros((Nr + 2, Nx + 2), dtype=bool)
     pp[1:-1, 1:-1] = partial
     geoA = np.zeros((Nr + 1, W1, 4), dtype=f32)
@@ -254,8 +281,8 @@ def build_cut_geometry(o):
     A64r = Ar.astype(np.float64)
     Wx = (A64x[:Nr, :Nx] - A64x[:Nr, 1:Nx + 1]).astype(f32)
     Wr = (Am.astype(np.float64) - (A64r[1:Nr + 1, :Nx] - A64r[:Nr, :Nx])).astype(f32)
-    Wx[np.abs(Wx) < 1e-6] = 0
-    Wr[np.abs(Wr) < 1e-6] = 0
+    Wx[np.abs(Wx.astype(np.float64)) < 1e-6] = 0
+    Wr[np.abs(Wr.astype(np.float64)) < 1e-6] = 0
     Wx[solid != 0] = 0
     Wr[solid != 0] = 0
 
@@ -307,7 +334,7 @@ def build_cut_geometry(o):
     geoM[fluid_idx, 1] = (hj - jj)[fluid_idx]
     geoM[fluid_idx, 2] = slaveMask[fluid_idx]
     geoM[fluid_idx, 3] = kapf[fluid_idx]
-    nCut = int(np.count_nonzero(kapf[fluid_idx] < 0.98))
+    nCut = int(np.count_nonzero(kapf[fluid_idx].astype(np.float64) < 0.98))
     nMerged = int(np.count_nonzero(hostf[fluid_idx] >= 0))
     return {"mask": solidf.copy(), "geoA": geoA.reshape(-1), "geoG": geoG.reshape(-1),
             "geoM": geoM.reshape(-1), "Ax": Ax.reshape(-1), "Ar": Ar.reshape(-1), "W1": W1,

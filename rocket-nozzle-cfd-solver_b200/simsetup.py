@@ -305,9 +305,9 @@ def build_sim_setup(cfg):
         x = (i + 0.5) * dx
         RinCol[i] = contour.radiusAt(x) if x <= contour.xe else math.inf
     hw = chamber_solids(cfg, contour, dx) if injOn else []
-    geo = build_cut_geometry({"Nx": Nx, "Nr": Nr, "dx": dx, "contour": contour, "tw": tw,
-                              "base": cfg.get("base"), "xBase": xBase, "bodyR": bodyR,
-                              "mode": cfg.get("wallModel") or "cut", "solids": hw})
+    cut_input = {"Nx": Nx, "Nr": Nr, "dx": dx, "contour": contour, "tw": tw, "base": cfg.get("base"),
+                 "xBase": xBase, "bodyR": bodyR, "mode": cfg.get("wallModel") or "cut", "solids": hw}
+    geo = build_cut_geometry(cut_input)
     mask = geo["mask"]
     # turbulence length scale and boundary-layer band flag in geoM (simsetup.js:51-63)
     CS, KAPPA = 0.17, 0.41
@@ -392,6 +392,7 @@ def build_sim_setup(cfg):
     return SimSetup(
         cfg=cfg, Nx=Nx, Nr=Nr, dx=dx, tw=tw, bodyR=bodyR, xBase=xBase, contour=contour, atm=atm,
         theory=theory, mask=mask, geo=geo, P=P, initialState=initial_state, solids=hw,
+        cutInput=cut_input, rinCol=RinCol,
         injector=build_injector_table(cfg, contour, dx, P) if injOn else None,
         iExit=iExit, jExit=jExit, iChamber=iChamber, iThroat=iThroat, tScale=tScale,
         resolution={"throatCells": contour.Rt / dx, "exitCells": contour.Re / dx,

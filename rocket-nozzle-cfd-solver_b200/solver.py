@@ -35,7 +35,7 @@ EXPORTS = ("rn_create", "rn_destroy", "rn_resize", "rn_set_mask", "rn_set_geomet
            "rn_batch_kernel_launches", "rn_residual_mark", "rn_residual", "rn_server_default_opts",
            "rn_server_create", "rn_server_destroy", "rn_serve_submit", "rn_serve_poll", "rn_serve_wait",
            "rn_serve_stats", "rn_solve_bytes", "rn_set_wall_profile", "rn_wall_separation", "rn_derived",
-           "rn_derived_buffer",
+           "rn_derived_buffer", "rn_build_geometry", "rn_get_geometry",
            "rn_last_error")
 PRECISION = {"fast": 0, "exact": 1}
 TILES = {"16x16": 0, "16x8": 1}
@@ -139,6 +139,17 @@ def derived_spec(setup, field, value_range=(0.0, 1.0), schl_gain=10.0, Tc=None):
             "range": tuple(value_range), "RaN": P["RaN"], "Rs": tuple(P["Rs"]), "chemV": tuple(P["chemK"]),
             "Tscale": (T_REF, Tc if Tc is not None else setup["cfg"]["Tc"], P["Ta"], 0.0),
             "schlGain": schl_gain, "velScale": U_REF, "dx": setup["dx"]}
+
+
+class RnCutSpec(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in ("Nx", "Nr", "cut", "base", "nSolids", "iExit")] + \
+               [(n, ctypes.c_double) for n in ("xeC", "twC", "xBaseC", "bodyC", "dx", "xt", "xe", "Rt")] + \
+               [("Rtab", ctypes.c_void_p), ("rin", ctypes.c_void_p), ("solids", ctypes.c_void_p),
+                ("rinCol", ctypes.c_void_p)]
+
+
+class RnCutStats(ctypes.Structure):
+    _fields_ = [("nCut", ctypes.c_int), ("nMerged", ctypes.c_int)]
 
 
 SOLVE_STATUS = {0: "converged", 1: "time", 2: "max_steps", -1: "rejected", -2: "failed"}
@@ -266,6 +277,8 @@ def lib():
     L.rn_wall_separation.argtypes = [H, ctypes.POINTER(RnSeparationSpec), ctypes.POINTER(RnSeparationOut)]
     L.rn_derived.argtypes = [H, ctypes.POINTER(RnDerivedSpec), ctypes.POINTER(RnParams), ctypes.c_void_p]
     L.rn_derived_buffer.argtypes = [H, ctypes.POINTER(ctypes.c_void_p)]
+    L.rn_build_geometry.argtypes = [H, ctypes.POINTER(RnCutSpec), ctypes.POINTER(RnCutStats)]
+    L.rn_get_geometry.argtypes = [H] + [ctypes.c_void_p] * 5
     L.rn_last_error.restype = ctypes.c_char_p
     for n in EXPORTS[:-1]:
         getattr(L, n).restype = ctypes.c_int
@@ -341,6 +354,36 @@ class GPUSolver:
             jwp = jw.ctypes.data
         _check(lib().rn_set_geometry(self.h, m.ctypes.data, gA.ctypes.data, gG.ctypes.data, gM.ctypes.data, jwp))
         self.maskData = geo["mask"]
+
+    def buildGeometry(self, setup):
+        """Build the cut-cell geometry of ``setup`` on the device
+        (rn_build_geometry: buildCutGeometry, cutcell.js:14-186, and the geoM
+        post-pass, simsetup.js:51-63) in place of setGeometry(setup.geo).
+        Returns {nCut, nMerged}."""
+        from .cutcell import device_inputs
+        d = device_inputs(setup["cutInput"])
+        c = setup["contour"]
+        keep = [np.ascontiguousarray(d["Rtab"], np.float32), np.ascontiguousarray(d["rin"], np.float64),
+                np.ascontiguousarray(d["solids"], np.float64), np.ascontiguousarray(setup["rinCol"], np.float32)]
+        sp = RnCutSpec()
+        sp.Nx, sp.Nr, sp.cut, sp.base = self.Nx, self.Nr, 1 if d["cut"] else 0, 1 if d["base"] else 0
+        sp.nSolids, sp.iExit = len(d["solids"]), setup["iExit"]
+        sp.xeC, sp.twC, sp.xBaseC, sp.bodyC = d["xeC"], d["twC"], d["xBaseC"], d["bodyC"]
+        sp.dx, sp.xt, sp.xe, sp.Rt = setup["dx"], c.xt, c.xe, c.Rt
+        sp.Rtab, sp.rin, sp.solids, sp.rinCol = (a.ctypes.data if a.size else None for a in keep)
+        st = RnCutStats()
+        _check(lib().rn_build_geometry(self.h, ctypes.byref(sp), ctypes.byref(st)))
+        return {"nCut": st.nCut, "nMerged": st.nMerged}
+
+    def readGeometry(self):
+        """The handle's geometry planes: {mask, geoA, geoG, geoM, jWall} (host copies)."""
+        N, NF = self.Nx * self.Nr, (self.Nx + 1) * (self.Nr + 1)
+        out = {"mask": np.empty(N, np.uint8), "geoA": np.empty(NF * 4, np.float32),
+               "geoG": np.empty(N * 4, np.float32), "geoM": np.empty(N * 4, np.float32),
+               "jWall": np.empty(self.Nx * 4, np.float32)}
+        _check(lib().rn_get_geometry(self.h, *(out[k].ctypes.data for k in ("mask", "geoA", "geoG", "geoM",
+                                                                           "jWall"))))
+        return out
 
     def setState(self, A, B):
         """solver.js:816-828: every state slot; clears dt/t and the spray ring."""
