@@ -474,9 +474,9 @@ def serving_requests(rn, count, seed=7, spray_frac=0.2):
     return out
 
 
-def serve_once(rn, reqs, arrivals, max_active, check_every, drop, t_end_s):
+def serve_once(rn, reqs, arrivals, max_active, check_every, drop, t_end_s, max_cells=0):
     """Submits reqs at their arrival times (s) to a SolveServer; returns the results."""
-    srv = rn.SolveServer(max_active=max_active, check_every=check_every)
+    srv = rn.SolveServer(max_active=max_active, check_every=check_every, max_active_cells=max_cells)
     ids = []
     t0 = time.perf_counter()
     for (kind, s), ta in zip(reqs, arrivals):
@@ -511,7 +511,7 @@ def run_serving(args):
     arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
     arrivals -= arrivals[0]
     K, drop, t_end = 60, 1e-4, 2e-3
-    served, st = serve_once(rn, reqs, arrivals, 0, K, drop, t_end)
+    served, st = serve_once(rn, reqs, arrivals, 0, K, drop, t_end, args.serve_max_cells)
     plain, _ = serve_once(rn, reqs, arrivals, 1, K, drop, t_end)
     same = all(a["integrals"] == b["integrals"] and a["steps"] == b["steps"] for a, b in zip(served, plain))
     status = {}
@@ -522,6 +522,7 @@ def run_serving(args):
     return {"metric": "solves/s", "value": sv["solves_per_s"], "unit": "solves/s", "rate_per_s": rate,
             "requests": len(reqs), "spray_requests": sum(1 for k, _ in reqs if k == "spray"),
             "stop": "density residual drop 1e-4 or 2 ms simulated", "check_every": K,
+            "max_active_cells": args.serve_max_cells,
             "p50_ms": sv["p50_ms"], "p99_ms": sv["p99_ms"], "makespan_s": sv["makespan_s"],
             "cell_updates_per_s": cells / sv["makespan_s"], "status": status, "ticks": st["ticks"],
             "one_at_a_time": pl, "speedup_solves_per_s": sv["solves_per_s"] / pl["solves_per_s"],
@@ -546,6 +547,8 @@ def main():
     ap.add_argument("--no-large", action="store_true", help="skip the 4096x1536 HBM-resident sweep point")
     ap.add_argument("--serve-requests", type=int, default=24, help="requests of the serving leg (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=5.0, help="Poisson arrival rate of the serving leg (1/s)")
+    ap.add_argument("--serve-max-cells", type=int, default=2000000,
+                    help="admission cap on the grid cells the server steps at once (0: memory budget only)")
     args = ap.parse_args()
     GRID = tuple(int(v) for v in args.grid.lower().split("x"))
     SOLVER_STEPS = args.solver_steps

@@ -43,6 +43,7 @@ extern "C" {
 #define RN_TEX_PARCEL_A 4   /* parcels (x, r, u, v), 256 x 256 */
 #define RN_TEX_PARCEL_B 5   /* parcels (d, m, type, x_imp), 256 x 256 */
 #define RN_TEX_PARCEL_C 6   /* parcels (dm, dp_x, dp_r, 0) given to the gas last step */
+#define RN_TEX_INJECTOR 7   /* injector table, 256 x 3 (the spray's uTab) */
 
 typedef struct rn_solver* rn_handle;
 
@@ -134,6 +135,16 @@ int rn_poll_async(rn_handle h, int* tag, float* out, size_t cap_floats);
 int rn_cancel_async(rn_handle h);
 /* GPUSpray.setInjector({tab}) (spray.js:236-241): 256 x 3 float4 */
 int rn_spray_set_injector(rn_handle h, const float* tab);
+/* The injector table built on the device from its spray elements (the fill of
+ * buildInjectorTable, simsetup.js:181-237): weights normalised and spread over
+ * the 256 rows by largest remainder (ties in element order), rows written in
+ * element order; the same table rn_spray_set_injector would upload. Element
+ * lengths in cells, speeds in U_REF, angles in radians. */
+#define RN_MAX_INJECTOR_ELEMENTS 64
+typedef struct {
+  double type, weight, x, r, angle, speed, drop, cone, width, xi;
+} rn_injector_element;
+int rn_spray_build_injector(rn_handle h, const rn_injector_element* el, int n);
 /* GPUSpray.reset() (spray.js:242-254) */
 int rn_spray_reset(rn_handle h);
 /* GPUSpray.stats(P) (spray.js:312-320): out = (fuel mass, oxidiser mass,
@@ -314,6 +325,8 @@ typedef struct {
   int check_every;     /* steps per tick (>= 2) */
   int precision;       /* RN_PRECISION_* of every solve */
   int tile;            /* RN_TILE_* of the class batches */
+  long long max_active_cells;   /* most grid cells on the device at once; 0 = no limit. Enough cells to
+                                   fill the GPU keep its throughput; fewer concurrent solves finish sooner */
 } rn_server_opts;
 typedef struct {
   int Nx, Nr;

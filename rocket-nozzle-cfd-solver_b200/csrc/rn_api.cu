@@ -529,6 +529,7 @@ int tex_ptr(rn_solver* h, int tex, const float4** p, int* W, int* H) {
     case RN_TEX_PARCEL_A: *p = h->PA[h->scur]; *W = 256; *H = 256; return RN_OK;
     case RN_TEX_PARCEL_B: *p = h->PB[h->scur]; *W = 256; *H = 256; return RN_OK;
     case RN_TEX_PARCEL_C: *p = h->PC[h->scur]; *W = 256; *H = 256; return RN_OK;
+    case RN_TEX_INJECTOR: *p = h->tab; *W = 256; *H = 3; return RN_OK;
     default: return fail(RN_ERR_ARG, "unknown texture " + std::to_string(tex));
   }
 }

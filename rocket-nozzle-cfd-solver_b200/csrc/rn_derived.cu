@@ -147,3 +147,79 @@ int rn_derived_buffer(rn_handle h, void** dev) {
 }
 
 }  // extern "C"
+
+// --------------------------------------------------------------------------
+// Injector table on the device (buildInjectorTable's fill, simsetup.js:181-237):
+// the spray elements (a handful, from the injector layout) are weighted into
+// the 256-row table by largest remainder, in one thread: the remainders are
+// ranked by a stable descending order, as Array.prototype.sort does, and the
+// rows are written in element order. Arithmetic in doubles, rows stored as
+// float32 like the reference's Float32Array.
+namespace {
+
+__global__ void k_injector_table(const rn_injector_element* el, int n, float4* tab) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  constexpr int NROW = 256;
+  double total = 0.0;
+  for (int e = 0; e < n; e++) total = total + el[e].weight;
+  double q[RN_MAX_INJECTOR_ELEMENTS];
+  int cnt[RN_MAX_INJECTOR_ELEMENTS], order[RN_MAX_INJECTOR_ELEMENTS];
+  int used = 0;
+  for (int e = 0; e < n; e++) {
+    q[e] = el[e].weight / total * NROW;
+    cnt[e] = int(floor(q[e]));
+    used += cnt[e];
+    order[e] = e;
+  }
+  // stable insertion sort by descending remainder
+  for (int a = 1; a < n; a++) {
+    const int v = order[a];
+    const double rv = -(q[v] - cnt[v]);
+    int b = a - 1;
+    while (b >= 0 && -(q[order[b]] - cnt[order[b]]) > rv) {
+      order[b + 1] = order[b];
+      b--;
+    }
+    order[b + 1] = v;
+  }
+  for (int a = 0; a < n && used < NROW; a++) {
+    cnt[order[a]]++;
+    used++;
+  }
+  int t = 0;
+  for (int e = 0; e < n; e++)
+    for (int r = 0; r < cnt[e] && t < NROW; r++, t++) {
+      const rn_injector_element& x = el[e];
+      tab[t] = make_float4(float(x.x), float(x.r), float(x.angle), float(x.speed));
+      tab[NROW + t] = make_float4(float(x.type), float(x.drop), float(x.cone), float(x.width));
+      tab[2 * NROW + t] = make_float4(float(x.xi), 0.0f, 0.0f, 0.0f);
+    }
+  for (; t < NROW; t++) {
+    tab[t] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    tab[NROW + t] = tab[t];
+    tab[2 * NROW + t] = tab[t];
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int rn_spray_build_injector(rn_handle h, const rn_injector_element* el, int n) {
+  if (!h || !h->SA[0] || !el || n < 1 || n > RN_MAX_INJECTOR_ELEMENTS)
+    return rn_record_error(RN_ERR_ARG, "rn_spray_build_injector: bad argument or element count");
+  rn_injector_element* d = nullptr;
+  RN_CK(cudaMalloc(&d, sizeof(rn_injector_element) * n));
+  cudaError_t e = cudaMemcpyAsync(d, el, sizeof(rn_injector_element) * n, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) {
+    k_injector_table<<<1, 32, 0, h->stream>>>(d, n, h->tab);
+    h->launches++;
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return rn_record_cuda(e, "rn_spray_build_injector");
+  return RN_OK;
+}
+
+}  // extern "C"

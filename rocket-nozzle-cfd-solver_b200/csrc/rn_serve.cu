@@ -99,6 +99,7 @@ struct rn_server_t {
   // worker-side state (read under mu by rn_serve_stats)
   std::vector<Active> active;
   size_t used = 0;
+  long long cells = 0;        // grid cells of the active solves
   std::atomic<long long> ticks{0};
   long long admitted = 0, retired = 0;
   std::map<int, rn_batch_t*> batches;
@@ -169,6 +170,7 @@ void retire(rn_server_t* s, Active& a, int status) {
   d.res.done_ms = s->now_ms();
   std::lock_guard<std::mutex> lk(s->mu);
   s->used -= a.req.bytes;
+  s->cells -= (long long)a.req.Nx * a.req.Nr;
   s->retired++;
   s->done[a.req.id] = std::move(d);
 }
@@ -193,6 +195,7 @@ void fail_all(rn_server_t* s, const std::string& msg) {
   s->active.clear();
   std::lock_guard<std::mutex> lk(s->mu);
   s->used = 0;
+  s->cells = 0;
   s->failed = 1;
   s->failMsg = msg;
   for (Request& r : s->queue) {
@@ -295,9 +298,12 @@ void work(rn_server_t* s) {
         }
         if (s->used + head.bytes > s->opts.hbm_budget) break;
         if (s->opts.max_active > 0 && int(s->active.size()) >= s->opts.max_active) break;
+        const long long hc = (long long)head.Nx * head.Nr;
+        if (s->opts.max_active_cells > 0 && !s->active.empty() && s->cells + hc > s->opts.max_active_cells) break;
         r = std::move(head);
         s->queue.pop_front();
         s->used += r.bytes;
+        s->cells += hc;
         s->admitted++;
       }
       Active a;
@@ -313,6 +319,7 @@ void work(rn_server_t* s) {
         d.res.done_ms = s->now_ms();
         std::lock_guard<std::mutex> lk(s->mu);
         s->used -= a.req.bytes;
+        s->cells -= (long long)a.req.Nx * a.req.Nr;
         s->done[a.req.id] = std::move(d);
         s->cvDone.notify_all();
         continue;
@@ -357,7 +364,8 @@ int rn_server_create(const rn_server_opts* opts, rn_server* out) {
   rn_server_default_opts(&o);
   if (opts) o = *opts;
   if (o.check_every < 2 || o.tile < 0 || o.tile >= rn::NTILES ||
-      (o.precision != RN_PRECISION_FAST && o.precision != RN_PRECISION_EXACT) || o.max_active < 0)
+      (o.precision != RN_PRECISION_FAST && o.precision != RN_PRECISION_EXACT) || o.max_active < 0 ||
+      o.max_active_cells < 0)
     return sfail(RN_ERR_ARG, "rn_server_create: bad options");
   int dev = 0;
   RN_CK(cudaGetDevice(&dev));

@@ -20,7 +20,7 @@ LIB_PATH = os.path.join(HERE, "librn.so")
 
 RN_OK, RN_NOT_READY, RN_BUSY = 0, 1, 2
 RN_TEX_A, RN_TEX_B, RN_TEX_STEPINFO, RN_TEX_WALLROW = 0, 1, 2, 3
-RN_TEX_PARCEL_A, RN_TEX_PARCEL_B, RN_TEX_PARCEL_C = 4, 5, 6
+RN_TEX_PARCEL_A, RN_TEX_PARCEL_B, RN_TEX_PARCEL_C, RN_TEX_INJECTOR = 4, 5, 6, 7
 SPRAY_W = SPRAY_H = 256
 SPRAY_N = SPRAY_W * SPRAY_H
 
@@ -35,7 +35,7 @@ EXPORTS = ("rn_create", "rn_destroy", "rn_resize", "rn_set_mask", "rn_set_geomet
            "rn_batch_kernel_launches", "rn_residual_mark", "rn_residual", "rn_server_default_opts",
            "rn_server_create", "rn_server_destroy", "rn_serve_submit", "rn_serve_poll", "rn_serve_wait",
            "rn_serve_stats", "rn_solve_bytes", "rn_set_wall_profile", "rn_wall_separation", "rn_derived",
-           "rn_derived_buffer", "rn_build_geometry", "rn_get_geometry",
+           "rn_derived_buffer", "rn_build_geometry", "rn_get_geometry", "rn_spray_build_injector",
            "rn_last_error")
 PRECISION = {"fast": 0, "exact": 1}
 TILES = {"16x16": 0, "16x8": 1}
@@ -85,7 +85,7 @@ class RnIntegralsOut(ctypes.Structure):
 
 class RnServerOpts(ctypes.Structure):
     _fields_ = [("hbm_budget", ctypes.c_size_t), ("max_active", ctypes.c_int), ("check_every", ctypes.c_int),
-                ("precision", ctypes.c_int), ("tile", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("tile", ctypes.c_int), ("max_active_cells", ctypes.c_longlong)]
 
 
 class RnSolveRequest(ctypes.Structure):
@@ -150,6 +150,11 @@ class RnCutSpec(ctypes.Structure):
 
 class RnCutStats(ctypes.Structure):
     _fields_ = [("nCut", ctypes.c_int), ("nMerged", ctypes.c_int)]
+
+
+class RnInjectorElement(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in ("type", "weight", "x", "r", "angle", "speed", "drop", "cone",
+                                               "width", "xi")]
 
 
 SOLVE_STATUS = {0: "converged", 1: "time", 2: "max_steps", -1: "rejected", -2: "failed"}
@@ -279,6 +284,7 @@ def lib():
     L.rn_derived_buffer.argtypes = [H, ctypes.POINTER(ctypes.c_void_p)]
     L.rn_build_geometry.argtypes = [H, ctypes.POINTER(RnCutSpec), ctypes.POINTER(RnCutStats)]
     L.rn_get_geometry.argtypes = [H] + [ctypes.c_void_p] * 5
+    L.rn_spray_build_injector.argtypes = [H, ctypes.POINTER(RnInjectorElement), i]
     L.rn_last_error.restype = ctypes.c_char_p
     for n in EXPORTS[:-1]:
         getattr(L, n).restype = ctypes.c_int
@@ -633,6 +639,16 @@ class GPUSpray:
         tab = _f32(inj["tab"], 256 * 3 * 4)
         _check(lib().rn_spray_set_injector(self.s.h, tab.ctypes.data))
 
+    def buildInjector(self, inj):
+        """The injector table of ``inj`` (build_injector_table's result) built on
+        the device from its element list (rn_spray_build_injector)."""
+        el = inj["elements"]
+        arr = (RnInjectorElement * len(el))()
+        for q, e in enumerate(el):
+            for n in ("type", "weight", "x", "r", "angle", "speed", "drop", "cone", "width", "xi"):
+                setattr(arr[q], n, float(e[n]))
+        _check(lib().rn_spray_build_injector(self.s.h, arr, len(el)))
+
     def reset(self):
         """spray.js:242-254"""
         if not self.ready:
@@ -736,7 +752,8 @@ class SolveServer:
     FP64 read-outs, latencies and (optionally) final states. No reference
     counterpart: the reference runs one interactive solve per page."""
 
-    def __init__(self, budget_bytes=0, max_active=0, check_every=60, precision="fast", tile="16x16"):
+    def __init__(self, budget_bytes=0, max_active=0, check_every=60, precision="fast", tile="16x16",
+                 max_active_cells=0):
         o = RnServerOpts()
         _check(lib().rn_server_default_opts(ctypes.byref(o)))
         o.hbm_budget = int(budget_bytes)
@@ -744,6 +761,7 @@ class SolveServer:
         o.check_every = int(check_every)
         o.precision = PRECISION[precision]
         o.tile = TILES[tile]
+        o.max_active_cells = int(max_active_cells)
         self.s = ctypes.c_void_p()
         _check(lib().rn_server_create(ctypes.byref(o), ctypes.byref(self.s)))
         self.shapes = {}

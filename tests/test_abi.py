@@ -48,7 +48,7 @@ int main(void) {
   F(rn_integral_spec, dx) F(rn_integral_spec, Rs) F(rn_integral_spec, inj) F(rn_integrals_out, t)
   printf("rn_server_opts %zu\nrn_solve_request %zu\nrn_solve_result %zu\nrn_serve_status %zu\n",
          sizeof(rn_server_opts), sizeof(rn_solve_request), sizeof(rn_solve_result), sizeof(rn_serve_status));
-  F(rn_server_opts, max_active) F(rn_server_opts, tile) F(rn_solve_request, mask) F(rn_solve_request, injTab)
+  F(rn_server_opts, max_active) F(rn_server_opts, tile) F(rn_server_opts, max_active_cells) F(rn_solve_request, mask) F(rn_solve_request, injTab)
   F(rn_solve_request, P) F(rn_solve_request, spec) F(rn_solve_request, drop) F(rn_solve_request, max_steps)
   F(rn_solve_result, steps) F(rn_solve_result, done_ms) F(rn_solve_result, integrals) F(rn_serve_status, failed)
   printf("rn_separation_spec %zu\nrn_separation_out %zu\n", sizeof(rn_separation_spec), sizeof(rn_separation_out));

@@ -141,3 +141,20 @@ def test_derived_turbulence_fields_need_a_step(rn):
     with pytest.raises(rn.RnError):
         g.derived(solver.derived_spec(s, "turb", RANGES["turb"]))              # P required
     g.close()
+
+
+@pytest.mark.parametrize("key", ["injShower", "injCoax", "injImpinge", "injPintle", "injHardware"])
+def test_injector_table_built_on_device(rn, key):
+    """The device fill of the injector table equals the host table of
+    build_injector_table (bit for bit), also with a film-cooling element."""
+    from rocket_nozzle_cfd_solver_b200 import configs, solver
+    for film in (0, 12):
+        cfg = dict(configs.preset(key, 192), film=film)
+        s = rn.build_sim_setup(cfg)
+        g = rn.GPUSolver(s.Nx, s.Nr)
+        rn.GPUSpray(g).resize()
+        g.spray.buildInjector(s.injector)
+        tab = g._readRect(solver.RN_TEX_INJECTOR, 0, 0, 256, 3)
+        ref = np.asarray(s.injector["tab"], np.float32)
+        assert np.array_equal(tab.view(np.uint32), ref.view(np.uint32)), (key, film)
+        g.close()

@@ -133,3 +133,23 @@ def test_server_time_and_poll(rn):
     assert r is not None
     assert r["status"] == "time" and r["t"] * s.tScale >= 2e-5 and r["steps"] % 25 == 0
     assert np.isfinite(r["integrals"]["F"]) and r["integrals"]["t"] == pytest.approx(r["t"], rel=1e-6)
+
+
+def test_server_cell_cap(rn):
+    """max_active_cells admits solves while their grids fit the cap (always at
+    least one); results are unchanged by the admission order."""
+    ss = [setup_of(rn, "plain", 128, 48), setup_of(rn, "plain", 128, 48), setup_of(rn, "plain", 96, 36)]
+    srv = rn.SolveServer(check_every=20, max_active_cells=128 * 48 + 96 * 36, precision="exact")
+    ids = [srv.submit(s, drop=0, t_end_s=0, max_steps=100) for s in ss]
+    peak = 0
+    t0 = time.time()
+    while srv.stats()["admitted"] < len(ss) and time.time() - t0 < 120:
+        peak = max(peak, srv.stats()["active"])
+        time.sleep(0.0005)
+    res = [srv.wait(i, timeout_s=120, state=True) for i in ids]
+    srv.close()
+    assert peak <= 2
+    assert res[0]["done_ms"] <= res[1]["admit_ms"]          # the second 128x48 waits for the first
+    for s, r in zip(ss, res):
+        out, _ = alone(rn, s, 100)
+        assert np.array_equal(r["A"], out["A"])
