@@ -290,8 +290,8 @@ def run_ours(args, rank, world, local_rank):
     if world == 1 and not args.no_large:
         large = run_large_grid(args)
         torch.cuda.empty_cache()
-    if world == 1 and args.batch_instances > 0:
-        batched = run_batched(args, local_rank)
+    if args.batch_instances > 0:
+        batched = run_batched(args, local_rank, rank, world)
     if world == 1 and args.serve_requests > 0:
         serving = run_serving(args)
 
@@ -318,7 +318,7 @@ def run_ours(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
-def run_batched(args, local_rank):
+def run_batched(args, local_rank, rank=0, world=1):
     """The batched workload: `--batch-instances` seeded nozzles (grids drawn
     from 128x48 .. 1024x384, expansion 4-40, p0 10-100 bar, gamma 1.2/1.4,
     altitude 0-30 km, all viscous) stepped by one SolverBatch (one launch per
@@ -329,7 +329,12 @@ def run_batched(args, local_rank):
     import torch
     rn = ge.load_package()
     from rocket_nozzle_cfd_solver_b200 import configs
+    from rocket_nozzle_cfd_solver_b200 import replicas
     cfgs = configs.batched(args.batch_instances, seed=2024)
+    if world > 1:
+        # instances shard across ranks by grid cells (no data-path collective)
+        cells_of = [c["Nx"] * round(c["aspect"] * c["Nx"]) for c in cfgs]
+        cfgs = [cfgs[k] for k in replicas.partition_by_cost(cells_of, rank, world)]
     t0 = time.perf_counter()
     setups = [rn.build_sim_setup(c) for c in cfgs]
     t_setup = time.perf_counter() - t0
@@ -360,7 +365,10 @@ def run_batched(args, local_rank):
             evs[k][1].record(stream)
     batch.sync()
     launches = batch.kernelLaunches() - l0
-    ms = sum(a.elapsed_time(b) for a, b in evs)
+    dev = f"cuda:{local_rank}"
+    ms = replicas.max_over_ranks(sum(a.elapsed_time(b) for a, b in evs), dev)
+    my_cells = cells
+    cells = int(replicas.sum_over_ranks(cells, dev))
     value = cells * nsteps * args.steps / (ms * 1e-3)
     # FP64 read-outs of every member after the batch run (thrust, mass flow)
     F = [g.integrals(s) for g, s in zip(handles, setups)]
@@ -388,7 +396,8 @@ def run_batched(args, local_rank):
                 b.record(st)
             b.synchronize()
             single_ms += a.elapsed_time(b)
-    single_wall = time.perf_counter() - t0
+    single_wall = replicas.max_over_ranks(time.perf_counter() - t0, dev)
+    single_ms = replicas.max_over_ranks(single_ms, dev)
     single = cells * nsteps * rounds / (single_ms * 1e-3)
     for g in handles:
         g.close()
@@ -397,7 +406,9 @@ def run_batched(args, local_rank):
         sizes[f"{s.Nx}x{s.Nr}"] = sizes.get(f"{s.Nx}x{s.Nr}", 0) + 1
     peak, src = measured_peak()
     bpc = BYTES_PER_CELL["stage1"] + BYTES_PER_CELL["stage2_physics"]
-    return {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "instances": len(setups),
+    instances = int(replicas.sum_over_ranks(len(setups), dev))
+    return {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "instances": instances,
+            "ranks": world, "cells_this_rank": my_cells,
             "achieved_gbs": value * bpc / 1e9, "bytes_per_cell_step": bpc, "frac": value * bpc / 1e9 / peak,
             "peak_source": src,
             "cells": cells, "grids": sizes, "solver_steps_per_bench_step": nsteps, "steps": args.steps,

@@ -22,6 +22,7 @@
 // turbulence length and boundary-layer band; jWall.
 #include <cuda_runtime.h>
 #include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
 #include <math.h>
 #include <string>
 #include <vector>
@@ -374,7 +375,7 @@ int rn_build_geometry(rn_handle h, const rn_cut_spec* sp, rn_cut_stats* stats) {
   const size_t oF = take(sizeof(float) * 3 * size_t(N)), oFace = take(sizeof(float) * 2 * size_t(NF));
   const size_t oSl = take(sizeof(int) * (size_t(N) + 1)), oCnt = take(sizeof(unsigned) * 4);
   size_t cubBytes = 0;
-  cub::DeviceSelect::Flagged(nullptr, cubBytes, cub::CountingInputIterator<int>(0), (const uint8_t*)nullptr,
+  cub::DeviceSelect::Flagged(nullptr, cubBytes, thrust::counting_iterator<int>(0), (const uint8_t*)nullptr,
                              (int*)nullptr, (int*)nullptr, N, s);
   const size_t oCub = take(cubBytes + 16);
   char* base = nullptr;
@@ -422,7 +423,7 @@ int rn_build_geometry(rn_handle h, const rn_cut_spec* sp, rn_cut_stats* stats) {
     k_sliver_flags<<<(N + 255) / 256, 256, 0, s>>>(c, flags);
     ck(cudaGetLastError());
     size_t cb = cubBytes;
-    ck(cub::DeviceSelect::Flagged(base + oCub, cb, cub::CountingInputIterator<int>(0), flags, sliv, nSliv, N, s));
+    ck(cub::DeviceSelect::Flagged(base + oCub, cb, thrust::counting_iterator<int>(0), flags, sliv, nSliv, N, s));
     k_merge<<<1, 32, 0, s>>>(c, sliv, nSliv);
     k_solid_faces<<<gL, b2, 0, s>>>(c);
     k_geoA<<<gL, b2, 0, s>>>(c, o);

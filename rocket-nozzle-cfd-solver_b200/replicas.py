@@ -17,6 +17,22 @@ def partition(n_items, rank, world):
     return range(start, start + base + (1 if rank < extra else 0))
 
 
+def partition_by_cost(costs, rank, world):
+    """Indices of the items ``rank`` takes when items of the given costs (e.g.
+    grid cells) are spread over ``world`` ranks by longest-processing-time:
+    largest first, each to the least-loaded rank (ties to the lower rank).
+    Deterministic, so every rank computes the same assignment on its own."""
+    if world < 1 or not (0 <= rank < world):
+        raise ValueError("bad rank/world")
+    load = [0] * world
+    owner = [0] * len(costs)
+    for k in sorted(range(len(costs)), key=lambda q: (-costs[q], q)):
+        r = min(range(world), key=lambda w: (load[w], w))
+        owner[k] = r
+        load[r] += costs[k]
+    return [k for k in range(len(costs)) if owner[k] == rank]
+
+
 def max_over_ranks(value, device="cpu"):
     """Max of a float over all ranks of the default process group (identity when not distributed)."""
     import torch

@@ -61,3 +61,20 @@ def test_partition_covers_uneven_batches(rn):
             assert max(map(len, parts)) - min(map(len, parts)) <= 1
     with pytest.raises(ValueError):
         replicas.partition(4, 2, 2)
+
+
+def test_partition_by_cost_balances_uneven_instances(rn):
+    """Longest-processing-time split of the batched workload's grids: every
+    instance lands on exactly one rank and the largest load is within one
+    largest item of the mean."""
+    from rocket_nozzle_cfd_solver_b200 import configs, replicas
+    cfgs = configs.batched(64, seed=2024)
+    cost = [c["Nx"] * round(c["aspect"] * c["Nx"]) for c in cfgs]
+    for world in (1, 2, 3, 4, 8):
+        parts = [replicas.partition_by_cost(cost, r, world) for r in range(world)]
+        flat = sorted(k for p in parts for k in p)
+        assert flat == list(range(64))
+        loads = [sum(cost[k] for k in p) for p in parts]
+        assert max(loads) - sum(cost) / world <= max(cost)
+    with pytest.raises(ValueError):
+        replicas.partition_by_cost(cost, 2, 2)
