@@ -174,14 +174,16 @@ int rn_kernel_launches(rn_handle h, long long* out);
 int rn_set_precision(rn_handle h, int mode);
 int rn_get_precision(rn_handle h, int* mode);
 
-/* Tile shape of the stage/physics kernels (one thread per cell):
- * RN_TILE_16x16 (default) or RN_TILE_16x8. rn_autotune times `steps` steps
+/* Tile shape of the stage/physics kernels (a thread per cell):
+ * RN_TILE_16x15 (default), RN_TILE_16x16, RN_TILE_16x8 or RN_TILE_32x15. rn_autotune times `steps` steps
  * with each shape on a copy of the handle's current state (the state, step
  * info and spray ring are restored afterwards), keeps the fastest and returns
  * it in *chosen. No reference counterpart (the reference draws full-screen
  * fragment passes). */
 #define RN_TILE_16x16 0
 #define RN_TILE_16x8 1
+#define RN_TILE_16x15 2   /* 16 x 15 cells on 256 threads */
+#define RN_TILE_32x15 3   /* 32 x 15 cells on 512 threads */
 int rn_set_tile(rn_handle h, int shape);
 int rn_get_tile(rn_handle h, int* shape);
 int rn_autotune(rn_handle h, const rn_params* P, int steps, int* chosen);

@@ -51,7 +51,7 @@ struct rn_batch_t {
   cudaStream_t stream = nullptr;
   cudaEvent_t done = nullptr;           // end of the last rn_batch_step
   cudaEvent_t staged = nullptr;         // the last descriptor upload has read the pinned buffer
-  int tile = 0;
+  int tile = RN_TILE_16x15;
   Flags flags;
   std::vector<rn_solver*> members;
   std::vector<rn_params> params;

@@ -46,7 +46,7 @@ struct rn_solver {
   long long profN[RN_NKERNELS] = {0};
   // tile shape of the stage/physics kernels and, per tile, the out-of-tile
   // members of its cut-cell groups (built from host copies of the topology)
-  int tile = 0;
+  int tile = RN_TILE_16x15;
   int* xoff = nullptr;
   int* xcell = nullptr;
   int maxX = 1;

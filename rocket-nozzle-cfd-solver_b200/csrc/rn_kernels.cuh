@@ -7,13 +7,20 @@
 
 namespace rn {
 
-// Tile shapes of the stage/physics blocks (one thread per cell). Measured on
-// the viscous plume (B200, fast precision): 16x16 beats 32x8 by 4.5 % at
-// 512x192 and 17 % at 1024x384 (fewer halo primitives and faces per cell);
-// 16x8 gives twice the blocks for small grids. The autotuner picks per handle.
-constexpr int NTILES = 2;
-constexpr int TILE_TX[NTILES] = {16, 16};
-constexpr int TILE_TY[NTILES] = {16, 8};
+// Tile shapes of the stage/physics blocks: TX x TY cells on TILE_NT threads,
+// a thread per cell (threads beyond TX*TY idle in the cell phases). 16x15 on
+// 256 threads (the default) has 511 faces, so its face phase is exactly two
+// passes of the block, where 16x16's 544 faces need a third pass for one warp
+// while the other seven wait at the barrier. Measured on B200 (fast
+// precision, G cell-updates/s, 16x16 / 16x8 / 16x15 / 32x15): viscous
+// 512x192 2.43 / 2.31 / 2.47 / 2.26, viscous 1024x384 3.67 / 3.26 / 4.00 /
+// 3.99, plain 4096x1536 5.51 / 5.49 / 5.73 / 5.51, 64 batched instances
+// 3.59 / 3.07 / 4.05 / 3.98. (16x16 itself beat 32x8 by 4.5-17 %.) The
+// autotuner picks per handle or batch.
+constexpr int NTILES = 4;
+constexpr int TILE_TX[NTILES] = {16, 16, 16, 32};
+constexpr int TILE_TY[NTILES] = {16, 8, 15, 15};
+constexpr int TILE_NT[NTILES] = {256, 128, 256, 512};
 // Most out-of-tile group members one tile may list (set_geometry rejects more).
 constexpr int MAXX = 64;
 

@@ -353,7 +353,7 @@ int rn_server_default_opts(rn_server_opts* o) {
   o->max_active = 0;
   o->check_every = 60;
   o->precision = RN_PRECISION_FAST;
-  o->tile = RN_TILE_16x16;
+  o->tile = RN_TILE_16x15;
   return RN_OK;
 }
 

@@ -49,16 +49,20 @@ namespace RN_VARIANT {
 #define RN_MIN_WARPS 32
 #endif
 
-template <int TX_, int TY_>
+template <int TX_, int TY_, int NT_>
 struct TileT {
-  static constexpr int TX = TX_, TY = TY_, NT = TX * TY;
+  static constexpr int TX = TX_, TY = TY_, NT = NT_, NC = TX * TY;   // NT threads, NC cells (NC <= NT)
   static constexpr int MINB = RN_MIN_WARPS / (NT / 32) > 0 ? RN_MIN_WARPS / (NT / 32) : 1;
   static constexpr int PX = TX + 4, PY = TY + 4, NPT = PX * PY;   // primitives with a 2-cell halo
   static constexpr int NXF = TY * (TX + 1), NRF = (TY + 1) * TX;  // x- and r-faces of a tile
   static constexpr int TW = TX + 2, NTT = (TX + 2) * (TY + 2);    // vcell ring (tile + 1)
 };
-using Tile0 = TileT<TILE_TX[0], TILE_TY[0]>;
-using Tile1 = TileT<TILE_TX[1], TILE_TY[1]>;
+using Tile0 = TileT<TILE_TX[0], TILE_TY[0], TILE_NT[0]>;
+using Tile1 = TileT<TILE_TX[1], TILE_TY[1], TILE_NT[1]>;
+using Tile2 = TileT<TILE_TX[2], TILE_TY[2], TILE_NT[2]>;
+using Tile3 = TileT<TILE_TX[3], TILE_TY[3], TILE_NT[3]>;
+static_assert(Tile0::NC <= Tile0::NT && Tile1::NC <= Tile1::NT && Tile2::NC <= Tile2::NT && Tile3::NC <= Tile3::NT,
+              "a thread per cell");
 
 // --------------------------------------------------------------------------
 // block-wide max of non-negative floats -> one atomicMax on the bit pattern
@@ -350,7 +354,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const rn_params& 
 
   const int i = x0 + tid % TX, j = y0 + tid / TX;
   float wcell = 0.0f;
-  if (i < Nx && j < Nr) {
+  if (tid < T::NC && i < Nx && j < Nr) {
     float4 oA, oB;
     const bool fluid = update_cell<T, STAGE>(a, P, i, j, dt, t, x0, y0, xc, xn, sF, sY, sO, oA, oB);
     const int k = j * Nx + i;
@@ -621,7 +625,7 @@ __device__ __forceinline__ void stage2_physics_body(const StageArgs& a, const Ph
     inviscid_faces<T>(g, P, x0, y0, xc, NF, sW, sWb, sF, sY, sO);
     __syncthreads();
     const int i = x0 + tid % TX, j = y0 + tid / TX;
-    if (i < Nx && j < Nr) {
+    if (tid < T::NC && i < Nx && j < Nr) {
       float4 oA, oB;
       update_cell<T, 2>(a, P, i, j, dt, t, x0, y0, xc, xn, sF, sY, sO, oA, oB);
       sA2[tid] = oA;
@@ -647,7 +651,7 @@ __device__ __forceinline__ void stage2_physics_body(const StageArgs& a, const Ph
 
   const int i = x0 + tid % TX, j = y0 + tid / TX;
   float wcell = 0.0f;
-  if (i < Nx && j < Nr) {
+  if (tid < T::NC && i < Nx && j < Nr) {
     const int k = j * Nx + i;
     float4 oA, oB, A = make_float4(0.f, 0.f, 0.f, 0.f), B = A;
     float Bw = 0.0f;
@@ -906,32 +910,50 @@ static int init_tile() {
 }
 // Raises the dynamic shared-memory limits of the stage and physics kernels to
 // what a member list of MAXX cells needs (process-wide function attributes).
-int stage_kernels_init() { return (init_tile<Tile0>() == 0 && init_tile<Tile1>() == 0) ? 0 : -1; }
+int stage_kernels_init() {
+  return (init_tile<Tile0>() == 0 && init_tile<Tile1>() == 0 && init_tile<Tile2>() == 0 && init_tile<Tile3>() == 0)
+             ? 0
+             : -1;
+}
 
 void launch_stage1(const StageArgs& a, const rn_params& P, int tile, cudaStream_t s) {
-  if (tile == 1) k_stage<Tile1, 1><<<tiles_of<Tile1>(a.g), Tile1::NT, stage_smem_t<Tile1>(a.maxX), s>>>(a, P);
+  if (tile == 3) k_stage<Tile3, 1><<<tiles_of<Tile3>(a.g), Tile3::NT, stage_smem_t<Tile3>(a.maxX), s>>>(a, P);
+  else if (tile == 2) k_stage<Tile2, 1><<<tiles_of<Tile2>(a.g), Tile2::NT, stage_smem_t<Tile2>(a.maxX), s>>>(a, P);
+  else if (tile == 1) k_stage<Tile1, 1><<<tiles_of<Tile1>(a.g), Tile1::NT, stage_smem_t<Tile1>(a.maxX), s>>>(a, P);
   else k_stage<Tile0, 1><<<tiles_of<Tile0>(a.g), Tile0::NT, stage_smem_t<Tile0>(a.maxX), s>>>(a, P);
 }
 void launch_stage2(const StageArgs& a, const rn_params& P, int tile, cudaStream_t s) {
-  if (tile == 1) k_stage<Tile1, 2><<<tiles_of<Tile1>(a.g), Tile1::NT, stage_smem_t<Tile1>(a.maxX), s>>>(a, P);
+  if (tile == 3) k_stage<Tile3, 2><<<tiles_of<Tile3>(a.g), Tile3::NT, stage_smem_t<Tile3>(a.maxX), s>>>(a, P);
+  else if (tile == 2) k_stage<Tile2, 2><<<tiles_of<Tile2>(a.g), Tile2::NT, stage_smem_t<Tile2>(a.maxX), s>>>(a, P);
+  else if (tile == 1) k_stage<Tile1, 2><<<tiles_of<Tile1>(a.g), Tile1::NT, stage_smem_t<Tile1>(a.maxX), s>>>(a, P);
   else k_stage<Tile0, 2><<<tiles_of<Tile0>(a.g), Tile0::NT, stage_smem_t<Tile0>(a.maxX), s>>>(a, P);
 }
 void launch_stage2phys(const StageArgs& a, const PhysArgs& p, const rn_params& P, int tile, cudaStream_t s) {
-  if (tile == 1)
+  if (tile == 3)
+    k_stage2phys<Tile3><<<tiles_of<Tile3>(a.g), Tile3::NT, fused_smem_t<Tile3>(a.maxX), s>>>(a, p, P);
+  else if (tile == 2)
+    k_stage2phys<Tile2><<<tiles_of<Tile2>(a.g), Tile2::NT, fused_smem_t<Tile2>(a.maxX), s>>>(a, p, P);
+  else if (tile == 1)
     k_stage2phys<Tile1><<<tiles_of<Tile1>(a.g), Tile1::NT, fused_smem_t<Tile1>(a.maxX), s>>>(a, p, P);
   else
     k_stage2phys<Tile0><<<tiles_of<Tile0>(a.g), Tile0::NT, fused_smem_t<Tile0>(a.maxX), s>>>(a, p, P);
 }
 void launch_batch_stage1(const BatchInst* d, const int* bi, int nb, BatchPhase ph, int tile, cudaStream_t s) {
-  if (tile == 1) k_stage_batch<Tile1, 1><<<nb, Tile1::NT, stage_smem_t<Tile1>(ph.maxX), s>>>(d, bi, ph);
+  if (tile == 3) k_stage_batch<Tile3, 1><<<nb, Tile3::NT, stage_smem_t<Tile3>(ph.maxX), s>>>(d, bi, ph);
+  else if (tile == 2) k_stage_batch<Tile2, 1><<<nb, Tile2::NT, stage_smem_t<Tile2>(ph.maxX), s>>>(d, bi, ph);
+  else if (tile == 1) k_stage_batch<Tile1, 1><<<nb, Tile1::NT, stage_smem_t<Tile1>(ph.maxX), s>>>(d, bi, ph);
   else k_stage_batch<Tile0, 1><<<nb, Tile0::NT, stage_smem_t<Tile0>(ph.maxX), s>>>(d, bi, ph);
 }
 void launch_batch_stage2(const BatchInst* d, const int* bi, int nb, BatchPhase ph, int tile, cudaStream_t s) {
-  if (tile == 1) k_stage_batch<Tile1, 2><<<nb, Tile1::NT, stage_smem_t<Tile1>(ph.maxX), s>>>(d, bi, ph);
+  if (tile == 3) k_stage_batch<Tile3, 2><<<nb, Tile3::NT, stage_smem_t<Tile3>(ph.maxX), s>>>(d, bi, ph);
+  else if (tile == 2) k_stage_batch<Tile2, 2><<<nb, Tile2::NT, stage_smem_t<Tile2>(ph.maxX), s>>>(d, bi, ph);
+  else if (tile == 1) k_stage_batch<Tile1, 2><<<nb, Tile1::NT, stage_smem_t<Tile1>(ph.maxX), s>>>(d, bi, ph);
   else k_stage_batch<Tile0, 2><<<nb, Tile0::NT, stage_smem_t<Tile0>(ph.maxX), s>>>(d, bi, ph);
 }
 void launch_batch_stage2phys(const BatchInst* d, const int* bi, int nb, BatchPhase ph, int tile, cudaStream_t s) {
-  if (tile == 1) k_stage2phys_batch<Tile1><<<nb, Tile1::NT, fused_smem_t<Tile1>(ph.maxX), s>>>(d, bi, ph);
+  if (tile == 3) k_stage2phys_batch<Tile3><<<nb, Tile3::NT, fused_smem_t<Tile3>(ph.maxX), s>>>(d, bi, ph);
+  else if (tile == 2) k_stage2phys_batch<Tile2><<<nb, Tile2::NT, fused_smem_t<Tile2>(ph.maxX), s>>>(d, bi, ph);
+  else if (tile == 1) k_stage2phys_batch<Tile1><<<nb, Tile1::NT, fused_smem_t<Tile1>(ph.maxX), s>>>(d, bi, ph);
   else k_stage2phys_batch<Tile0><<<nb, Tile0::NT, fused_smem_t<Tile0>(ph.maxX), s>>>(d, bi, ph);
 }
 void launch_reduce(const Grid& g, const float4* A, const float4* B, unsigned* w, cudaStream_t s) {

@@ -38,7 +38,7 @@ EXPORTS = ("rn_create", "rn_destroy", "rn_resize", "rn_set_mask", "rn_set_geomet
            "rn_derived_buffer", "rn_build_geometry", "rn_get_geometry", "rn_spray_build_injector",
            "rn_last_error")
 PRECISION = {"fast": 0, "exact": 1}
-TILES = {"16x16": 0, "16x8": 1}
+TILES = {"16x16": 0, "16x8": 1, "16x15": 2, "32x15": 3}
 KERNEL_KINDS = ("reduce", "stage1", "stage2", "physics", "parcels", "apply", "other", "stage2_physics")
 
 
@@ -577,7 +577,7 @@ class GPUSolver:
         return {b: a for a, b in PRECISION.items()}[v.value]
 
     def setTile(self, shape):
-        """Tile shape of the stage/physics kernels: '16x16' (default) or '16x8'."""
+        """Tile shape of the stage/physics kernels: '16x15' (default), '16x16', '16x8' or '32x15'."""
         _check(lib().rn_set_tile(self.h, TILES[shape]))
 
     @property
@@ -752,7 +752,7 @@ class SolveServer:
     FP64 read-outs, latencies and (optionally) final states. No reference
     counterpart: the reference runs one interactive solve per page."""
 
-    def __init__(self, budget_bytes=0, max_active=0, check_every=60, precision="fast", tile="16x16",
+    def __init__(self, budget_bytes=0, max_active=0, check_every=60, precision="fast", tile="16x15",
                  max_active_cells=0):
         o = RnServerOpts()
         _check(lib().rn_server_default_opts(ctypes.byref(o)))

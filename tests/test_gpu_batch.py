@@ -41,25 +41,26 @@ def setups(rn, kind, sizes):
 def test_tile_shapes_bit_identical(rn, oracle, kind):
     s = setups(rn, kind, [(160, 60)])[0]
     outs = []
-    for tile in ("16x16", "16x8"):
+    for tile in ("16x16", "16x8", "16x15", "32x15"):
         g = make(rn, s, tile=tile)
         assert g.tile == tile
         g.step(40, s.P)
         outs.append((g.readAll(), g.readStepInfo()))
         g.close()
-    assert identical(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+    for o in outs[1:]:
+        assert identical(outs[0][0], o[0]) and np.array_equal(outs[0][1], o[1])
     assert identical(outs[0][0], run_oracle(oracle, s, 40).readAll())
 
 
 def test_fast_tile_shapes_agree(rn):
     s = setups(rn, "viscous", [(256, 96)])[0]
     outs = []
-    for tile in ("16x16", "16x8"):
+    for tile in ("16x16", "16x8", "16x15", "32x15"):
         g = make(rn, s, precision="fast", tile=tile)
         g.step(60, s.P)
         outs.append(g.readAll())
         g.close()
-    assert identical(outs[0], outs[1])
+    assert all(identical(outs[0], o) for o in outs[1:])
 
 
 def test_autotune_restores_state(rn):
@@ -71,7 +72,7 @@ def test_autotune_restores_state(rn):
     before, si = g.readAll(), g.readStepInfo()
     launches = g.kernelLaunches()
     chosen = g.autotune(s.P, steps=4)
-    assert chosen in ("16x16", "16x8") and g.tile == chosen
+    assert chosen in ("16x16", "16x8", "16x15", "32x15") and g.tile == chosen
     assert identical(g.readAll(), before) and np.array_equal(g.readStepInfo(), si)
     assert g.kernelLaunches() == launches
     g.step(9, s.P)
@@ -166,8 +167,8 @@ def test_batch_launches_and_tile(rn, oracle):
     gs = [make(rn, s) for s in ss]
     for g, s in zip(gs, ss):
         batch.add(g, s.P)
-    batch.setTile("16x8")
-    assert all(g.tile == "16x8" for g in gs)
+    batch.setTile("16x15")
+    assert all(g.tile == "16x15" for g in gs)
     n0 = batch.kernelLaunches()
     batch.step(20)
     batch.sync()
@@ -192,7 +193,7 @@ def test_batch_autotune_restores_members(rn):
     snaps = [(g.readAll(), g.readStepInfo()) for g in members]
     n0 = batch.kernelLaunches()
     chosen = batch.autotune(steps=6)
-    assert chosen in ("16x16", "16x8") and batch.tile == chosen
+    assert chosen in ("16x16", "16x8", "16x15", "32x15") and batch.tile == chosen
     assert batch.kernelLaunches() == n0
     for g, (st, si) in zip(members, snaps):
         assert identical(g.readAll(), st) and np.array_equal(g.readStepInfo(), si)
