@@ -271,22 +271,32 @@ def run_ours(args, rank, world, local_rank):
     h2d = ctypes.sizeof(params)
     if world > 1:
         torch.distributed.barrier()
+    # The app's frame loop: queue the next step(n, P) before waiting for the
+    # previous read-back, then turn that read-back into the read-outs while
+    # the GPU runs (requestAsync / pollAsync keep one read in flight).
     t0 = time.perf_counter()
     perf = None
+    g.step(SOLVER_STEPS, setup.P)              # parameter block converted and passed every call
+    g.requestAsync(reqs, 0)
     for k in range(args.steps):
-        g.step(SOLVER_STEPS, setup.P)          # parameter block converted and passed every call
-        g.requestAsync(reqs, k)
+        if k + 1 < args.steps:
+            g.step(SOLVER_STEPS, setup.P)
         res = None
         while res is None:
             res = g.pollAsync()
         d = res["data"]
         perf = rn.exit_performance(setup, {"A": d["colA"], "B": d["colB"]})
+        if k + 1 < args.steps:
+            g.requestAsync(reqs, k + 1)
+    g.sync()
     e2e_s = replicas.max_over_ranks(time.perf_counter() - t0, dev)
     e2e = world * cells * SOLVER_STEPS * args.steps / e2e_s
     g.close()
     del flush
     torch.cuda.empty_cache()
-    batched = serving = large = None
+    batched = serving = large = spray = None
+    if world == 1 and not args.no_large:
+        spray = run_spray(args, local_rank)
     if world == 1 and not args.no_large:
         large = run_large_grid(args)
         torch.cuda.empty_cache()
@@ -298,6 +308,7 @@ def run_ours(args, rank, world, local_rank):
     if rank != 0:
         return
     cpu = None
+    fp64 = run_fp64_check(args) if world == 1 and not args.no_cpu else None
     if world == 1 and not args.no_cpu:
         cv, threads, nst, el = cpu_sample(setup)
         cpu = {"value": cv, "unit": "cell-updates/s", "cores": threads, "kind": "port",
@@ -313,7 +324,7 @@ def run_ours(args, rank, world, local_rank):
             "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "exit_thrust_N": perf["F"] if perf else None},
             "steady_state_value": steady,
-            "gpu_launches": launches, "clocks": clk.summary(), "large_grid": large,
+            "gpu_launches": launches, "clocks": clk.summary(), "fp64_error": fp64, "spray": spray, "large_grid": large,
             "batched": batched, "serving": serving}
     print(json.dumps(line), flush=True)
 
@@ -469,19 +480,109 @@ def run_large_grid(args):
             "frac": rate * bpc / 1e9 / peak, "kernels": kern}
 
 
+def run_spray(args, local_rank):
+    """Injector + spray chamber (coaxial methalox at 70 bar, 512 x 192, the
+    65,536-parcel ring spawning 4 parcels per step from the injector table):
+    device time per step with the parcel update, the deterministic deposit
+    sort, the two stages + split step and the source apply; parcel-steps/s
+    counts every ring slot each step (the reference's spray pass draws all
+    65,536 fragments)."""
+    import torch
+    rn = ge.load_package()
+    from rocket_nozzle_cfd_solver_b200.configs import injector_spray
+    s = rn.build_sim_setup(injector_spray(512, 192)[0])
+    g = rn.GPUSolver(s.Nx, s.Nr)
+    g.setGeometry(s.geo)
+    init = s.initialState()
+    g.setState(init["A"], init["B"])
+    rn.GPUSpray(g).resize()
+    g.spray.setInjector(s.injector)
+    p = rn.params_from_P(s.P)
+    n = 50
+    for _ in range(max(args.warmup, 1)):
+        g.step(n, p)
+    g.sync()
+    st = torch.cuda.ExternalStream(g.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(st):
+        e0.record(st)
+    g.step(n * args.steps, p)
+    with torch.cuda.stream(st):
+        e1.record(st)
+    g.sync()
+    ms = e0.elapsed_time(e1)
+    steps = n * args.steps
+    g.profile(True)
+    g.step(n, p)
+    prof = g.profileRead()
+    g.profile(False)
+    total = sum(v[0] for v in prof.values())
+    live = g.spray.stats()["parcels"]
+    g.close()
+    return {"workload": "injector + spray chamber 512x192 (injCoax, methalox 70 bar), 65,536-parcel ring",
+            "cell_updates_per_s": s.Nx * s.Nr * steps / (ms * 1e-3),
+            "parcel_steps_per_s": 65536 * steps / (ms * 1e-3), "steps_per_s": steps / (ms * 1e-3),
+            "live_parcels_at_end": live, "ms_per_step": ms / steps,
+            "share": {k: round(v[0] / total, 4) for k, v in prof.items() if v[1]}}
+
+
+def exit_column(state, s):
+    """The exit-plane column (iExit) of a full state, as exit_performance reads it."""
+    A = np.asarray(state["A"]).reshape(s.Nr, s.Nx, 4)[:, s.iExit].ravel()
+    B = np.asarray(state["B"]).reshape(s.Nr, s.Nx, 4)[:, s.iExit].ravel()
+    return {"A": A, "B": B}
+
+
+def run_fp64_check(args):
+    """Thrust and exhaust mass flow of the CUDA path (FP32, default precision)
+    against an FP64 run of the same scheme (the oracle in double precision),
+    after the same number of steps: config 1 at its full 2000 steps and the
+    viscous plume over a bounded 1000-step sample (its 10k steps take minutes
+    in FP64 on the host)."""
+    rn = ge.load_package()
+    oracle = ge.load_oracle()
+    oracle.set_threads(os.cpu_count() or 1)
+    from rocket_nozzle_cfd_solver_b200 import configs
+    out = {}
+    for name, cfg, n in (("plain 256x96 (config 1)", configs.plain_small()[0], 2000),
+                         ("viscous plume 512x192", configs.viscous_plume()[0], 1000)):
+        s = rn.build_sim_setup(cfg)
+        g = rn.GPUSolver(s.Nx, s.Nr)
+        g.setGeometry(s.geo)
+        init = s.initialState()
+        g.setState(init["A"], init["B"])
+        g.step(n, s.P)
+        gp = rn.exit_performance(s, exit_column(g.readAll(), s))
+        g.close()
+        o = oracle.OracleSolver(s.Nx, s.Nr, fp64=True)
+        o.setGeometry(s.geo)
+        o.setState(init["A"], init["B"])
+        o.step(n, s.P)
+        op = rn.exit_performance(s, exit_column(o.readAll(), s))
+        o.close()
+        out[name] = {"steps": n, "thrust_N": gp["F"], "mdot_kg_s": gp["mdot"],
+                     "thrust_rel_err": abs(gp["F"] - op["F"]) / max(abs(op["F"]), 1e-30),
+                     "mdot_rel_err": abs(gp["mdot"] - op["mdot"]) / max(abs(op["mdot"]), 1e-30)}
+    return out
+
+
 def serving_requests(rn, count, seed=7, spray_frac=0.2):
     """Seeded serving workload: nozzles drawn as in the batched workload; a
-    fraction are injector chambers with the spray (their parcel ring spawns
-    from the injector, 4 parcels per step, as the reference does)."""
+    fraction are injector chambers with the spray whose parcel ring starts with
+    U{16,384 .. 65,536} seeded parcels (configs.prepopulated_parcels) and keeps
+    spawning from the injector, 4 parcels per step, as the reference does.
+    Entries: (kind, setup, parcels or None)."""
     from rocket_nozzle_cfd_solver_b200 import configs
     rng = np.random.default_rng(seed)
     out = []
-    for _ in range(count):
+    for q in range(count):
         if rng.uniform() < spray_frac:
             Nx, Nr = configs.BATCH_SIZES[int(rng.integers(len(configs.BATCH_SIZES)))]
-            out.append(("spray", rn.build_sim_setup(configs.injector_spray(Nx, Nr)[0])))
+            s = rn.build_sim_setup(configs.injector_spray(Nx, Nr)[0])
+            npar = int(rng.integers(16384, 65537))
+            out.append(("spray", s, configs.prepopulated_parcels(s, npar, seed=20261203 + q)))
         else:
-            out.append(("nozzle", rn.build_sim_setup(configs.batched_instance(rng))))
+            out.append(("nozzle", rn.build_sim_setup(configs.batched_instance(rng)), None))
     return out
 
 
@@ -490,11 +591,11 @@ def serve_once(rn, reqs, arrivals, max_active, check_every, drop, t_end_s, max_c
     srv = rn.SolveServer(max_active=max_active, check_every=check_every, max_active_cells=max_cells)
     ids = []
     t0 = time.perf_counter()
-    for (kind, s), ta in zip(reqs, arrivals):
+    for (kind, s, parcels), ta in zip(reqs, arrivals):
         delay = ta - (time.perf_counter() - t0)
         if delay > 0:
             time.sleep(delay)
-        ids.append(srv.submit(s, drop=drop, t_end_s=t_end_s))
+        ids.append(srv.submit(s, drop=drop, t_end_s=t_end_s, parcels=parcels))
     res = [srv.wait(i, timeout_s=1800) for i in ids]
     st = srv.stats()
     srv.close()
@@ -528,10 +629,11 @@ def run_serving(args):
     status = {}
     for r in served:
         status[r["status"]] = status.get(r["status"], 0) + 1
-    cells = sum(s.Nx * s.Nr * r["steps"] for (_, s), r in zip(reqs, served))
+    cells = sum(s.Nx * s.Nr * r["steps"] for (_, s, _), r in zip(reqs, served))
     sv, pl = latency_summary(served), latency_summary(plain)
     return {"metric": "solves/s", "value": sv["solves_per_s"], "unit": "solves/s", "rate_per_s": rate,
-            "requests": len(reqs), "spray_requests": sum(1 for k, _ in reqs if k == "spray"),
+            "requests": len(reqs), "spray_requests": sum(1 for k, _, _ in reqs if k == "spray"),
+            "spray_parcels": [int((np.asarray(pc[1]).reshape(-1, 4)[:, 1] > 0).sum()) for k, _, pc in reqs if pc],
             "stop": "density residual drop 1e-4 or 2 ms simulated", "check_every": K,
             "max_active_cells": args.serve_max_cells,
             "p50_ms": sv["p50_ms"], "p99_ms": sv["p99_ms"], "makespan_s": sv["makespan_s"],
@@ -555,7 +657,10 @@ def main():
                     help="grid of the main viscous-plume leg (other sizes are for profiling; the bench line's "
                          "workload is 512x192)")
     ap.add_argument("--solver-steps", type=int, default=SOLVER_STEPS, help="time steps per bench step")
-    ap.add_argument("--no-large", action="store_true", help="skip the 4096x1536 HBM-resident sweep point")
+    ap.add_argument("--no-large", action="store_true",
+                    help="skip the 4096x1536 HBM-resident sweep point and the spray chamber leg")
+    ap.add_argument("--only-spray", action="store_true",
+                    help="run only the spray chamber leg and print its JSON object (for profiling)")
     ap.add_argument("--serve-requests", type=int, default=24, help="requests of the serving leg (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=5.0, help="Poisson arrival rate of the serving leg (1/s)")
     ap.add_argument("--serve-max-cells", type=int, default=2000000,
@@ -570,6 +675,11 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.only_spray:
+        import torch
+        torch.cuda.set_device(local_rank)
+        print(json.dumps(run_spray(args, local_rank)), flush=True)
         return
     if world > 1:
         import datetime

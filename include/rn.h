@@ -145,6 +145,11 @@ typedef struct {
   double type, weight, x, r, angle, speed, drop, cone, width, xi;
 } rn_injector_element;
 int rn_spray_build_injector(rn_handle h, const rn_injector_element* el, int n);
+/* A pre-populated parcel ring (no reference counterpart: the reference only
+ * spawns parcels from the injector): PA = (x, r, u, v) and PB = (d, m, type,
+ * x_imp), 65,536 float4 each in the ring's layout, become the current
+ * parcels; the given head is where the next 4 spawn. Dead slots have m <= 0. */
+int rn_spray_set_parcels(rn_handle h, const float* PA, const float* PB, int head);
 /* GPUSpray.reset() (spray.js:242-254) */
 int rn_spray_reset(rn_handle h);
 /* GPUSpray.stats(P) (spray.js:312-320): out = (fuel mass, oxidiser mass,
@@ -345,6 +350,9 @@ typedef struct {
   double drop;                      /* density-residual drop that ends the solve (0: off) */
   double t_end;                     /* normalised time that ends the solve (0: off) */
   long long max_steps;              /* step count that ends the solve (0: off) */
+  const float* parcelsA;            /* a pre-populated parcel ring (rn_spray_set_parcels), or NULL */
+  const float* parcelsB;
+  int parcelHead;
 } rn_solve_request;
 #define RN_SOLVE_CONVERGED 0
 #define RN_SOLVE_TIME 1

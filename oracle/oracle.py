@@ -81,6 +81,8 @@ def lib():
         L.rno_get_step_info.argtypes = [vp, dptr]
         L.rno_get_wall_row.argtypes = [vp, dptr]
         L.rno_get_t2.argtypes = [vp, dptr]
+        fptr32 = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+        L.rno_set_parcels.argtypes = [vp, fptr32, fptr32, i]
         L.rno_get_parcels.argtypes = [vp, dptr, dptr, dptr]
         L.rno_get_spray_counters.argtypes = [vp, np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")]
         L.rno_get_src.argtypes = [vp, dptr]
@@ -151,6 +153,11 @@ class OracleSolver:
         o = np.empty(self.Nx * 4)
         lib().rno_get_wall_row(self.h, o)
         return o
+
+    def setParcels(self, PA, PB, head):
+        """A pre-populated parcel ring (65,536 x 4 each) and its head."""
+        lib().rno_set_parcels(self.h, np.ascontiguousarray(PA, dtype=np.float32),
+                              np.ascontiguousarray(PB, dtype=np.float32), int(head))
 
     def readT2(self):
         """T2 of the last physics pass (effective viscosity, h, strain, laminar viscosity)."""

@@ -32,6 +32,7 @@
 #include <cstring>
 #include <vector>
 #include <algorithm>
+#include <type_traits>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -994,6 +995,20 @@ void rno_set_state(void* hp, const float* A, const float* B) {
 void rno_set_injector(void* hp, const float* tab) {
   Handle* h = static_cast<Handle*>(hp);
   for (int q = 0; q < 256 * 3 * 4; q++) { if (h->fp64) h->d.tab[q] = tab[q]; else h->f.tab[q] = tab[q]; }
+}
+// a pre-populated parcel ring: PA, PB (65536 x 4 each) into the current slot, PC cleared, ring head
+void rno_set_parcels(void* hp, const float* PA, const float* PB, int head) {
+  Handle* h = static_cast<Handle*>(hp);
+  auto set = [&](auto& s) {
+    using R = typename std::decay_t<decltype(s.PA[0])>::value_type;
+    for (int q = 0; q < SPRAY_N * 4; q++) {
+      s.PA[s.scur][q] = R(PA[q]);
+      s.PB[s.scur][q] = R(PB[q]);
+      s.PC[s.scur][q] = R(0);
+    }
+    s.head = uint32_t(((head % SPRAY_N) + SPRAY_N) % SPRAY_N);
+  };
+  if (h->fp64) set(h->d); else set(h->f);
 }
 void rno_step(void* hp, int n, const rno_params* p) {
   Handle* h = static_cast<Handle*>(hp);

@@ -34,6 +34,7 @@ void rno_get_state(void* h, double* A, double* B);
 void rno_get_step_info(void* h, double* out4);
 void rno_get_wall_row(void* h, double* out);
 void rno_get_t2(void* h, double* out);
+void rno_set_parcels(void* h, const float* PA, const float* PB, int head);
 void rno_get_parcels(void* h, double* PA, double* PB, double* PC);
 void rno_get_spray_counters(void* h, uint32_t* head_seed);
 void rno_get_src(void* h, double* out);

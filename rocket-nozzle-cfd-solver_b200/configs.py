@@ -90,3 +90,45 @@ def batched(count=64, seed=2024):
     import numpy as np
     rng = np.random.default_rng(seed)
     return [batched_instance(rng) for _ in range(count)]
+
+
+def prepopulated_parcels(setup, n, seed=20261203):
+    """A parcel ring already holding ``n`` parcels, for the injector chamber
+    ``setup``: each on a seeded uniform draw of the injector table's rows
+    (position on that element across its width), diameter lognormal (median
+    60 um, sigma 0.4), axial speed 30 m/s (oxidiser) or 120 m/s (fuel) times
+    U(0.9, 1.1), and the mass the reference gives a spawned parcel at the
+    initial time step (mhat dt / 4). Returns (PA, PB, head) in the ring's
+    layout: 65,536 x 4 float32 each, free slots dead, spawning resumes at n."""
+    import numpy as np
+    from .physics import U_REF
+    N = 65536
+    if not (0 <= n <= N):
+        raise ValueError("parcel count out of range")
+    rng = np.random.default_rng(seed)
+    tab = np.asarray(setup.injector["tab"], dtype=np.float64).reshape(3, 256, 4)
+    P = setup.P
+    init = setup.initialState()
+    A = init["A"].reshape(-1, 4).astype(np.float64)
+    B = init["B"].reshape(-1, 4).astype(np.float64)
+    fluid = np.asarray(setup.mask) == 0
+    rho = np.maximum(A[:, 0], 1e-7)
+    u, v = A[:, 1] / rho, A[:, 2] / rho
+    G = np.maximum(B[:, 2], 0.5)
+    p = np.maximum((A[:, 3] - 0.5 * rho * (u * u + v * v)) / G, 1e-7)
+    w = np.abs(u) + np.abs(v) + 2 * np.sqrt((1 + 1 / G) * p / rho)
+    dt = min(P["cfl"] / max(float(w[fluid].max()), P["wFloor"]), P["dtMax"])
+    m = P["spray"]["mhat"] * dt / 4
+    PA = np.zeros((N, 4), np.float32)
+    PB = np.zeros((N, 4), np.float32)
+    PA[:, 0] = PA[:, 1] = -1
+    rows = rng.integers(0, 256, size=n)
+    typ = tab[1, rows, 0]
+    PA[:n, 0] = tab[0, rows, 0]
+    PA[:n, 1] = np.maximum(tab[0, rows, 1] + (rng.uniform(size=n) - 0.5) * tab[1, rows, 3], 0.05)
+    PA[:n, 2] = np.where(typ >= 0.5, 30.0, 120.0) * rng.uniform(0.9, 1.1, size=n) / U_REF
+    PB[:n, 0] = 60e-6 * np.exp(0.4 * rng.standard_normal(n))
+    PB[:n, 1] = m
+    PB[:n, 2] = typ
+    PB[:n, 3] = tab[2, rows, 0]
+    return PA.reshape(-1), PB.reshape(-1), n % N

@@ -610,6 +610,16 @@ int rn_spray_set_injector(rn_handle h, const float* tab) {
   return RN_OK;
 }
 
+int rn_spray_set_parcels(rn_handle h, const float* PA, const float* PB, int head) {
+  if (!valid(h) || !PA || !PB) return fail(RN_ERR_ARG, "rn_spray_set_parcels: bad argument");
+  CK(cudaMemcpyAsync(h->PA[h->scur], PA, sizeof(float4) * SPRAY_N, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemcpyAsync(h->PB[h->scur], PB, sizeof(float4) * SPRAY_N, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemsetAsync(h->PC[h->scur], 0, sizeof(float4) * SPRAY_N, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->head = uint32_t(((head % SPRAY_N) + SPRAY_N) % SPRAY_N);
+  return RN_OK;
+}
+
 int rn_spray_reset(rn_handle h) {
   if (!valid(h)) return fail(RN_ERR_ARG, "rn_spray_reset: bad handle");
   return spray_reset_dev(h);

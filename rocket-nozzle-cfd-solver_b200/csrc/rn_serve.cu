@@ -42,7 +42,8 @@ struct Request {
   long long id = 0;
   int Nx = 0, Nr = 0;
   std::vector<uint8_t> mask;
-  std::vector<float> geoA, geoG, geoM, jWall, A, B, injTab;
+  std::vector<float> geoA, geoG, geoM, jWall, A, B, injTab, parA, parB;
+  int parHead = 0;
   rn_params P;
   double drop = 0.0, tEnd = 0.0;
   long long maxSteps = 0;
@@ -130,6 +131,8 @@ int admit(rn_server_t* s, Request& r, Active& a) {
     return bail(rc);
   if ((rc = rn_set_state(h, r.A.data(), r.B.data())) != RN_OK) return bail(rc);
   if (!r.injTab.empty() && (rc = rn_spray_set_injector(h, r.injTab.data())) != RN_OK) return bail(rc);
+  if (!r.parA.empty() && (rc = rn_spray_set_parcels(h, r.parA.data(), r.parB.data(), r.parHead)) != RN_OK)
+    return bail(rc);
   const int cls = class_of(r.P);
   rn_batch_t*& b = s->batches[cls];
   if (!b) {
@@ -423,6 +426,13 @@ int rn_serve_submit(rn_server s, const rn_solve_request* q, long long* id) {
   copy_in(r.A, q->A, N * 4);
   copy_in(r.B, q->B, N * 4);
   if (q->injTab) copy_in(r.injTab, q->injTab, size_t(768) * 4);
+  if ((q->parcelsA != nullptr) != (q->parcelsB != nullptr))
+    return sfail(RN_ERR_ARG, "rn_serve_submit: parcel ring needs both planes");
+  if (q->parcelsA) {
+    copy_in(r.parA, q->parcelsA, size_t(SPRAY_N) * 4);
+    copy_in(r.parB, q->parcelsB, size_t(SPRAY_N) * 4);
+    r.parHead = q->parcelHead;
+  }
   r.P = q->P;
   r.drop = q->drop;
   r.tEnd = q->t_end;

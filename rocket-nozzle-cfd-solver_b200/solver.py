@@ -36,6 +36,7 @@ EXPORTS = ("rn_create", "rn_destroy", "rn_resize", "rn_set_mask", "rn_set_geomet
            "rn_server_create", "rn_server_destroy", "rn_serve_submit", "rn_serve_poll", "rn_serve_wait",
            "rn_serve_stats", "rn_solve_bytes", "rn_set_wall_profile", "rn_wall_separation", "rn_derived",
            "rn_derived_buffer", "rn_build_geometry", "rn_get_geometry", "rn_spray_build_injector",
+           "rn_spray_set_parcels",
            "rn_last_error")
 PRECISION = {"fast": 0, "exact": 1}
 TILES = {"16x16": 0, "16x8": 1, "16x15": 2, "32x15": 3}
@@ -93,7 +94,8 @@ class RnSolveRequest(ctypes.Structure):
                 ("geoG", ctypes.c_void_p), ("geoM", ctypes.c_void_p), ("jWall", ctypes.c_void_p),
                 ("A", ctypes.c_void_p), ("B", ctypes.c_void_p), ("injTab", ctypes.c_void_p), ("P", RnParams),
                 ("spec", RnIntegralSpec), ("drop", ctypes.c_double), ("t_end", ctypes.c_double),
-                ("max_steps", ctypes.c_longlong)]
+                ("max_steps", ctypes.c_longlong), ("parcelsA", ctypes.c_void_p), ("parcelsB", ctypes.c_void_p),
+                ("parcelHead", ctypes.c_int)]
 
 
 class RnSolveResult(ctypes.Structure):
@@ -285,6 +287,7 @@ def lib():
     L.rn_build_geometry.argtypes = [H, ctypes.POINTER(RnCutSpec), ctypes.POINTER(RnCutStats)]
     L.rn_get_geometry.argtypes = [H] + [ctypes.c_void_p] * 5
     L.rn_spray_build_injector.argtypes = [H, ctypes.POINTER(RnInjectorElement), i]
+    L.rn_spray_set_parcels.argtypes = [H, ctypes.c_void_p, ctypes.c_void_p, i]
     L.rn_last_error.restype = ctypes.c_char_p
     for n in EXPORTS[:-1]:
         getattr(L, n).restype = ctypes.c_int
@@ -649,6 +652,12 @@ class GPUSpray:
                 setattr(arr[q], n, float(e[n]))
         _check(lib().rn_spray_build_injector(self.s.h, arr, len(el)))
 
+    def setParcels(self, PA, PB, head):
+        """Pre-populate the parcel ring: PA = (x, r, u, v), PB = (d, m, type,
+        x_imp), 65,536 x 4 floats each; ``head`` is where spawning continues."""
+        a, b = _f32(PA, SPRAY_N * 4), _f32(PB, SPRAY_N * 4)
+        _check(lib().rn_spray_set_parcels(self.s.h, a.ctypes.data, b.ctypes.data, int(head)))
+
     def reset(self):
         """spray.js:242-254"""
         if not self.ready:
@@ -772,10 +781,11 @@ class SolveServer:
         _check(lib().rn_solve_bytes(int(Nx), int(Nr), ctypes.byref(v)))
         return v.value
 
-    def submit(self, setup, drop=1e-4, t_end_s=2e-3, max_steps=0, state=None):
+    def submit(self, setup, drop=1e-4, t_end_s=2e-3, max_steps=0, state=None, parcels=None):
         """Queue a solve of ``setup`` from its initial state (or ``state``);
         stop at a density-residual drop of ``drop``, ``t_end_s`` seconds of
-        simulated time or ``max_steps`` steps. Returns the request id."""
+        simulated time or ``max_steps`` steps. ``parcels`` = (PA, PB, head)
+        pre-populates the spray ring. Returns the request id."""
         s = setup
         N, NF = s.Nx * s.Nr, (s.Nx + 1) * (s.Nr + 1)
         geo = s.geo
@@ -798,6 +808,10 @@ class SolveServer:
         r.drop = float(drop or 0.0)
         r.t_end = float(t_end_s) / float(s.tScale) if t_end_s else 0.0
         r.max_steps = int(max_steps or 0)
+        if parcels is not None:
+            pa, pb = _f32(parcels[0], SPRAY_N * 4), _f32(parcels[1], SPRAY_N * 4)
+            keep += [pa, pb]
+            r.parcelsA, r.parcelsB, r.parcelHead = pa.ctypes.data, pb.ctypes.data, int(parcels[2])
         rid = ctypes.c_longlong()
         _check(lib().rn_serve_submit(self.s, ctypes.byref(r), ctypes.byref(rid)))
         self.shapes[rid.value] = (s.Nx, s.Nr)

@@ -50,6 +50,7 @@ int main(void) {
          sizeof(rn_server_opts), sizeof(rn_solve_request), sizeof(rn_solve_result), sizeof(rn_serve_status));
   F(rn_server_opts, max_active) F(rn_server_opts, tile) F(rn_server_opts, max_active_cells) F(rn_solve_request, mask) F(rn_solve_request, injTab)
   F(rn_solve_request, P) F(rn_solve_request, spec) F(rn_solve_request, drop) F(rn_solve_request, max_steps)
+  F(rn_solve_request, parcelsA) F(rn_solve_request, parcelHead)
   F(rn_solve_result, steps) F(rn_solve_result, done_ms) F(rn_solve_result, integrals) F(rn_serve_status, failed)
   printf("rn_separation_spec %zu\nrn_separation_out %zu\n", sizeof(rn_separation_spec), sizeof(rn_separation_out));
   F(rn_separation_spec, dx) F(rn_separation_spec, pRef) F(rn_separation_out, x) F(rn_separation_out, Msep)

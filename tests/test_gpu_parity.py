@@ -77,3 +77,29 @@ def test_injector_spray_small(rn, oracle, n, precision):
     from rocket_nozzle_cfd_solver_b200.configs import injector_spray
     setup = rn.build_sim_setup(injector_spray(Nx=128, Nr=48)[0])
     compare(rn, oracle, setup, n, precision)
+
+
+def exit_column(state, s):
+    A = np.asarray(state["A"]).reshape(s.Nr, s.Nx, 4)[:, s.iExit].ravel()
+    B = np.asarray(state["B"]).reshape(s.Nr, s.Nx, 4)[:, s.iExit].ravel()
+    return {"A": A, "B": B}
+
+
+@pytest.mark.parametrize("case", ["config1", "viscous"])
+def test_thrust_and_mass_flow_against_fp64_scheme(rn, oracle, case):
+    """Exit thrust and exhaust mass flow of the FP32 CUDA path (default
+    precision) within 1e-3 relative of an FP64 run of the same scheme (the
+    oracle in double precision) after the same steps."""
+    from rocket_nozzle_cfd_solver_b200 import configs
+    if case == "config1":
+        cfg, n = configs.plain_small()[0], 2000
+    else:
+        cfg, n = configs.viscous_plume(256, 96)[0], 2400
+    s = rn.build_sim_setup(cfg)
+    g = gpu_run(rn, s, n, "fast")
+    gp = rn.exit_performance(s, exit_column(g.readAll(), s))
+    g.close()
+    op = rn.exit_performance(s, exit_column(run_oracle(oracle, s, n, fp64=True).readAll(), s))
+    assert op["mdot"] > 0 and op["F"] != 0
+    assert abs(gp["F"] - op["F"]) <= 1e-3 * abs(op["F"])
+    assert abs(gp["mdot"] - op["mdot"]) <= 1e-3 * abs(op["mdot"])
