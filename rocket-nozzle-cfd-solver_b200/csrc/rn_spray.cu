@@ -150,17 +150,31 @@ __global__ void __launch_bounds__(256) k_parcels(SprayArgs a, rn_params P) {
   a.dep[idx] = dep;
 }
 
-// one thread per run of equal keys: sum in parcel-index order
+// one thread per run of equal keys: sum in parcel-index order. The run is read
+// 8 records at a time so that their gathers are in flight together; the adds
+// stay sequential, in the same order.
 __global__ void k_segsum(const unsigned* __restrict__ key, const unsigned* __restrict__ val,
                          const float4* __restrict__ dep, float4* src, unsigned none) {
+  constexpr int U = 8;
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= SPRAY_N) return;
-  unsigned k = key[q];
+  const unsigned k = key[q];
   if (k == none || (q > 0 && key[q - 1] == k)) return;
   float sx = 0.f, sy = 0.f, sz = 0.f, sw = 0.f;
-  for (int r = q; r < SPRAY_N && key[r] == k; r++) {
-    float4 d = dep[val[r]];
-    sx = d.x + sx; sy = d.y + sy; sz = d.z + sz; sw = d.w + sw;
+  for (int r = q; r < SPRAY_N; r += U) {
+    bool in[U];
+    float4 d[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) in[u] = r + u < SPRAY_N && key[r + u] == k;
+#pragma unroll
+    for (int u = 0; u < U; u++) d[u] = in[u] ? dep[val[r + u]] : make_float4(0.f, 0.f, 0.f, 0.f);
+    bool more = true;
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      more = more && in[u];
+      if (more) { sx = d[u].x + sx; sy = d[u].y + sy; sz = d[u].z + sz; sw = d[u].w + sw; }
+    }
+    if (!more) break;
   }
   src[k] = make_float4(sx, sy, sz, sw);
 }
