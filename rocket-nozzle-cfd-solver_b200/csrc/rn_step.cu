@@ -175,7 +175,7 @@ __device__ __forceinline__ void member_faces(int cx, int cy, int x0, int y0, con
 template <class T>
 __host__ __device__ constexpr size_t stage_smem_t(int maxX) {
   return sizeof(float4) * (2 * (T::NPT + 25 * maxX) + 2 * (T::NXF + T::NRF + 4 * maxX)) +
-         sizeof(float) * (T::NXF + T::NRF + 4 * maxX);
+         sizeof(float) * 2 * (T::NXF + T::NRF + 4 * maxX);
 }
 // --------------------------------------------------------------------------
 // Phases shared by the stage, physics and fused kernels. Each loops its slots
@@ -203,20 +203,22 @@ __device__ __forceinline__ void load_prims(const Grid& g, const float4* __restri
 template <class T>
 __device__ __forceinline__ void inviscid_faces(const Grid& g, const rn_params& P, int x0, int y0, const int* xc,
                                                int NF, const float4* sW, const float4* sWb, float4* sF, float4* sY,
-                                               float* sO) {
+                                               float* sO, float* sAr) {
   const int Nx = g.Nx, Nr = g.Nr, W1 = Nx + 1;
   for (int k = threadIdx.x; k < NF; k += T::NT) {
     const FaceSlot s = face_slot<T>(k, x0, y0, xc, Nx, Nr);
     Flux f;
     f.F = make_float4(0.f, 0.f, 0.f, 0.f); f.Y = f.F; f.O = 0.f;
+    float area = 0.0f;
     if (s.valid) {
       float4 geo = g.geoA[s.j * W1 + s.i];
-      float area = s.dirR ? geo.w : geo.z;
+      area = s.dirR ? geo.w : geo.z;
       if (area != 0.0f)
         f = face_flux(s.dirR, area, sW[s.c[0]], sWb[s.c[0]], sW[s.c[1]], sWb[s.c[1]], sW[s.c[2]], sWb[s.c[2]],
                       sW[s.c[3]], sWb[s.c[3]], sW[s.s[0]], sW[s.s[1]], sW[s.s[2]], sW[s.s[3]], P);
     }
     sF[k] = f.F; sY[k] = f.Y; sO[k] = f.O;
+    sAr[k] = area;   // the face's (signed) open area, for the group sums
   }
 }
 
@@ -225,9 +227,10 @@ __device__ __forceinline__ void inviscid_faces(const Grid& g, const rn_params& P
 template <class T, int STAGE>
 __device__ __forceinline__ bool update_cell(const StageArgs& a, const rn_params& P, int i, int j, float dt, float t,
                                             int x0, int y0, const int* xc, int xn, const float4* sF,
-                                            const float4* sY, const float* sO, float4& oA, float4& oB) {
+                                            const float4* sY, const float* sO, const float* sAr, float4& oA,
+                                            float4& oB) {
   const Grid& g = a.g;
-  const int Nx = g.Nx, W1 = Nx + 1;
+  const int Nx = g.Nx;
   const int k = j * Nx + i;
   if (g.mask[k]) {
     oA = make_float4(P.ambCons[0], P.ambCons[1], P.ambCons[2], P.ambCons[3]);
@@ -248,11 +251,11 @@ __device__ __forceinline__ bool update_cell(const StageArgs& a, const rn_params&
     else if (m == 2) { if (!(sm_ & 2)) continue; cx += 1; }
     else if (m == 3) { if (!(sm_ & 4)) continue; cy -= 1; }
     else if (m == 4) { if (!(sm_ & 8)) continue; cy += 1; }
-    float4 gc = g.geoA[cy * W1 + cx];
-    float aw = fabsf(gc.z), ae = fabsf(g.geoA[cy * W1 + cx + 1].z);
-    float as_ = fabsf(gc.w), an = fabsf(g.geoA[(cy + 1) * W1 + cx].w);
+    // the member's four faces; their open areas are the ones the face phase
+    // read from geoA (0 on the axis face, whose flux is 0 too)
     int fw, fe, fs, fn;
     member_faces<T>(cx, cy, x0, y0, xc, xn, Nx, fw, fe, fs, fn);
+    const float aw = fabsf(sAr[fw]), ae = fabsf(sAr[fe]), as_ = fabsf(sAr[fs]), an = fabsf(sAr[fn]);
     sub4(L, ae, sF[fe], aw, sF[fw]);
     sub4(L, an, sF[fn], as_, sF[fs]);
     sub4(LY, ae, sY[fe], aw, sY[fw]);
@@ -328,6 +331,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const rn_params& 
   float4* sF = sWb + NP;
   float4* sY = sF + NF;
   float* sO = reinterpret_cast<float*>(sY + NF);
+  float* sAr = sO + NF;
   for (int q = tid; q < xn; q += NT) xc[q] = a.xcell[xb + q];
 
   float dt, t;
@@ -349,14 +353,14 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const rn_params& 
   __syncthreads();
   load_prims<T>(g, a.A, a.B, t, P, x0, y0, xc, NP, sW, sWb);
   __syncthreads();
-  inviscid_faces<T>(g, P, x0, y0, xc, NF, sW, sWb, sF, sY, sO);
+  inviscid_faces<T>(g, P, x0, y0, xc, NF, sW, sWb, sF, sY, sO, sAr);
   __syncthreads();
 
   const int i = x0 + tid % TX, j = y0 + tid / TX;
   float wcell = 0.0f;
   if (tid < T::NC && i < Nx && j < Nr) {
     float4 oA, oB;
-    const bool fluid = update_cell<T, STAGE>(a, P, i, j, dt, t, x0, y0, xc, xn, sF, sY, sO, oA, oB);
+    const bool fluid = update_cell<T, STAGE>(a, P, i, j, dt, t, x0, y0, xc, xn, sF, sY, sO, sAr, oA, oB);
     const int k = j * Nx + i;
     a.oA[k] = oA;
     a.oB[k] = oB;
@@ -453,10 +457,11 @@ template <class T>
 __device__ __forceinline__ bool source_cell(const Grid& g, const float4* __restrict__ A1,
                                             const float4* __restrict__ B1, const rn_params& P, int i, int j,
                                             float dt, int x0, int y0, const int* xc, int xn, const float4* sF,
-                                            const float4* sY, const float4* sT1, const float4* sT2, float4 A,
-                                            float4 B, float Bw, float4& oA, float4& oB) {
+                                            const float4* sY, const float* sAr, const float4* sT1,
+                                            const float4* sT2, float4 A, float4 B, float Bw, float4& oA,
+                                            float4& oB) {
   constexpr int TW = T::TW;
-  const int Nx = g.Nx, Nr = g.Nr, W1 = Nx + 1;
+  const int Nx = g.Nx, Nr = g.Nr;
   const int k = j * Nx + i;
   if (g.mask[k]) {
     oA = make_float4(P.ambCons[0], P.ambCons[1], P.ambCons[2], P.ambCons[3]);
@@ -482,11 +487,9 @@ __device__ __forceinline__ bool source_cell(const Grid& g, const float4* __restr
       else if (m == 2) { if (!(sm_ & 2)) continue; cx += 1; }
       else if (m == 3) { if (!(sm_ & 4)) continue; cy -= 1; }
       else if (m == 4) { if (!(sm_ & 8)) continue; cy += 1; }
-      float4 gc = g.geoA[cy * W1 + cx];
-      float aw = fabsf(gc.z), ae = fabsf(g.geoA[cy * W1 + cx + 1].z);
-      float as_ = fabsf(gc.w), an = fabsf(g.geoA[(cy + 1) * W1 + cx].w);
       int fw, fe, fs, fn;
       member_faces<T>(cx, cy, x0, y0, xc, xn, Nx, fw, fe, fs, fn);
+      const float aw = fabsf(sAr[fw]), ae = fabsf(sAr[fe]), as_ = fabsf(sAr[fs]), an = fabsf(sAr[fn]);
       sub4(L, ae, sF[fe], aw, sF[fw]);
       sub4(L, an, sF[fn], as_, sF[fs]);
       sub4(LY, ae, sY[fe], aw, sY[fw]);
@@ -594,7 +597,8 @@ __host__ __device__ constexpr size_t fused_region_t(int maxX) {
 }
 template <class T>
 __host__ __device__ constexpr size_t fused_smem_t(int maxX) {
-  return sizeof(float4) * (2 * (T::NPT + 25 * maxX) + fused_region_t<T>(maxX) + 2 * (T::NT + maxX));
+  return sizeof(float4) * (2 * (T::NPT + 25 * maxX) + fused_region_t<T>(maxX) + 2 * (T::NT + maxX)) +
+         sizeof(float) * (T::NXF + T::NRF + 4 * maxX);
 }
 template <class T>
 __device__ __forceinline__ void stage2_physics_body(const StageArgs& a, const PhysArgs& p, const rn_params& P, int bx,
@@ -612,6 +616,7 @@ __device__ __forceinline__ void stage2_physics_body(const StageArgs& a, const Ph
   float4* R = sWb + NP;
   float4* sA2 = R + fused_region_t<T>(xn);
   float4* sB2 = sA2 + NT + xn;
+  float* sAr = reinterpret_cast<float*>(sB2 + NT + xn);   // face areas, kept for FS_SOURCE
   for (int q = tid; q < xn; q += NT) xc[q] = a.xcell[xb + q];
   const float4 st = *a.stNew;
   const float dt = st.x, t = st.z;
@@ -622,19 +627,19 @@ __device__ __forceinline__ void stage2_physics_body(const StageArgs& a, const Ph
     float4* sF = R;
     float4* sY = sF + NF;
     float* sO = reinterpret_cast<float*>(sY + NF);
-    inviscid_faces<T>(g, P, x0, y0, xc, NF, sW, sWb, sF, sY, sO);
+    inviscid_faces<T>(g, P, x0, y0, xc, NF, sW, sWb, sF, sY, sO, sAr);
     __syncthreads();
     const int i = x0 + tid % TX, j = y0 + tid / TX;
     if (tid < T::NC && i < Nx && j < Nr) {
       float4 oA, oB;
-      update_cell<T, 2>(a, P, i, j, dt, t, x0, y0, xc, xn, sF, sY, sO, oA, oB);
+      update_cell<T, 2>(a, P, i, j, dt, t, x0, y0, xc, xn, sF, sY, sO, sAr, oA, oB);
       sA2[tid] = oA;
       sB2[tid] = oB;
     }
     for (int q = tid; q < xn; q += NT) {
       const int m = xc[q];
       float4 oA, oB;
-      update_cell<T, 2>(a, P, m % Nx, m / Nx, dt, t, x0, y0, xc, xn, sF, sY, sO, oA, oB);
+      update_cell<T, 2>(a, P, m % Nx, m / Nx, dt, t, x0, y0, xc, xn, sF, sY, sO, sAr, oA, oB);
       sA2[NT + q] = oA;
       sB2[NT + q] = oB;
     }
@@ -672,7 +677,8 @@ __device__ __forceinline__ void stage2_physics_body(const StageArgs& a, const Ph
       B = sB2[s];
       Bw = sB2[tid].w;
     }
-    const bool fluid = source_cell<T>(g, p.A1, p.B1, P, i, j, dt, x0, y0, xc, xnP, sF, sY, sT1, sT2, A, B, Bw, oA, oB);
+    const bool fluid = source_cell<T>(g, p.A1, p.B1, P, i, j, dt, x0, y0, xc, xnP, sF, sY, sAr, sT1, sT2, A, B, Bw,
+                                      oA, oB);
     p.oA[k] = oA;
     p.oB[k] = oB;
     if (p.finalCfl && fluid) wcell = wave_speed(oA, oB);
