@@ -57,8 +57,10 @@ void free_buffers(rn_solver* h) {
   cudaFree(h->PA[0]);   // base of the 6-plane parcel ring
   for (int p = 0; p < 2; p++) h->PA[p] = h->PB[p] = h->PC[p] = nullptr;
   cudaFree(h->src); cudaFree(h->tab); cudaFree(h->dep); cudaFree(h->key); cudaFree(h->sortTemp);
-  cudaFree(h->xoff); cudaFree(h->xcell);
+  cudaFree(h->xoff); cudaFree(h->xcell); cudaFree(h->heavy);
   h->xoff = h->xcell = nullptr;
+  h->heavy = nullptr;
+  h->nHeavy = 0;
   cudaFree(h->mark); cudaFree(h->dRes); cudaFree(h->wallProf); cudaFree(h->derived);
   h->mark = h->markSt = nullptr;
   h->dRes = nullptr;
@@ -197,8 +199,21 @@ int rn_build_member_lists(rn_solver* h) {
   CK(cudaMalloc(&h->xcell, sizeof(int) * cells.size()));
   CK(cudaMemcpyAsync(h->xoff, off.data(), sizeof(int) * (nT + 1), cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync(h->xcell, cells.data(), sizeof(int) * cells.size(), cudaMemcpyHostToDevice, h->stream));
+  // tiles whose lists need more shared memory than the common launch holds
+  std::vector<int> heavy;
+  for (int t = 0; t < nT; t++)
+    if (off[t + 1] - off[t] > XSMALL) heavy.push_back(t);
+  cudaFree(h->heavy);
+  h->heavy = nullptr;
+  h->nHeavy = 0;
+  if (!heavy.empty()) {
+    CK(cudaMalloc(&h->heavy, sizeof(int) * heavy.size()));
+    CK(cudaMemcpyAsync(h->heavy, heavy.data(), sizeof(int) * heavy.size(), cudaMemcpyHostToDevice, h->stream));
+    h->nHeavy = int(heavy.size());
+  }
   CK(cudaStreamSynchronize(h->stream));
   h->maxX = maxX;
+  h->hostXoff = off;
   return RN_OK;
 }
 
@@ -268,6 +283,7 @@ int rn_create(int Nx, int Nr, rn_handle* out) {
   if (e != cudaSuccess) { delete h; return cuda_fail(e, "cudaStreamCreate"); }
   e = cudaEventCreateWithFlags(&h->asyncEv, cudaEventDisableTiming);
   if (e != cudaSuccess) { cudaStreamDestroy(h->stream); delete h; return cuda_fail(e, "cudaEventCreate"); }
+  cudaDeviceGetAttribute(&h->numSMs, cudaDevAttrMultiProcessorCount, h->device);
   {
     // process-wide kernel attributes, once (the solve server creates handles
     // on its worker thread while callers may create their own)
@@ -306,6 +322,12 @@ int rn_destroy(rn_handle h) {
   for (auto& p : h->evPending) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
   for (auto e : h->evPool) cudaEventDestroy(e);
   cudaEventDestroy(h->asyncEv);
+  if (h->side) {
+    cudaStreamSynchronize(h->side);
+    cudaEventDestroy(h->evFork);
+    cudaEventDestroy(h->evJoin);
+    cudaStreamDestroy(h->side);
+  }
   cudaStreamDestroy(h->stream);
   delete h;
   return RN_OK;
@@ -458,7 +480,24 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
       p.st = stNew; p.wOut = wOut; p.finalCfl = inj ? 0 : 1;
       p.xoff = h->xoff; p.xcell = h->xcell; p.maxX = h->maxX;
       ProfScope ps(h, RN_K_STAGE2_PHYSICS);
-      h->K->stage2phys(b, p, *P, h->tile, h->stream);
+      const int nTiles = int(h->hostXoff.size()) - 1;
+      if (h->nHeavy > 0 && nTiles > SPLIT_BLOCKS_PER_SM * h->numSMs) {
+        // the few tiles with long member lists on the side stream, at the same time
+        if (!h->side) {
+          CK(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+          CK(cudaEventCreateWithFlags(&h->evFork, cudaEventDisableTiming));
+          CK(cudaEventCreateWithFlags(&h->evJoin, cudaEventDisableTiming));
+        }
+        CK(cudaEventRecord(h->evFork, h->stream));
+        CK(cudaStreamWaitEvent(h->side, h->evFork, 0));
+        h->K->stage2phys(b, p, *P, h->tile, h->heavy, h->nHeavy, false, h->side);
+        CK(cudaEventRecord(h->evJoin, h->side));
+        h->K->stage2phys(b, p, *P, h->tile, nullptr, h->nHeavy, true, h->stream);
+        CK(cudaStreamWaitEvent(h->stream, h->evJoin, 0));
+        h->launches++;
+      } else {
+        h->K->stage2phys(b, p, *P, h->tile, nullptr, 0, false, h->stream);
+      }
     } else {
       ProfScope ps(h, RN_K_STAGE2);
       h->K->stage2(b, *P, h->tile, h->stream);

@@ -67,11 +67,19 @@ struct rn_batch_t {
   std::vector<BatchInst> uploaded;      // what dInst holds
   std::vector<int> layout;              // (Nx, Nr) per member the block table was built for
   int nblocks = 0, maxX = 1;
+  int2* dHeavy = nullptr;               // (member, tile) of the tiles with long out-of-tile lists
+  size_t heavyCap = 0;
+  std::vector<int2> heavy;              // what dHeavy holds
+  int nHeavy = 0;
+  bool split = false;                   // heavy tiles run beside the main launch (see XSMALL)
+  int numSMs = 148;
+  cudaStream_t side = nullptr;
+  cudaEvent_t evFork = nullptr, evJoin = nullptr;
   const KernelSet* K = nullptr;
   // the graph of one period
   cudaGraphExec_t graph = nullptr;
   const KernelSet* graphK = nullptr;
-  int graphBlocks = -1, graphTile = -1, graphMaxX = -1;
+  int graphBlocks = -1, graphTile = -1, graphMaxX = -1, graphHeavy = -1;
   Flags graphFlags;
   long long launches = 0;
 };
@@ -89,7 +97,7 @@ void drop_graph(rn_batch_t* b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
   b->graph = nullptr;
   b->graphK = nullptr;
-  b->graphBlocks = b->graphTile = b->graphMaxX = -1;
+  b->graphBlocks = b->graphTile = b->graphMaxX = b->graphHeavy = -1;
 }
 
 int index_of(const rn_batch_t* b, const rn_solver* h) {
@@ -164,6 +172,31 @@ int refresh(rn_batch_t* b) {
     maxX = std::max(maxX, h->maxX);
   }
   b->maxX = maxX;
+  // heavy tiles: their own fused launch (see XSMALL)
+  std::vector<int2> heavy;
+  for (int m = 0; m < nm; m++) {
+    const std::vector<int>& off = b->members[m]->hostXoff;
+    for (size_t t = 0; t + 1 < off.size(); t++)
+      if (off[t + 1] - off[t] > XSMALL) heavy.push_back(make_int2(m, int(t)));
+  }
+  const bool heavySame = heavy.size() == b->heavy.size() &&
+                         (heavy.empty() || std::memcmp(heavy.data(), b->heavy.data(), sizeof(int2) * heavy.size()) == 0);
+  if (!heavySame) {
+    BCK(cudaStreamSynchronize(b->stream));
+    if (heavy.size() > b->heavyCap) {
+      cudaFree(b->dHeavy);
+      b->dHeavy = nullptr;
+      b->heavyCap = 0;
+      BCK(cudaMalloc(&b->dHeavy, sizeof(int2) * heavy.size()));
+      b->heavyCap = heavy.size();
+      drop_graph(b);
+    }
+    if (!heavy.empty())
+      BCK(cudaMemcpy(b->dHeavy, heavy.data(), sizeof(int2) * heavy.size(), cudaMemcpyHostToDevice));
+    b->heavy = heavy;
+    b->nHeavy = int(heavy.size());
+  }
+  b->split = b->nHeavy > 0 && b->nblocks > SPLIT_BLOCKS_PER_SM * b->numSMs;
   const bool same = inst.size() == b->uploaded.size() &&
                     (inst.empty() || std::memcmp(inst.data(), b->uploaded.data(), sizeof(BatchInst) * inst.size()) == 0);
   if (!same && nm > 0) {
@@ -230,8 +263,22 @@ int launch_step(rn_batch_t* b, int c, bool withSpray) {
     }
   }
   ph.finalCfl = f.inj ? 0 : 1;
-  if (f.phys()) b->K->batchStage2Phys(b->dInst, b->dBlock, nb, ph, b->tile, b->stream);
-  else b->K->batchStage2(b->dInst, b->dBlock, nb, ph, b->tile, b->stream);
+  if (f.phys()) {
+    if (b->split) {
+      // the few tiles with long member lists on the side stream, at the same time
+      cudaEventRecord(b->evFork, b->stream);
+      cudaStreamWaitEvent(b->side, b->evFork, 0);
+      b->K->batchStage2Phys(b->dInst, b->dBlock, nb, ph, b->tile, b->dHeavy, b->nHeavy, false, b->side);
+      cudaEventRecord(b->evJoin, b->side);
+      b->K->batchStage2Phys(b->dInst, b->dBlock, nb, ph, b->tile, nullptr, b->nHeavy, true, b->stream);
+      cudaStreamWaitEvent(b->stream, b->evJoin, 0);
+      b->launches++;
+    } else {
+      b->K->batchStage2Phys(b->dInst, b->dBlock, nb, ph, b->tile, nullptr, 0, false, b->stream);
+    }
+  } else {
+    b->K->batchStage2(b->dInst, b->dBlock, nb, ph, b->tile, b->stream);
+  }
   b->launches++;
   if (f.inj && withSpray) {
     for (size_t m = 0; m < b->members.size(); m++) {
@@ -280,11 +327,12 @@ int build_graph(rn_batch_t* b) {
   b->graphBlocks = b->nblocks;
   b->graphTile = b->tile;
   b->graphMaxX = b->maxX;
+  b->graphHeavy = b->split ? b->nHeavy : 0;
   b->graphFlags = b->flags;
   return RN_OK;
 }
 
-int launches_per_step(const rn_batch_t*) { return 2; }
+int launches_per_step(const rn_batch_t* b) { return 2 + ((b->flags.phys() && b->split) ? 1 : 0); }
 
 }  // namespace
 
@@ -303,7 +351,14 @@ int rn_batch_create(rn_batch* out) {
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->staged, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->evFork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->evJoin, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&b->numSMs, cudaDevAttrMultiProcessorCount, b->device);
   if (e != cudaSuccess) {
+    if (b->evJoin) cudaEventDestroy(b->evJoin);
+    if (b->evFork) cudaEventDestroy(b->evFork);
+    if (b->side) cudaStreamDestroy(b->side);
     if (b->staged) cudaEventDestroy(b->staged);
     if (b->done) cudaEventDestroy(b->done);
     if (b->stream) cudaStreamDestroy(b->stream);
@@ -322,9 +377,14 @@ int rn_batch_destroy(rn_batch b) {
   drop_graph(b);
   cudaFree(b->dInst);
   cudaFree(b->dBlock);
+  cudaFree(b->dHeavy);
   cudaFreeHost(b->hInst);
   cudaEventDestroy(b->staged);
   cudaEventDestroy(b->done);
+  cudaStreamSynchronize(b->side);
+  cudaEventDestroy(b->evFork);
+  cudaEventDestroy(b->evJoin);
+  cudaStreamDestroy(b->side);
   cudaStreamDestroy(b->stream);
   delete b;
   return RN_OK;
@@ -454,7 +514,7 @@ int rn_batch_step(rn_batch b, int n) {
     }
     if (n - done >= PERIOD) {
       if (!b->graph || b->graphK != b->K || b->graphBlocks != b->nblocks || b->graphTile != b->tile ||
-          b->graphMaxX != b->maxX || !(b->graphFlags == f)) {
+          b->graphMaxX != b->maxX || b->graphHeavy != (b->split ? b->nHeavy : 0) || !(b->graphFlags == f)) {
         rc = build_graph(b);
         if (rc != RN_OK) return rc;
       }

@@ -50,6 +50,13 @@ struct rn_solver {
   int* xoff = nullptr;
   int* xcell = nullptr;
   int maxX = 1;
+  std::vector<int> hostXoff;
+  // tiles listing more than XSMALL out-of-tile members (own fused launch)
+  int* heavy = nullptr;
+  int nHeavy = 0;
+  int numSMs = 148;
+  cudaStream_t side = nullptr;          // runs the heavy tiles' launch beside the main one
+  cudaEvent_t evFork = nullptr, evJoin = nullptr;
   std::vector<uint8_t> hostMask;
   std::vector<float> hostGeoM;
   // kernels of the selected precision (rn_set_precision)

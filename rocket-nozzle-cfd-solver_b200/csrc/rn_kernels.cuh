@@ -23,6 +23,17 @@ constexpr int TILE_TY[NTILES] = {16, 8, 15, 15};
 constexpr int TILE_NT[NTILES] = {256, 128, 256, 512};
 // Most out-of-tile group members one tile may list (set_geometry rejects more).
 constexpr int MAXX = 64;
+// Tiles listing more out-of-tile members than this run the fused stage-2 +
+// split-step kernel in a launch of their own, sized for them, so that the
+// shared memory of every other block stays within 4 blocks per SM (a 1024x384
+// bell has a wall tile with 16; it cost the whole launch a quarter of its
+// occupancy).
+constexpr int XSMALL = 4;
+// The split (a side-stream launch joined back) pays only on grids of many
+// waves: more tiles than SPLIT_BLOCKS_PER_SM x SMs. Measured with 16x16 tiles:
+// 64 batched instances (36,400 blocks) 3.59 -> 3.97 G cell-updates/s; a lone
+// 1024x384 grid (1,536 blocks) 3.67 -> 3.60, so it is not split.
+constexpr int SPLIT_BLOCKS_PER_SM = 16;
 
 struct StageArgs {
   Grid g;
@@ -110,11 +121,14 @@ struct KernelSet {
   void (*stage1)(const StageArgs& a, const rn_params& P, int tile, cudaStream_t s);
   void (*stage2)(const StageArgs& a, const rn_params& P, int tile, cudaStream_t s);
   // stage 2 + the viscous/wall/reaction split step in one kernel
-  void (*stage2phys)(const StageArgs& a, const PhysArgs& p, const rn_params& P, int tile, cudaStream_t s);
+  // heavy != nullptr: launch the tiles listing more than XSMALL out-of-tile
+  // members (nHeavy of them); else all tiles, skipping those when `skip`
+  void (*stage2phys)(const StageArgs& a, const PhysArgs& p, const rn_params& P, int tile, const int* heavy,
+                     int nHeavy, bool skip, cudaStream_t s);
   void (*batchStage1)(const BatchInst* d, const int* blockInst, int nblocks, BatchPhase ph, int tile, cudaStream_t s);
   void (*batchStage2)(const BatchInst* d, const int* blockInst, int nblocks, BatchPhase ph, int tile, cudaStream_t s);
   void (*batchStage2Phys)(const BatchInst* d, const int* blockInst, int nblocks, BatchPhase ph, int tile,
-                          cudaStream_t s);
+                          const int2* heavy, int nHeavy, bool skip, cudaStream_t s);
   void (*reduce)(const Grid& g, const float4* A, const float4* B, unsigned* w, cudaStream_t s);
   void (*rescale)(const Grid& g, const float4* A, const float4* B, float4* oA, float4* oB, float fp, float fT,
                   float du, const rn_params& P, cudaStream_t s);

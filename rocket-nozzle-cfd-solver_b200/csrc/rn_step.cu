@@ -695,19 +695,36 @@ __global__ void __launch_bounds__(T::NT, T::MINB) k_stage(StageArgs a, rn_params
   __shared__ int xc[MAXX];
   stage_body<T, STAGE>(a, P, blockIdx.x, blockIdx.y, blockIdx.y * gridDim.x + blockIdx.x, sm, red, xc);
 }
+// heavy == nullptr: one block per tile of the grid, skipping tiles that list
+// more than xSmall out-of-tile members (xSmall < 0: none skipped); otherwise
+// block b runs tile heavy[b] (the skipped tiles, in a launch of their own with
+// the shared memory their lists need).
 template <class T>
-__global__ void __launch_bounds__(T::NT, T::MINB) k_stage2phys(StageArgs a, PhysArgs p, rn_params P) {
+__global__ void __launch_bounds__(T::NT, T::MINB) k_stage2phys(StageArgs a, PhysArgs p, rn_params P,
+                                                               const int* heavy, int xSmall) {
   extern __shared__ float4 sm[];
   __shared__ float red[T::NT / 32];
   __shared__ int xc[MAXX];
-  stage2_physics_body<T>(a, p, P, blockIdx.x, blockIdx.y, blockIdx.y * gridDim.x + blockIdx.x, sm, red, xc);
+  int bx, by, tile;
+  if (heavy) {
+    const int tilesX = (a.g.Nx + T::TX - 1) / T::TX;
+    tile = heavy[blockIdx.x];
+    by = tile / tilesX;
+    bx = tile - by * tilesX;
+  } else {
+    bx = blockIdx.x;
+    by = blockIdx.y;
+    tile = by * gridDim.x + bx;
+    if (xSmall >= 0 && a.xoff[tile + 1] - a.xoff[tile] > xSmall) return;
+  }
+  stage2_physics_body<T>(a, p, P, bx, by, tile, sm, red, xc);
 }
 
 // Batch kernels: block b belongs to instance blockInst[b]; its descriptor
 // (buffers, ring position, parameter block) is staged in shared memory.
-__device__ __forceinline__ void load_inst(const BatchInst* insts, const int* blockInst, BatchInst& d) {
+__device__ __forceinline__ void load_inst(const BatchInst* insts, int inst, BatchInst& d) {
   __shared__ int di;
-  if (threadIdx.x == 0) di = blockInst[blockIdx.x];
+  if (threadIdx.x == 0) di = inst;
   __syncthreads();
   const int* src = reinterpret_cast<const int*>(insts + di);
   int* dst = reinterpret_cast<int*>(&d);
@@ -720,7 +737,7 @@ __global__ void __launch_bounds__(T::NT, T::MINB) k_stage_batch(const BatchInst*
   __shared__ float red[T::NT / 32];
   __shared__ int xc[MAXX];
   __shared__ BatchInst d;
-  load_inst(insts, blockInst, d);
+  load_inst(insts, blockInst[blockIdx.x], d);
   const int s0 = (d.cur0 + ph.shift) % 3, s1 = (s0 + 1) % 3, s2 = (s0 + 2) % 3;
   const int si = d.stepIdx0 ^ ph.par, ws = d.wslot0 ^ ph.par;
   StageArgs a;
@@ -741,12 +758,13 @@ __global__ void __launch_bounds__(T::NT, T::MINB) k_stage_batch(const BatchInst*
 }
 template <class T>
 __global__ void __launch_bounds__(T::NT, T::MINB) k_stage2phys_batch(const BatchInst* insts, const int* blockInst,
-                                                                     BatchPhase ph) {
+                                                                     BatchPhase ph, const int2* heavy, int xSmall) {
   extern __shared__ float4 sm[];
   __shared__ float red[T::NT / 32];
   __shared__ int xc[MAXX];
   __shared__ BatchInst d;
-  load_inst(insts, blockInst, d);
+  const int2 hv = heavy ? heavy[blockIdx.x] : make_int2(0, 0);   // (member, tile) of a heavy block
+  load_inst(insts, heavy ? hv.x : blockInst[blockIdx.x], d);
   const int s0 = (d.cur0 + ph.shift) % 3, s1 = (s0 + 1) % 3, s2 = (s0 + 2) % 3;
   const int si = d.stepIdx0 ^ ph.par, ws = d.wslot0 ^ ph.par;
   StageArgs a;
@@ -765,7 +783,8 @@ __global__ void __launch_bounds__(T::NT, T::MINB) k_stage2phys_batch(const Batch
   p.wOut = d.wmax + (1 - ws);
   p.finalCfl = ph.finalCfl;
   p.xoff = d.xoff; p.xcell = d.xcell; p.maxX = ph.maxX;
-  const int local = blockIdx.x - d.firstBlock, by = local / d.tilesX, bx = local - by * d.tilesX;
+  const int local = heavy ? hv.y : blockIdx.x - d.firstBlock, by = local / d.tilesX, bx = local - by * d.tilesX;
+  if (!heavy && xSmall >= 0 && d.xoff[local + 1] - d.xoff[local] > xSmall) return;   // in the heavy launch
   stage2_physics_body<T>(a, p, d.P, bx, by, local, sm, red, xc);
 }
 
@@ -934,15 +953,27 @@ void launch_stage2(const StageArgs& a, const rn_params& P, int tile, cudaStream_
   else if (tile == 1) k_stage<Tile1, 2><<<tiles_of<Tile1>(a.g), Tile1::NT, stage_smem_t<Tile1>(a.maxX), s>>>(a, P);
   else k_stage<Tile0, 2><<<tiles_of<Tile0>(a.g), Tile0::NT, stage_smem_t<Tile0>(a.maxX), s>>>(a, P);
 }
-void launch_stage2phys(const StageArgs& a, const PhysArgs& p, const rn_params& P, int tile, cudaStream_t s) {
-  if (tile == 3)
-    k_stage2phys<Tile3><<<tiles_of<Tile3>(a.g), Tile3::NT, fused_smem_t<Tile3>(a.maxX), s>>>(a, p, P);
-  else if (tile == 2)
-    k_stage2phys<Tile2><<<tiles_of<Tile2>(a.g), Tile2::NT, fused_smem_t<Tile2>(a.maxX), s>>>(a, p, P);
-  else if (tile == 1)
-    k_stage2phys<Tile1><<<tiles_of<Tile1>(a.g), Tile1::NT, fused_smem_t<Tile1>(a.maxX), s>>>(a, p, P);
-  else
-    k_stage2phys<Tile0><<<tiles_of<Tile0>(a.g), Tile0::NT, fused_smem_t<Tile0>(a.maxX), s>>>(a, p, P);
+// heavy != nullptr: the heavy tiles alone (nHeavy blocks, shared memory for
+// their lists); otherwise every tile, with the heavy ones skipped when `skip`
+// (they then run in the other launch, on another stream at the same time).
+template <class T>
+static void stage2phys_t(const StageArgs& a, const PhysArgs& p, const rn_params& P, const int* heavy, int nHeavy,
+                         bool skip, cudaStream_t s) {
+  if (heavy) {
+    k_stage2phys<T><<<nHeavy, T::NT, fused_smem_t<T>(a.maxX), s>>>(a, p, P, heavy, -1);
+  } else if (skip) {
+    const int xs = a.maxX < XSMALL ? a.maxX : XSMALL;
+    k_stage2phys<T><<<tiles_of<T>(a.g), T::NT, fused_smem_t<T>(xs), s>>>(a, p, P, nullptr, XSMALL);
+  } else {
+    k_stage2phys<T><<<tiles_of<T>(a.g), T::NT, fused_smem_t<T>(a.maxX), s>>>(a, p, P, nullptr, -1);
+  }
+}
+void launch_stage2phys(const StageArgs& a, const PhysArgs& p, const rn_params& P, int tile, const int* heavy,
+                       int nHeavy, bool skip, cudaStream_t s) {
+  if (tile == 3) stage2phys_t<Tile3>(a, p, P, heavy, nHeavy, skip, s);
+  else if (tile == 2) stage2phys_t<Tile2>(a, p, P, heavy, nHeavy, skip, s);
+  else if (tile == 1) stage2phys_t<Tile1>(a, p, P, heavy, nHeavy, skip, s);
+  else stage2phys_t<Tile0>(a, p, P, heavy, nHeavy, skip, s);
 }
 void launch_batch_stage1(const BatchInst* d, const int* bi, int nb, BatchPhase ph, int tile, cudaStream_t s) {
   if (tile == 3) k_stage_batch<Tile3, 1><<<nb, Tile3::NT, stage_smem_t<Tile3>(ph.maxX), s>>>(d, bi, ph);
@@ -956,11 +987,25 @@ void launch_batch_stage2(const BatchInst* d, const int* bi, int nb, BatchPhase p
   else if (tile == 1) k_stage_batch<Tile1, 2><<<nb, Tile1::NT, stage_smem_t<Tile1>(ph.maxX), s>>>(d, bi, ph);
   else k_stage_batch<Tile0, 2><<<nb, Tile0::NT, stage_smem_t<Tile0>(ph.maxX), s>>>(d, bi, ph);
 }
-void launch_batch_stage2phys(const BatchInst* d, const int* bi, int nb, BatchPhase ph, int tile, cudaStream_t s) {
-  if (tile == 3) k_stage2phys_batch<Tile3><<<nb, Tile3::NT, fused_smem_t<Tile3>(ph.maxX), s>>>(d, bi, ph);
-  else if (tile == 2) k_stage2phys_batch<Tile2><<<nb, Tile2::NT, fused_smem_t<Tile2>(ph.maxX), s>>>(d, bi, ph);
-  else if (tile == 1) k_stage2phys_batch<Tile1><<<nb, Tile1::NT, fused_smem_t<Tile1>(ph.maxX), s>>>(d, bi, ph);
-  else k_stage2phys_batch<Tile0><<<nb, Tile0::NT, fused_smem_t<Tile0>(ph.maxX), s>>>(d, bi, ph);
+template <class T>
+static void batch_stage2phys_t(const BatchInst* d, const int* bi, int nb, BatchPhase ph, const int2* heavy,
+                               int nHeavy, bool skip, cudaStream_t s) {
+  if (heavy) {
+    k_stage2phys_batch<T><<<nHeavy, T::NT, fused_smem_t<T>(ph.maxX), s>>>(d, bi, ph, heavy, -1);
+  } else if (skip) {
+    BatchPhase pl = ph;
+    pl.maxX = ph.maxX < XSMALL ? ph.maxX : XSMALL;
+    k_stage2phys_batch<T><<<nb, T::NT, fused_smem_t<T>(pl.maxX), s>>>(d, bi, pl, nullptr, XSMALL);
+  } else {
+    k_stage2phys_batch<T><<<nb, T::NT, fused_smem_t<T>(ph.maxX), s>>>(d, bi, ph, nullptr, -1);
+  }
+}
+void launch_batch_stage2phys(const BatchInst* d, const int* bi, int nb, BatchPhase ph, int tile, const int2* heavy,
+                             int nHeavy, bool skip, cudaStream_t s) {
+  if (tile == 3) batch_stage2phys_t<Tile3>(d, bi, nb, ph, heavy, nHeavy, skip, s);
+  else if (tile == 2) batch_stage2phys_t<Tile2>(d, bi, nb, ph, heavy, nHeavy, skip, s);
+  else if (tile == 1) batch_stage2phys_t<Tile1>(d, bi, nb, ph, heavy, nHeavy, skip, s);
+  else batch_stage2phys_t<Tile0>(d, bi, nb, ph, heavy, nHeavy, skip, s);
 }
 void launch_reduce(const Grid& g, const float4* A, const float4* B, unsigned* w, cudaStream_t s) {
   int N = g.Nx * g.Nr;

@@ -205,3 +205,37 @@ def test_batch_autotune_restores_members(rn):
     batch.close()
     for g in members + singles:
         g.close()
+
+
+def test_heavy_tiles_run_in_their_own_launch(rn):
+    """With 16x16 tiles a 1024x384 bell has wall tiles listing more out-of-tile
+    group members than the common fused launch holds. On a grid of many waves
+    those tiles run in a launch of their own, on a side stream beside the main
+    one. Results stay bit-identical to the 16x15 tiling (whose lists are all
+    short), alone and in a batch."""
+    s = setups(rn, "viscous", [(1024, 384)])[0]
+    small = setups(rn, "viscous", [(128, 48)])[0]
+    outs = []
+    for tile in ("16x15", "16x16"):
+        g = make(rn, s, tile=tile)
+        g.step(12, s.P)
+        outs.append(g.readAll())
+        g.close()
+    assert identical(outs[0], outs[1])
+    batch = rn.SolverBatch()
+    bigs = [make(rn, s) for _ in range(2)]
+    little = make(rn, small)
+    for g in bigs:
+        batch.add(g, s.P)
+    batch.add(little, small.P)
+    batch.setTile("16x16")                                    # 2 x 1,536 + 24 blocks: split
+    n0 = batch.kernelLaunches()
+    batch.step(12)
+    batch.sync()
+    assert batch.kernelLaunches() - n0 == 3 * 12
+    ref = make(rn, small)
+    ref.step(12, small.P)
+    assert all(identical(g.readAll(), outs[0]) for g in bigs) and identical(little.readAll(), ref.readAll())
+    batch.close()
+    for g in bigs + [little, ref]:
+        g.close()

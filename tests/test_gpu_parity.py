@@ -103,3 +103,38 @@ def test_thrust_and_mass_flow_against_fp64_scheme(rn, oracle, case):
     assert op["mdot"] > 0 and op["F"] != 0
     assert abs(gp["F"] - op["F"]) <= 1e-3 * abs(op["F"])
     assert abs(gp["mdot"] - op["mdot"]) <= 1e-3 * abs(op["mdot"])
+
+
+@pytest.mark.parametrize("size", [(40, 15), (129, 47), (97, 61)])
+def test_ragged_grids_bit_identical_in_exact_mode(rn, oracle, size):
+    """Grids that fill no tile evenly (odd widths and heights, fewer cells
+    than one row of tiles): in exact precision every tile shape gives the same
+    bits, within 1e-6 of the oracle (bit-identical where pow/exp/log agree
+    with the host libm) over 40 steps."""
+    from rocket_nozzle_cfd_solver_b200 import solver
+    from rocket_nozzle_cfd_solver_b200.configs import viscous_plume
+    s = rn.build_sim_setup(viscous_plume(*size)[0])
+    ref = run_oracle(oracle, s, 40).readAll()
+    first = None
+    for tile in solver.TILES:
+        g = rn.GPUSolver(s.Nx, s.Nr)
+        g.setPrecision("exact")
+        g.setTile(tile)
+        g.setGeometry(s.geo)
+        init = s.initialState()
+        g.setState(init["A"], init["B"])
+        g.step(40, s.P)
+        out = g.readAll()
+        g.close()
+        if first is None:
+            first = out
+            assert_state_close(out, ref, 1e-6)
+        assert np.array_equal(out["A"], first["A"]) and np.array_equal(out["B"], first["B"]), tile
+
+
+def test_largest_bench_grid_against_oracle(rn, oracle):
+    """The 4096 x 1536 plain grid of the HBM-resident bench point (6.3 M
+    cells): 15 steps against the oracle."""
+    from rocket_nozzle_cfd_solver_b200.configs import plain_small
+    s = rn.build_sim_setup(plain_small(4096, 1536)[0])
+    compare(rn, oracle, s, 15, "fast")
