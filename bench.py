@@ -579,7 +579,8 @@ def serving_requests(rn, count, seed=7, spray_frac=0.2):
         if rng.uniform() < spray_frac:
             Nx, Nr = configs.BATCH_SIZES[int(rng.integers(len(configs.BATCH_SIZES)))]
             s = rn.build_sim_setup(configs.injector_spray(Nx, Nr)[0])
-            npar = int(rng.integers(16384, 65537))
+            # the parcel count has its own stream, so the request mix is that of rng alone
+            npar = int(np.random.default_rng(seed * 1000 + q).integers(16384, 65537))
             out.append(("spray", s, configs.prepopulated_parcels(s, npar, seed=20261203 + q)))
         else:
             out.append(("nozzle", rn.build_sim_setup(configs.batched_instance(rng)), None))
