@@ -3,9 +3,10 @@
 // Every function states the reference shader lines it computes
 // (source/solver.js, source/spray.js). The kernels in rn_step.cu fuse these
 // into tiles; the arithmetic and its operation order are the reference's, so
-// that with multiply-add contraction off (-fmad=false) the fused kernels give
-// the same float32 results as the pass-by-pass restatement wherever the math
-// library functions (pow, exp, log, sin, cos) agree.
+// that in the exact variant (IEEE division and square root, multiply-add
+// contraction off) the fused kernels give the same float32 results as the
+// pass-by-pass restatement wherever the math library functions (pow, exp, log,
+// sin, cos) agree.
 // GLSL max/min are IEEE maxNum/minNum (fmaxf/fminf), what NVIDIA GPUs execute.
 #pragma once
 #include <cuda_runtime.h>
@@ -30,10 +31,23 @@ struct Grid {
 struct Prim { float4 w, s; };        // w = (rho, u, v, p), s = (Z, F, G, O)   solver.js:29
 struct Flux { float4 F, Y; float O; };   // face flux: F(4), (FZ, FF, u_f G_f, u_f), FO
 
+// Division of the time-step arithmetic. The fast variant (RN_FAST_DIV) takes
+// the hardware's reciprocal-based quotient (div.approx, within 2 ulp for
+// divisors of magnitude 2^-126 .. 2^126, which every divisor here is: densities,
+// pressures, wave speeds, face areas and volumes, all floored well above
+// 2^-126 and far below 2^126); the exact variant divides as IEEE does.
+RN_DEV float fdiv(float a, float b) {
+#ifdef RN_FAST_DIV
+  return __fdividef(a, b);
+#else
+  return a / b;
+#endif
+}
+
 RN_DEV float clampf(float x, float a, float b) { return fminf(fmaxf(x, a), b); }
 RN_DEV float mixf(float x, float y, float a) { return x * (1.0f - a) + y * a; }
 RN_DEV float smoothstepf(float e0, float e1, float x) {
-  float t = clampf((x - e0) / (e1 - e0), 0.0f, 1.0f);
+  float t = clampf(fdiv(x - e0, e1 - e0), 0.0f, 1.0f);
   return t * t * (3.0f - 2.0f * t);
 }
 RN_DEV float len2(float a, float b) { return sqrtf(a * a + b * b); }
@@ -45,15 +59,16 @@ RN_DEV bool solid_at(const Grid& g, int i, int j) { return g.mask[j * g.Nx + i] 
 RN_DEV Prim to_prim(float4 a, float4 b) {
   Prim q;
   float rho = fmaxf(a.x, RHO_MIN);
-  float vx = a.y / rho, vy = a.z / rho;
+  float vx = fdiv(a.y, rho), vy = fdiv(a.z, rho);
   float G = fmaxf(b.z, 0.5f);
-  float p = fmaxf((a.w - 0.5f * rho * (vx * vx + vy * vy)) / G, P_MIN);
+  float p = fmaxf(fdiv(a.w - 0.5f * rho * (vx * vx + vy * vy), G), P_MIN);
   q.w = make_float4(rho, vx, vy, p);
-  q.s = make_float4(clampf(b.x / rho, 0.0f, 1.0f), clampf(b.y / rho, 0.0f, 1.0f), G, clampf(b.w / rho, 0.0f, 1.0f));
+  q.s = make_float4(clampf(fdiv(b.x, rho), 0.0f, 1.0f), clampf(fdiv(b.y, rho), 0.0f, 1.0f), G,
+                    clampf(fdiv(b.w, rho), 0.0f, 1.0f));
   return q;
 }
 // soundSpeed (solver.js:40)
-RN_DEV float sound_speed(const Prim& q) { return sqrtf((1.0f + 1.0f / q.s.z) * q.w.w / q.w.x); }
+RN_DEV float sound_speed(const Prim& q) { return sqrtf(fdiv((1.0f + fdiv(1.0f, q.s.z)) * q.w.w, q.w.x)); }
 
 // CFL wave speed of one fluid cell (FS_REDUCE1, solver.js:376-379)
 RN_DEV float wave_speed(float4 a, float4 b) {
@@ -146,9 +161,9 @@ RN_DEV void interior_prim(const Grid& g, const float4* __restrict__ A, const flo
 RN_DEV float van_leer(float a, float b) {
   float ab = a * b, den = a + b;
   den = mixf(den, 1.0f, (1e-30f < fabsf(den)) ? 0.0f : 1.0f);   // step(abs(den), 1e-30)
-  return ab > 0.0f ? 2.0f * ab / den : copysignf(0.0f, den);
+  return ab > 0.0f ? fdiv(2.0f * ab, den) : copysignf(0.0f, den);
 }
-RN_DEV float jump_ratio(float a, float b) { return fabsf(a - b) / fminf(a, b); }
+RN_DEV float jump_ratio(float a, float b) { return fdiv(fabsf(a - b), fminf(a, b)); }
 
 // DIR_R selects the r-direction (normal velocity in .z); one instance of the
 // code serves both directions.
@@ -215,15 +230,15 @@ RN_DEV Flux face_flux(bool DIR_R, float area, float4 w0, float4 b0, float4 w1, f
   float GL = WLs.z, GR = WRs.z;
   float rL = WLw.x, uL = WLw.y, vL = WLw.z, pL = WLw.w;
   float rR = WRw.x, uR = WRw.y, vR = WRw.z, pR = WRw.w;
-  float cL = sqrtf((1.0f + 1.0f / GL) * pL / rL), cR = sqrtf((1.0f + 1.0f / GR) * pR / rR);
+  float cL = sqrtf(fdiv((1.0f + fdiv(1.0f, GL)) * pL, rL)), cR = sqrtf(fdiv((1.0f + fdiv(1.0f, GR)) * pR, rR));
   float EL = pL * GL + 0.5f * rL * (uL * uL + vL * vL);
   float ER = pR * GR + 0.5f * rR * (uR * uR + vR * vR);
   float sL = sqrtf(rL), sR = sqrtf(rR);
-  float uT = (sL * uL + sR * uR) / (sL + sR);
-  float HT = (sL * (EL + pL) / rL + sR * (ER + pR) / rR) / (sL + sR);
-  float vT = (sL * vL + sR * vR) / (sL + sR);
-  float GT = (sL * GL + sR * GR) / (sL + sR);
-  float cT = sqrtf(fmaxf((HT - 0.5f * (uT * uT + vT * vT)) / GT, 1e-12f));
+  float uT = fdiv(sL * uL + sR * uR, sL + sR);
+  float HT = fdiv(fdiv(sL * (EL + pL), rL) + fdiv(sR * (ER + pR), rR), sL + sR);
+  float vT = fdiv(sL * vL + sR * vR, sL + sR);
+  float GT = fdiv(sL * GL + sR * GR, sL + sR);
+  float cT = sqrtf(fmaxf(fdiv(HT - 0.5f * (uT * uT + vT * vT), GT), 1e-12f));
   float SL = fminf(uL - cL, uT - cT);
   float SR = fmaxf(uR + cR, uT + cT);
   float mL = rL * uL, mR = rR * uR;
@@ -235,7 +250,7 @@ RN_DEV Flux face_flux(bool DIR_R, float area, float4 w0, float4 b0, float4 w1, f
   if (SL >= 0.0f) { F0 = FL0; F1 = FL1; F2 = FL2; F3 = FL3; Y0 = YL0; Y1 = YL1; Y2 = YL2; uf = uL; Gf = GL; }
   else if (SR <= 0.0f) { F0 = FR0; F1 = FR1; F2 = FR2; F3 = FR3; Y0 = YR0; Y1 = YR1; Y2 = YR2; uf = uR; Gf = GR; }
   else {
-    float Ss = (pR - pL + mL * (SL - uL) - mR * (SR - uR)) / (rL * (SL - uL) - rR * (SR - uR));
+    float Ss = fdiv(pR - pL + mL * (SL - uL) - mR * (SR - uR), rL * (SL - uL) - rR * (SR - uR));
     bool left = Ss >= 0.0f;
     float rK = left ? rL : rR, uK = left ? uL : uR, vK = left ? vL : vR, pK = left ? pL : pR;
     float EK = left ? EL : ER, SK = left ? SL : SR;
@@ -243,13 +258,13 @@ RN_DEV Flux face_flux(bool DIR_R, float area, float4 w0, float4 b0, float4 w1, f
     float FK0 = left ? FL0 : FR0, FK1 = left ? FL1 : FR1, FK2 = left ? FL2 : FR2, FK3 = left ? FL3 : FR3;
     float FYK0 = left ? YL0 : YR0, FYK1 = left ? YL1 : YR1, FYK2 = left ? YL2 : YR2;
     float UK1 = left ? mL : mR, UK2 = rK * vK;
-    float kk = rK * (SK - uK) / (SK - Ss);
-    float Us0 = kk * 1.0f, Us1 = kk * Ss, Us2 = kk * vK, Us3 = kk * (EK / rK + (Ss - uK) * (Ss + pK / (rK * (SK - uK))));
+    float kk = fdiv(rK * (SK - uK), SK - Ss);
+    float Us0 = kk * 1.0f, Us1 = kk * Ss, Us2 = kk * vK, Us3 = kk * (fdiv(EK, rK) + (Ss - uK) * (Ss + fdiv(pK, rK * (SK - uK))));
     float C0 = FK0 + SK * (Us0 - rK), C1 = FK1 + SK * (Us1 - UK1), C2 = FK2 + SK * (Us2 - UK2), C3 = FK3 + SK * (Us3 - EK);
     float CY0 = FYK0 + SK * (kk * YK0 - rK * YK0), CY1 = FYK1 + SK * (kk * YK1 - rK * YK1);
     float CY2 = FYK2 + SK * (kk * YK2 - rK * YK2);
     if (hllw != 0.0f) {
-      float inv = 1.0f / (SR - SL);
+      float inv = fdiv(1.0f, SR - SL);
       float SLR = SL * SR;
       float H0 = (SR * FL0 - SL * FR0 + SLR * (rR - rL)) * inv;
       float H1 = (SR * FL1 - SL * FR1 + SLR * (mR - mL)) * inv;
@@ -266,7 +281,7 @@ RN_DEV Flux face_flux(bool DIR_R, float area, float4 w0, float4 b0, float4 w1, f
       F0 = C0; F1 = C1; F2 = C2; F3 = C3;
       Y0 = CY0; Y1 = CY1; Y2 = CY2;
     }
-    uf = uK + SK * ((SK - uK) / (SK - Ss) - 1.0f);
+    uf = uK + SK * (fdiv(SK - uK, SK - Ss) - 1.0f);
     Gf = left ? GL : GR;
   }
   if (DIR_R) { float t = F1; F1 = F2; F2 = t; }    // rotate momentum back to (x, r)
@@ -278,13 +293,13 @@ RN_DEV Flux face_flux(bool DIR_R, float area, float4 w0, float4 b0, float4 w1, f
 
 // wallPressure (solver.js:301-306): slip-wall pressure from the reflected Riemann problem
 RN_DEV float wall_pressure(const Prim& q, float un) {
-  float g = 1.0f + 1.0f / q.s.z, p = q.w.w, rho = q.w.x, c = sqrtf(g * p / rho);
+  float g = 1.0f + fdiv(1.0f, q.s.z), p = q.w.w, rho = q.w.x, c = sqrtf(fdiv(g * p, rho));
   if (un > 0.0f) {
     float a = 0.25f * (g + 1.0f) * un;
     return p + rho * un * (a + sqrtf(a * a + c * c));
   }
-  float f = fmaxf(1.0f + 0.5f * (g - 1.0f) * un / c, 0.0f);
-  return p * powf(f, 2.0f * g / (g - 1.0f));
+  float f = fmaxf(1.0f + fdiv(0.5f * (g - 1.0f) * un, c), 0.0f);
+  return p * powf(f, fdiv(2.0f * g, g - 1.0f));
 }
 
 // member flux accumulation of one group member (memberFlux, solver.js:287-299)
@@ -296,7 +311,7 @@ RN_DEV void sub4(float4& L, float ae, float4 fe, float aw, float4 fw) {
 }
 
 // GLSL_GAS (solver.js:445-450)
-RN_DEV float sutherland(float TK, const rn_params& P) { return P.gas[3] * 1.458e-6f * TK * sqrtf(TK) / (TK + 110.4f); }
+RN_DEV float sutherland(float TK, const rn_params& P) { return fdiv(P.gas[3] * 1.458e-6f * TK * sqrtf(TK), TK + 110.4f); }
 RN_DEV float rmix(float4 s, const rn_params& P) {
   return (1.0f - s.x) * P.gas[0] + s.y * P.Rs[0] + s.w * P.Rs[1] + fmaxf(s.x - s.y - s.w, 0.0f) * P.Rs[2];
 }
@@ -310,23 +325,23 @@ RN_DEV void vcell(float4 w0, float4 sc, float4 wE, float4 wW, float4 wN, float4 
   float fE = wE.x < 0.0f ? 0.0f : 1.0f, fW = wW.x < 0.0f ? 0.0f : 1.0f;
   float fN = wN.x < 0.0f ? 0.0f : 1.0f, fS = wS.x < 0.0f ? 0.0f : 1.0f;
   float dxn = fmaxf(fE + fW, 1.0f), drn = fmaxf(fN + fS, 1.0f);
-  float ux = (fE * (wE.y - w0.y) + fW * (w0.y - wW.y)) / dxn;
-  float vx = (fE * (wE.z - w0.z) + fW * (w0.z - wW.z)) / dxn;
-  float ur = (fN * (wN.y - w0.y) + fS * (w0.y - wS.y)) / drn;
-  float vr = (fN * (wN.z - w0.z) + fS * (w0.z - wS.z)) / drn;
-  float r = float(j) + 0.5f, vor = w0.z / r;
+  float ux = fdiv(fE * (wE.y - w0.y) + fW * (w0.y - wW.y), dxn);
+  float vx = fdiv(fE * (wE.z - w0.z) + fW * (w0.z - wW.z), dxn);
+  float ur = fdiv(fN * (wN.y - w0.y) + fS * (w0.y - wS.y), drn);
+  float vr = fdiv(fN * (wN.z - w0.z) + fS * (w0.z - wS.z), drn);
+  float r = float(j) + 0.5f, vor = fdiv(w0.z, r);
   float div = ux + vr + vor;
   float S2 = 2.0f * (ux * ux + vr * vr + vor * vor) + (ur + vx) * (ur + vx) - 0.6666667f * div * div;
   float om = vx - ur;
-  float sens = om * om / (om * om + div * div + 1e-8f);
+  float sens = fdiv(om * om, om * om + div * div + 1e-8f);
   float Smag = sqrtf(fmaxf(S2, 0.0f)) * sens;
   float rho = w0.x, p = w0.w;
   float Rm = rmix(sc, P);
-  float mu = sutherland(p / (rho * Rm) * P.gas[2], P);
+  float mu = sutherland(fdiv(p, rho * Rm) * P.gas[2], P);
   float mut = rho * l * l * Smag;
   if (float(i) < P.chamberNu[1]) mut = fmaxf(mut, rho * P.chamberNu[0]);
   T1 = make_float4(ux, ur, vx, vr);
-  T2 = make_float4(fminf(mu + mut, 0.08f * rho / fmaxf(dt, 1e-9f)), (sc.z + 1.0f) * p / rho, Smag, mu);
+  T2 = make_float4(fminf(mu + mut, fdiv(0.08f * rho, fmaxf(dt, 1e-9f))), fdiv((sc.z + 1.0f) * p, rho), Smag, mu);
 }
 
 // makeViscFluxShader (solver.js:499-536) for one face; returns false for a
@@ -340,7 +355,7 @@ RN_DEV void visc_flux(bool DIR_R, float4 w1, float4 s1, float4 t1, float4 m1, fl
   float r, ux, vx, ur, vr;
   if (DIR_R) { r = fmaxf(float(j), 0.5f); ux = ttx; vx = ttz; ur = w2.y - w1.y; vr = w2.z - w1.z; }
   else { r = float(j) + 0.5f; ux = w2.y - w1.y; vx = w2.z - w1.z; ur = tty; vr = ttw; }
-  float div = ux + vr + vf / r;
+  float div = ux + vr + fdiv(vf, r);
   float txr = mu * (ur + vx);
   float k = mu * 1.25f;
   if (DIR_R) {

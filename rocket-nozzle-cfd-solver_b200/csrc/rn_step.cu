@@ -268,13 +268,13 @@ __device__ __forceinline__ bool update_cell(const StageArgs& a, const rn_params&
   // embedded wall: pressure force along the r-weighted wall vector
   float wl = len2(gg.z, gg.w);
   if (wl > 1e-6f) {
-    float nx = gg.z / wl, nr = gg.w / wl;
+    float nx = fdiv(gg.z, wl), nr = fdiv(gg.w, wl);
     float pw = wall_pressure(q, q.w.y * nx + q.w.z * nr);
     L.y -= gg.z * pw;
     L.z -= gg.w * pw;
   }
   L.z += q.w.w * gg.y;                       // axisymmetric source p Am
-  float invV = 1.0f / fmaxf(gg.x, 1e-6f);
+  float invV = fdiv(1.0f, fmaxf(gg.x, 1e-6f));
   float4 LB = make_float4(LY.x, LY.y, LY.z - q.s.z * LY.w, LO);
   float f = dt * invV;
   float4 U, UY;
@@ -290,9 +290,9 @@ __device__ __forceinline__ bool update_cell(const StageArgs& a, const rn_params&
   }
   float rho = fmaxf(U.x, RHO_MIN);
   float den = fmaxf(U.x, RHO_MIN);
-  float vx = U.y / den, vy = U.z / den;
+  float vx = fdiv(U.y, den), vy = fdiv(U.z, den);
   float sp = len2(vx, vy);
-  if (sp > P.vMax) { float s = P.vMax / sp; vx *= s; vy *= s; }
+  if (sp > P.vMax) { float s = fdiv(P.vMax, sp); vx *= s; vy *= s; }
   if (!(rho < 1e30f) || !(vx < 1e30f && vx > -1e30f)) {   // NaN guard
     oA = make_float4(P.ambCons[0], P.ambCons[1], P.ambCons[2], P.ambCons[3]);
     oB = make_float4(P.ambB[0], P.ambB[1], P.ambB[2], P.ambB[3]);
@@ -475,7 +475,7 @@ __device__ __forceinline__ bool source_cell(const Grid& g, const float4* __restr
   float rho = q.w.x, p = q.w.w, G = q.s.z;
   float velx = q.w.y, vely = q.w.z;
   float V = fmaxf(gg.x, 1e-6f);
-  float Rm = rmix(q.s, P), Tg = p / (rho * Rm);
+  float Rm = rmix(q.s, P), Tg = fdiv(p, rho * Rm);
   float4 L = make_float4(0.f, 0.f, 0.f, 0.f), LY = L;
   const int vh = (Hy - y0 + 1) * TW + (Hx - x0 + 1);
   float4 T1h = sT1[vh], T2h = sT2[vh];
@@ -496,34 +496,34 @@ __device__ __forceinline__ bool source_cell(const Grid& g, const float4* __restr
       sub4(LY, an, sY[fn], as_, sY[fs]);
     }
     // axisymmetric hoop stress
-    float r = V / fmaxf(gg.y, 1e-6f), vor = vely / r;
+    float r = fdiv(V, fmaxf(gg.y, 1e-6f)), vor = fdiv(vely, r);
     L.z -= T2h.x * (2.0f * vor - 0.6666667f * (T1h.x + T1h.w + vor)) * gg.y;
     // Werner-Wengle wall shear and Reynolds-analogy heat flux
     float wl = len2(gg.z, gg.w);
     if (wl > 1e-6f) {
-      float nx = gg.z / wl, nr = gg.w / wl;
+      float nx = fdiv(gg.z, wl), nr = fdiv(gg.w, wl);
       float dn = velx * nx + vely * nr;
       float utx = velx - dn * nx, uty = vely - dn * nr;
       float up = len2(utx, uty);
       float cp = Rm * (G + 1.0f);
-      float Taw = Tg + 0.89f * up * up / (2.0f * cp);
+      float Taw = Tg + fdiv(0.89f * up * up, 2.0f * cp);
       float Ts = fmaxf(Tg + 0.5f * (P.Tw - Tg) + 0.22f * (Taw - Tg), 1e-3f);
-      float rs = p / (Rm * Ts), mus = sutherland(Ts * P.gas[2], P);
-      float dz = 2.0f * clampf(0.5f * V / wl, 0.25f, 1.0f);
-      float nz = mus / (rs * dz);
-      float tw = up <= 69.7f * nz ? 2.0f * mus * up / dz
+      float rs = fdiv(p, Rm * Ts), mus = sutherland(Ts * P.gas[2], P);
+      float dz = 2.0f * clampf(fdiv(0.5f * V, wl), 0.25f, 1.0f);
+      float nz = fdiv(mus, rs * dz);
+      float tw = up <= 69.7f * nz ? fdiv(2.0f * mus * up, dz)
                                   : rs * powf(7.187f * powf(nz, 1.142857f) + 0.13769f * powf(nz, 0.142857f) * up, 1.75f);
-      tw = fminf(tw, 0.3f * rho * up * V / fmaxf(wl * dt, 1e-9f));
-      if (up > 1e-6f) { L.y -= tw * wl * utx / up; L.z -= tw * wl * uty / up; }
-      float qw = tw / fmaxf(up, 1e-4f) * cp * (Taw - P.Tw) * 1.24f;
-      float qmax = 0.3f * p * G * V / fmaxf(wl * dt, 1e-9f);
+      tw = fminf(tw, fdiv(0.3f * rho * up * V, fmaxf(wl * dt, 1e-9f)));
+      if (up > 1e-6f) { L.y -= fdiv(tw * wl * utx, up); L.z -= fdiv(tw * wl * uty, up); }
+      float qw = fdiv(tw, fmaxf(up, 1e-4f)) * cp * (Taw - P.Tw) * 1.24f;
+      float qmax = fdiv(0.3f * p * G * V, fmaxf(wl * dt, 1e-9f));
       L.w -= clampf(qw, -qmax, qmax) * wl;
     }
     // shock / boundary-layer interaction on the bit-16 band
     if (sm_ & 16) {
-      float up = len2(velx, vely), Mn = up / sqrtf((1.0f + 1.0f / G) * p / rho);
+      float up = len2(velx, vely), Mn = fdiv(up, sqrtf(fdiv((1.0f + fdiv(1.0f, G)) * p, rho)));
       if (Mn > 1.0f) {
-        float shx = velx / up, shy = vely / up;
+        float shx = fdiv(velx, up), shy = fdiv(vely, up);
         float pd = 0.0f;
         for (int n = 4; n <= 6; n += 2)
           for (int mm = 0; mm <= 1; mm++) {
@@ -536,7 +536,7 @@ __device__ __forceinline__ bool source_cell(const Grid& g, const float4* __restr
             if (wd.x > 0.0f) pd = fmaxf(pd, wd.w);
           }
         float crit = 1.0f + 0.5f * Mn;
-        float fsep = smoothstepf(crit, 1.2f * crit, pd / p) * V * rho * up;
+        float fsep = smoothstepf(crit, 1.2f * crit, fdiv(pd, p)) * V * rho * up;
         L.y -= fsep * velx;
         L.z -= fsep * vely;
       } else if (velx > 0.0f && p < 1.3f * P.chemK[3]) {
@@ -546,11 +546,11 @@ __device__ __forceinline__ bool source_cell(const Grid& g, const float4* __restr
       }
     }
   }
-  float invV = dt / V;
+  float invV = fdiv(dt, V);
   float dO = invV * L.x;
   L.x = 0.0f;
   float4 U = make_float4(A.x + invV * L.x, A.y + invV * L.y, A.z + invV * L.z, A.w + invV * L.w);
-  float4 UY = make_float4(B.x + invV * LY.x / 1.0f, B.y + invV * LY.y / 1.0f, B.z + invV * LY.z / rho,
+  float4 UY = make_float4(B.x + invV * LY.x / 1.0f, B.y + invV * LY.y / 1.0f, B.z + fdiv(invV * LY.z, rho),
                           B.w + invV * 0.0f / 1.0f);
   if (P.inj) UY.w += dO;
   if (P.chem) {
@@ -568,7 +568,7 @@ __device__ __forceinline__ bool source_cell(const Grid& g, const float4* __restr
     }
   }
   float rn = fmaxf(U.x, RHO_MIN);
-  float vnx = U.y / rn, vny = U.z / rn;
+  float vnx = fdiv(U.y, rn), vny = fdiv(U.z, rn);
   if (!(rn < 1e30f) || !(vnx < 1e30f && vnx > -1e30f)) {
     oA = make_float4(P.ambCons[0], P.ambCons[1], P.ambCons[2], P.ambCons[3]);
     oB = make_float4(P.ambB[0], P.ambB[1], P.ambB[2], P.ambB[3]);
