@@ -189,10 +189,14 @@ def run_ours(args, rank, world, local_rank):
     setup = make_setup(rn)
     cells = setup.Nx * setup.Nr
     g = rn.GPUSolver(setup.Nx, setup.Nr)
+    if args.tile:
+        g.setTile(args.tile)
     g.setGeometry(setup.geo)
     init = setup.initialState()
     g.setState(init["A"], init["B"])
     params = rn.params_from_P(setup.P)
+    # tile shape: the autotuner's pick (timed on this state, which it restores)
+    tile_name = g.tile if args.tile else g.autotune(params, steps=100)
     stream = torch.cuda.ExternalStream(g.stream())
     flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=f"cuda:{local_rank}")
 
@@ -242,13 +246,16 @@ def run_ours(args, rank, world, local_rank):
     achieved = bpc * cells / (avg_ms * 1e-3) / 1e9 if bpc else None
     traffic_pc = profiled_traffic(kind)
     total_ms = sum(v[0] for v in prof.values())
+    resident_mb = cells * (3 * 32 + 49) / 1e6      # state ring + geometry
     roofline = {"bound": "hbm", "kernel": kind, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak if achieved else None, "peak_source": peak_kind,
                 "bytes_per_launch": bpc * cells if bpc else None, "avg_launch_us": avg_ms * 1e3,
                 "traffic": traffic_pc * cells if traffic_pc else None,
                 "share": {k: round(v[0] / total_ms, 4) for k, v in prof.items() if v[1] > 0},
-                "l2_note": "512x192 state + geometry (~14 MB) fits in the 126 MB L2: within a bench step the "
-                           "kernels run mostly from L2, so achieved can exceed the HBM copy bandwidth"}
+                "l2_note": (f"{setup.Nx}x{setup.Nr} state + geometry (~{resident_mb:.0f} MB) fits in the 126 MB L2: "
+                            "within a bench step the kernels run mostly from L2, so achieved can exceed the HBM "
+                            "copy bandwidth") if resident_mb < 126 else
+                           f"{setup.Nx}x{setup.Nr} state + geometry (~{resident_mb:.0f} MB) exceeds the 126 MB L2"}
 
     # ---- steady state: back-to-back steps, no flush (for reference)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -319,7 +326,8 @@ def run_ours(args, rank, world, local_rank):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "grid": [setup.Nx, setup.Nr], "cells": cells,
                        "solver_steps_per_bench_step": SOLVER_STEPS, "l2": "flushed before every bench step",
-                       "parallelism": f"replicas x{world}", "physics": "viscous+wall model+afterburning"},
+                       "parallelism": f"replicas x{world}", "physics": "viscous+wall model+afterburning",
+                       "tile": tile_name},
             "roofline": roofline, "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "exit_thrust_N": perf["F"] if perf else None},
@@ -446,6 +454,7 @@ def run_large_grid(args):
     init = s.initialState()
     g.setState(init["A"], init["B"])
     p = rn.params_from_P(s.P)
+    tile = g.autotune(p, steps=10)
     stream = torch.cuda.ExternalStream(g.stream())
     n = 20
     for _ in range(max(args.warmup, 1)):
@@ -477,7 +486,7 @@ def run_large_grid(args):
     return {"workload": "plain cold-gas nozzle 4096x1536 (inviscid, 2 kernels per step)", "cells": cells,
             "value": rate, "unit": "cell-updates/s", "bytes_per_cell_step": bpc,
             "achieved_gbs": rate * bpc / 1e9, "peak_gbs": peak, "peak_source": src,
-            "frac": rate * bpc / 1e9 / peak, "kernels": kern}
+            "frac": rate * bpc / 1e9 / peak, "kernels": kern, "tile": tile}
 
 
 def run_spray(args, local_rank):
@@ -658,6 +667,7 @@ def main():
                     help="grid of the main viscous-plume leg (other sizes are for profiling; the bench line's "
                          "workload is 512x192)")
     ap.add_argument("--solver-steps", type=int, default=SOLVER_STEPS, help="time steps per bench step")
+    ap.add_argument("--tile", default=None, help="tile shape of the main leg (default: the library's)")
     ap.add_argument("--no-large", action="store_true",
                     help="skip the 4096x1536 HBM-resident sweep point and the spray chamber leg")
     ap.add_argument("--only-spray", action="store_true",

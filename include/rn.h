@@ -180,7 +180,7 @@ int rn_set_precision(rn_handle h, int mode);
 int rn_get_precision(rn_handle h, int* mode);
 
 /* Tile shape of the stage/physics kernels (a thread per cell):
- * RN_TILE_16x15 (default), RN_TILE_16x16, RN_TILE_16x8 or RN_TILE_32x15. rn_autotune times `steps` steps
+ * RN_TILE_16x15 (default), RN_TILE_16x16, RN_TILE_16x8, RN_TILE_32x15 or RN_TILE_14x16. rn_autotune times `steps` steps
  * with each shape on a copy of the handle's current state (the state, step
  * info and spray ring are restored afterwards), keeps the fastest and returns
  * it in *chosen. No reference counterpart (the reference draws full-screen
@@ -189,6 +189,7 @@ int rn_get_precision(rn_handle h, int* mode);
 #define RN_TILE_16x8 1
 #define RN_TILE_16x15 2   /* 16 x 15 cells on 256 threads */
 #define RN_TILE_32x15 3   /* 32 x 15 cells on 512 threads */
+#define RN_TILE_14x16 4   /* 14 x 16 cells on 256 threads */
 int rn_set_tile(rn_handle h, int shape);
 int rn_get_tile(rn_handle h, int* shape);
 int rn_autotune(rn_handle h, const rn_params* P, int steps, int* chosen);

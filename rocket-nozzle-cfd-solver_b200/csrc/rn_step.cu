@@ -61,7 +61,9 @@ using Tile0 = TileT<TILE_TX[0], TILE_TY[0], TILE_NT[0]>;
 using Tile1 = TileT<TILE_TX[1], TILE_TY[1], TILE_NT[1]>;
 using Tile2 = TileT<TILE_TX[2], TILE_TY[2], TILE_NT[2]>;
 using Tile3 = TileT<TILE_TX[3], TILE_TY[3], TILE_NT[3]>;
-static_assert(Tile0::NC <= Tile0::NT && Tile1::NC <= Tile1::NT && Tile2::NC <= Tile2::NT && Tile3::NC <= Tile3::NT,
+using Tile4 = TileT<TILE_TX[4], TILE_TY[4], TILE_NT[4]>;
+static_assert(Tile0::NC <= Tile0::NT && Tile1::NC <= Tile1::NT && Tile2::NC <= Tile2::NT && Tile3::NC <= Tile3::NT &&
+                  Tile4::NC <= Tile4::NT,
               "a thread per cell");
 
 // --------------------------------------------------------------------------
@@ -936,19 +938,22 @@ static int init_tile() {
 // Raises the dynamic shared-memory limits of the stage and physics kernels to
 // what a member list of MAXX cells needs (process-wide function attributes).
 int stage_kernels_init() {
-  return (init_tile<Tile0>() == 0 && init_tile<Tile1>() == 0 && init_tile<Tile2>() == 0 && init_tile<Tile3>() == 0)
+  return (init_tile<Tile0>() == 0 && init_tile<Tile1>() == 0 && init_tile<Tile2>() == 0 && init_tile<Tile3>() == 0 &&
+          init_tile<Tile4>() == 0)
              ? 0
              : -1;
 }
 
 void launch_stage1(const StageArgs& a, const rn_params& P, int tile, cudaStream_t s) {
-  if (tile == 3) k_stage<Tile3, 1><<<tiles_of<Tile3>(a.g), Tile3::NT, stage_smem_t<Tile3>(a.maxX), s>>>(a, P);
+  if (tile == 4) k_stage<Tile4, 1><<<tiles_of<Tile4>(a.g), Tile4::NT, stage_smem_t<Tile4>(a.maxX), s>>>(a, P);
+  else if (tile == 3) k_stage<Tile3, 1><<<tiles_of<Tile3>(a.g), Tile3::NT, stage_smem_t<Tile3>(a.maxX), s>>>(a, P);
   else if (tile == 2) k_stage<Tile2, 1><<<tiles_of<Tile2>(a.g), Tile2::NT, stage_smem_t<Tile2>(a.maxX), s>>>(a, P);
   else if (tile == 1) k_stage<Tile1, 1><<<tiles_of<Tile1>(a.g), Tile1::NT, stage_smem_t<Tile1>(a.maxX), s>>>(a, P);
   else k_stage<Tile0, 1><<<tiles_of<Tile0>(a.g), Tile0::NT, stage_smem_t<Tile0>(a.maxX), s>>>(a, P);
 }
 void launch_stage2(const StageArgs& a, const rn_params& P, int tile, cudaStream_t s) {
-  if (tile == 3) k_stage<Tile3, 2><<<tiles_of<Tile3>(a.g), Tile3::NT, stage_smem_t<Tile3>(a.maxX), s>>>(a, P);
+  if (tile == 4) k_stage<Tile4, 2><<<tiles_of<Tile4>(a.g), Tile4::NT, stage_smem_t<Tile4>(a.maxX), s>>>(a, P);
+  else if (tile == 3) k_stage<Tile3, 2><<<tiles_of<Tile3>(a.g), Tile3::NT, stage_smem_t<Tile3>(a.maxX), s>>>(a, P);
   else if (tile == 2) k_stage<Tile2, 2><<<tiles_of<Tile2>(a.g), Tile2::NT, stage_smem_t<Tile2>(a.maxX), s>>>(a, P);
   else if (tile == 1) k_stage<Tile1, 2><<<tiles_of<Tile1>(a.g), Tile1::NT, stage_smem_t<Tile1>(a.maxX), s>>>(a, P);
   else k_stage<Tile0, 2><<<tiles_of<Tile0>(a.g), Tile0::NT, stage_smem_t<Tile0>(a.maxX), s>>>(a, P);
@@ -970,19 +975,22 @@ static void stage2phys_t(const StageArgs& a, const PhysArgs& p, const rn_params&
 }
 void launch_stage2phys(const StageArgs& a, const PhysArgs& p, const rn_params& P, int tile, const int* heavy,
                        int nHeavy, bool skip, cudaStream_t s) {
-  if (tile == 3) stage2phys_t<Tile3>(a, p, P, heavy, nHeavy, skip, s);
+  if (tile == 4) stage2phys_t<Tile4>(a, p, P, heavy, nHeavy, skip, s);
+  else if (tile == 3) stage2phys_t<Tile3>(a, p, P, heavy, nHeavy, skip, s);
   else if (tile == 2) stage2phys_t<Tile2>(a, p, P, heavy, nHeavy, skip, s);
   else if (tile == 1) stage2phys_t<Tile1>(a, p, P, heavy, nHeavy, skip, s);
   else stage2phys_t<Tile0>(a, p, P, heavy, nHeavy, skip, s);
 }
 void launch_batch_stage1(const BatchInst* d, const int* bi, int nb, BatchPhase ph, int tile, cudaStream_t s) {
-  if (tile == 3) k_stage_batch<Tile3, 1><<<nb, Tile3::NT, stage_smem_t<Tile3>(ph.maxX), s>>>(d, bi, ph);
+  if (tile == 4) k_stage_batch<Tile4, 1><<<nb, Tile4::NT, stage_smem_t<Tile4>(ph.maxX), s>>>(d, bi, ph);
+  else if (tile == 3) k_stage_batch<Tile3, 1><<<nb, Tile3::NT, stage_smem_t<Tile3>(ph.maxX), s>>>(d, bi, ph);
   else if (tile == 2) k_stage_batch<Tile2, 1><<<nb, Tile2::NT, stage_smem_t<Tile2>(ph.maxX), s>>>(d, bi, ph);
   else if (tile == 1) k_stage_batch<Tile1, 1><<<nb, Tile1::NT, stage_smem_t<Tile1>(ph.maxX), s>>>(d, bi, ph);
   else k_stage_batch<Tile0, 1><<<nb, Tile0::NT, stage_smem_t<Tile0>(ph.maxX), s>>>(d, bi, ph);
 }
 void launch_batch_stage2(const BatchInst* d, const int* bi, int nb, BatchPhase ph, int tile, cudaStream_t s) {
-  if (tile == 3) k_stage_batch<Tile3, 2><<<nb, Tile3::NT, stage_smem_t<Tile3>(ph.maxX), s>>>(d, bi, ph);
+  if (tile == 4) k_stage_batch<Tile4, 2><<<nb, Tile4::NT, stage_smem_t<Tile4>(ph.maxX), s>>>(d, bi, ph);
+  else if (tile == 3) k_stage_batch<Tile3, 2><<<nb, Tile3::NT, stage_smem_t<Tile3>(ph.maxX), s>>>(d, bi, ph);
   else if (tile == 2) k_stage_batch<Tile2, 2><<<nb, Tile2::NT, stage_smem_t<Tile2>(ph.maxX), s>>>(d, bi, ph);
   else if (tile == 1) k_stage_batch<Tile1, 2><<<nb, Tile1::NT, stage_smem_t<Tile1>(ph.maxX), s>>>(d, bi, ph);
   else k_stage_batch<Tile0, 2><<<nb, Tile0::NT, stage_smem_t<Tile0>(ph.maxX), s>>>(d, bi, ph);
@@ -1002,7 +1010,8 @@ static void batch_stage2phys_t(const BatchInst* d, const int* bi, int nb, BatchP
 }
 void launch_batch_stage2phys(const BatchInst* d, const int* bi, int nb, BatchPhase ph, int tile, const int2* heavy,
                              int nHeavy, bool skip, cudaStream_t s) {
-  if (tile == 3) batch_stage2phys_t<Tile3>(d, bi, nb, ph, heavy, nHeavy, skip, s);
+  if (tile == 4) batch_stage2phys_t<Tile4>(d, bi, nb, ph, heavy, nHeavy, skip, s);
+  else if (tile == 3) batch_stage2phys_t<Tile3>(d, bi, nb, ph, heavy, nHeavy, skip, s);
   else if (tile == 2) batch_stage2phys_t<Tile2>(d, bi, nb, ph, heavy, nHeavy, skip, s);
   else if (tile == 1) batch_stage2phys_t<Tile1>(d, bi, nb, ph, heavy, nHeavy, skip, s);
   else batch_stage2phys_t<Tile0>(d, bi, nb, ph, heavy, nHeavy, skip, s);

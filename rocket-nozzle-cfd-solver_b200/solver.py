@@ -39,7 +39,7 @@ EXPORTS = ("rn_create", "rn_destroy", "rn_resize", "rn_set_mask", "rn_set_geomet
            "rn_spray_set_parcels",
            "rn_last_error")
 PRECISION = {"fast": 0, "exact": 1}
-TILES = {"16x16": 0, "16x8": 1, "16x15": 2, "32x15": 3}
+TILES = {"16x16": 0, "16x8": 1, "16x15": 2, "32x15": 3, "14x16": 4}
 KERNEL_KINDS = ("reduce", "stage1", "stage2", "physics", "parcels", "apply", "other", "stage2_physics")
 
 
@@ -580,7 +580,7 @@ class GPUSolver:
         return {b: a for a, b in PRECISION.items()}[v.value]
 
     def setTile(self, shape):
-        """Tile shape of the stage/physics kernels: '16x15' (default), '16x16', '16x8' or '32x15'."""
+        """Tile shape of the stage/physics kernels: '16x15' (default), '16x16', '16x8', '32x15' or '14x16'."""
         _check(lib().rn_set_tile(self.h, TILES[shape]))
 
     @property

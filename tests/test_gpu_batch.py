@@ -41,7 +41,7 @@ def setups(rn, kind, sizes):
 def test_tile_shapes_bit_identical(rn, oracle, kind):
     s = setups(rn, kind, [(160, 60)])[0]
     outs = []
-    for tile in ("16x16", "16x8", "16x15", "32x15"):
+    for tile in ("16x16", "16x8", "16x15", "32x15", "14x16"):
         g = make(rn, s, tile=tile)
         assert g.tile == tile
         g.step(40, s.P)
@@ -55,7 +55,7 @@ def test_tile_shapes_bit_identical(rn, oracle, kind):
 def test_fast_tile_shapes_agree(rn):
     s = setups(rn, "viscous", [(256, 96)])[0]
     outs = []
-    for tile in ("16x16", "16x8", "16x15", "32x15"):
+    for tile in ("16x16", "16x8", "16x15", "32x15", "14x16"):
         g = make(rn, s, precision="fast", tile=tile)
         g.step(60, s.P)
         outs.append(g.readAll())
@@ -72,7 +72,7 @@ def test_autotune_restores_state(rn):
     before, si = g.readAll(), g.readStepInfo()
     launches = g.kernelLaunches()
     chosen = g.autotune(s.P, steps=4)
-    assert chosen in ("16x16", "16x8", "16x15", "32x15") and g.tile == chosen
+    assert chosen in ("16x16", "16x8", "16x15", "32x15", "14x16") and g.tile == chosen
     assert identical(g.readAll(), before) and np.array_equal(g.readStepInfo(), si)
     assert g.kernelLaunches() == launches
     g.step(9, s.P)
@@ -193,7 +193,7 @@ def test_batch_autotune_restores_members(rn):
     snaps = [(g.readAll(), g.readStepInfo()) for g in members]
     n0 = batch.kernelLaunches()
     chosen = batch.autotune(steps=6)
-    assert chosen in ("16x16", "16x8", "16x15", "32x15") and batch.tile == chosen
+    assert chosen in ("16x16", "16x8", "16x15", "32x15", "14x16") and batch.tile == chosen
     assert batch.kernelLaunches() == n0
     for g, (st, si) in zip(members, snaps):
         assert identical(g.readAll(), st) and np.array_equal(g.readStepInfo(), si)
