@@ -180,7 +180,9 @@ int rn_set_precision(rn_handle h, int mode);
 int rn_get_precision(rn_handle h, int* mode);
 
 /* Tile shape of the stage/physics kernels (a thread per cell):
- * RN_TILE_16x15 (default), RN_TILE_16x16, RN_TILE_16x8, RN_TILE_32x15 or RN_TILE_14x16. rn_autotune times `steps` steps
+ * RN_TILE_16x15, RN_TILE_16x16, RN_TILE_16x8, RN_TILE_32x15 or RN_TILE_14x16. A new handle
+ * starts with RN_TILE_14x16 when the grid's 14 x 16 tiles number at most 3 per
+ * SM (all resident at once), else with RN_TILE_16x15. rn_autotune times `steps` steps
  * with each shape on a copy of the handle's current state (the state, step
  * info and spray ring are restored afterwards), keeps the fastest and returns
  * it in *chosen. No reference counterpart (the reference draws full-screen

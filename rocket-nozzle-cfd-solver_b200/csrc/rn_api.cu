@@ -300,6 +300,9 @@ int rn_create(int Nx, int Nr, rn_handle* out) {
       kernels_ready = true;
     }
   }
+  // default tile shape: 14x16 (compiled for 3 blocks per SM) when the grid's
+  // tiles are all resident at 3 per SM at once, else 16x15
+  if (Nx > 0 && Nr > 0 && ((Nx + 13) / 14) * ((Nr + 15) / 16) <= 3 * h->numSMs) h->tile = RN_TILE_14x16;
   int rc = alloc_buffers(h, Nx, Nr);
   if (rc != RN_OK) {
     std::string msg = g_err;
@@ -319,6 +322,7 @@ int rn_destroy(rn_handle h) {
   cudaStreamSynchronize(h->stream);
   free_buffers(h);
   if (h->pinned) cudaFreeHost(h->pinned);
+  if (h->asyncDev) cudaFree(h->asyncDev);
   for (auto& p : h->evPending) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
   for (auto e : h->evPool) cudaEventDestroy(e);
   cudaEventDestroy(h->asyncEv);
@@ -600,25 +604,43 @@ int rn_read_step_info(rn_handle h, float out[4]) { return rn_read_rect(h, RN_TEX
 int rn_request_async(rn_handle h, const rn_read_req* reqs, int nreq, int tag) {
   if (!valid(h) || (nreq > 0 && !reqs) || nreq < 0) return fail(RN_ERR_ARG, "rn_request_async: bad argument");
   if (h->asyncBusy) return RN_BUSY;
-  size_t total = 0;
-  for (int r = 0; r < nreq; r++) total += size_t(reqs[r].w) * reqs[r].h * 4;
-  if (total > h->pinnedCap) {
-    if (h->pinned) cudaFreeHost(h->pinned);
-    h->pinned = nullptr;
-    h->pinnedCap = 0;
-    CK(cudaHostAlloc(&h->pinned, sizeof(float) * (total > 0 ? total : 4), cudaHostAllocDefault));
-    h->pinnedCap = total;
-  }
-  size_t off = 0;
+  // the rectangles are gathered on the device by one kernel into a staging
+  // buffer, which then crosses to pinned host memory in one copy
+  std::vector<RectCopy> rects;
+  size_t total = 0;   // float4 texels
   for (int r = 0; r < nreq; r++) {
-    int rc = queue_rect(h, reqs[r].tex, reqs[r].x, reqs[r].y, reqs[r].w, reqs[r].h, h->pinned + off);
+    const float4* p;
+    int W, H;
+    int rc = tex_ptr(h, reqs[r].tex, &p, &W, &H);
     if (rc != RN_OK) return rc;
-    off += size_t(reqs[r].w) * reqs[r].h * 4;
+    const int x = reqs[r].x, y = reqs[r].y, w = reqs[r].w, hg = reqs[r].h;
+    if (x < 0 || y < 0 || w < 0 || hg < 0 || x + w > W || y + hg > H)
+      return fail(RN_ERR_ARG, "read rectangle out of range");
+    if (w > 0 && hg > 0) rects.push_back(RectCopy{p, W, x, y, w, hg, (long long)total});
+    total += size_t(w) * hg;
+  }
+  if (total > h->pinnedCap / 4 || total > h->asyncDevCap) {
+    if (h->pinned) cudaFreeHost(h->pinned);
+    if (h->asyncDev) cudaFree(h->asyncDev);
+    h->pinned = nullptr;
+    h->asyncDev = nullptr;
+    h->pinnedCap = 0;
+    h->asyncDevCap = 0;
+    CK(cudaHostAlloc(&h->pinned, sizeof(float4) * (total > 0 ? total : 1), cudaHostAllocDefault));
+    h->pinnedCap = 4 * (total > 0 ? total : 1);
+    CK(cudaMalloc(&h->asyncDev, sizeof(float4) * (total > 0 ? total : 1)));
+    h->asyncDevCap = total > 0 ? total : 1;
+  }
+  if (!rects.empty()) {
+    int rc = rn_gather_rects(rects.data(), int(rects.size()), h->asyncDev, h->stream);
+    if (rc != RN_OK) return rc;
+    h->launches++;
+    CK(cudaMemcpyAsync(h->pinned, h->asyncDev, sizeof(float4) * total, cudaMemcpyDeviceToHost, h->stream));
   }
   CK(cudaEventRecord(h->asyncEv, h->stream));
   h->asyncBusy = true;
   h->asyncTag = tag;
-  h->asyncFloats = total;
+  h->asyncFloats = 4 * total;
   return RN_OK;
 }
 

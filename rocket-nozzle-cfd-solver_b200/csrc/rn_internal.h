@@ -35,6 +35,8 @@ struct rn_solver {
   float* pinned = nullptr;
   size_t pinnedCap = 0, asyncFloats = 0;
   cudaEvent_t asyncEv = nullptr;
+  float4* asyncDev = nullptr;      // device staging of the gathered rectangles
+  size_t asyncDevCap = 0;          // float4 capacity of asyncDev
   bool asyncBusy = false;
   int asyncTag = 0;
   double* dInt = nullptr;
@@ -89,6 +91,15 @@ void rn_batch_detach(rn_solver* h);
 // Residual of the current state against the mark, into h->dRes[0..5], and the
 // mark itself, queued on `stream` (rn_readout.cu); device bytes they hold.
 int rn_residual_launch(rn_solver* h, cudaStream_t stream);
+// One rectangle (x, y, w, h) of a W-wide float4 plane, gathered row by row to
+// dst + off (rn_readout.cu). Up to RN_GATHER_RECTS per launch.
+struct RectCopy {
+  const float4* src;
+  int W, x, y, w, h;
+  long long off;
+};
+constexpr int RN_GATHER_RECTS = 8;
+int rn_gather_rects(const RectCopy* r, int n, float4* dst, cudaStream_t stream);
 int rn_residual_mark_on(rn_solver* h, cudaStream_t stream);
 size_t rn_residual_bytes(int Nx, int Nr);
 

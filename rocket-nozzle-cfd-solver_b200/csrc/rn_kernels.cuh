@@ -17,11 +17,14 @@ namespace rn {
 // 3.99, plain 4096x1536 5.51 / 5.49 / 5.73 / 5.51, 64 batched instances
 // 3.59 / 3.07 / 4.05 / 3.98. (16x16 itself beat 32x8 by 4.5-17 %.) The
 // autotuner picks per handle or batch.
-// 14x16 spreads a 512x192 grid over 37 x 12 = 444 tiles, 3 per SM on 148 SMs.
+// 14x16 spreads a 512x192 grid over 37 x 12 = 444 tiles, 3 per SM on 148 SMs,
+// and is compiled for those 3 blocks (24 warps: 80 registers, no spills); the
+// others for 32 resident warps (64 registers).
 constexpr int NTILES = 5;
 constexpr int TILE_TX[NTILES] = {16, 16, 16, 32, 14};
 constexpr int TILE_TY[NTILES] = {16, 8, 15, 15, 16};
 constexpr int TILE_NT[NTILES] = {256, 128, 256, 512, 256};
+constexpr int TILE_WARPS[NTILES] = {32, 32, 32, 32, 24};
 // Most out-of-tile group members one tile may list (set_geometry rejects more).
 constexpr int MAXX = 64;
 // Tiles listing more out-of-tile members than this run the fused stage-2 +

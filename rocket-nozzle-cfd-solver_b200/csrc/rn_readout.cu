@@ -19,6 +19,19 @@
 
 namespace {
 
+struct RectBatch {
+  RectCopy r[RN_GATHER_RECTS];
+};
+// blockIdx.y = rectangle; threads stride over its w*h texels in row order.
+__global__ void k_gather_rects(RectBatch b, float4* __restrict__ dst) {
+  const RectCopy& r = b.r[blockIdx.y];
+  const int n = r.w * r.h;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int row = k / r.w, col = k - row * r.w;
+    dst[r.off + k] = r.src[size_t(r.y + row) * r.W + r.x + col];
+  }
+}
+
 constexpr int RES_NT = 256;
 constexpr int RES_BLOCKS = 296;   // 2 per SM
 constexpr int RES_Q = 5;          // 4 components + fluid-cell count
@@ -110,6 +123,25 @@ int rn_residual_mark_on(rn_solver* h, cudaStream_t stream) {
 
 size_t rn_residual_bytes(int Nx, int Nr) {
   return sizeof(float4) * (size_t(Nx) * Nr + 1) + sizeof(double) * (8 + RES_BLOCKS * RES_Q);
+}
+
+// Gathers the rectangles into dst in launches of up to RN_GATHER_RECTS.
+int rn_gather_rects(const RectCopy* r, int n, float4* dst, cudaStream_t stream) {
+  for (int b0 = 0; b0 < n; b0 += RN_GATHER_RECTS) {
+    RectBatch b;
+    const int m = n - b0 < RN_GATHER_RECTS ? n - b0 : RN_GATHER_RECTS;
+    int most = 1;
+    for (int k = 0; k < m; k++) {
+      b.r[k] = r[b0 + k];
+      if (r[b0 + k].w * r[b0 + k].h > most) most = r[b0 + k].w * r[b0 + k].h;
+    }
+    int blocks = (most + 255) / 256;
+    if (blocks > 64) blocks = 64;
+    k_gather_rects<<<dim3(blocks, m), 256, 0, stream>>>(b, dst);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return rn_record_cuda(e, "k_gather_rects");
+  }
+  return RN_OK;
 }
 
 extern "C" {

@@ -39,29 +39,25 @@
 namespace rn {
 namespace RN_VARIANT {
 
-// Resident warps per SM the step kernels are compiled for: 32 caps them at 64
-// registers (4 blocks of 256 threads per SM). Measured on B200 (fast
-// precision, G cell-updates/s, caps of 8 / 24 / 32 / 40 warps): 64 batched
-// instances 2.24 / 3.05 / 3.44 / 3.04, plain 4096x1536 3.33 / 4.55 / 5.52 /
-// 5.65, viscous 512x192 1.71 / 2.24 / 2.18 / 1.89. Results are bit-identical
-// across caps.
-#ifndef RN_MIN_WARPS
-#define RN_MIN_WARPS 32
-#endif
-
-template <int TX_, int TY_, int NT_>
+// Resident warps per SM a tile shape's kernels are compiled for (TILE_WARPS):
+// 32 caps them at 64 registers (4 blocks of 256 threads per SM), 24 at 80.
+// Measured on B200 with 16x16 tiles (fast precision, G cell-updates/s, caps of
+// 8 / 24 / 32 / 40 warps): 64 batched instances 2.24 / 3.05 / 3.44 / 3.04,
+// plain 4096x1536 3.33 / 4.55 / 5.52 / 5.65, viscous 512x192 1.71 / 2.24 /
+// 2.18 / 1.89. Results are bit-identical across caps.
+template <int TX_, int TY_, int NT_, int WARPS_>
 struct TileT {
   static constexpr int TX = TX_, TY = TY_, NT = NT_, NC = TX * TY;   // NT threads, NC cells (NC <= NT)
-  static constexpr int MINB = RN_MIN_WARPS / (NT / 32) > 0 ? RN_MIN_WARPS / (NT / 32) : 1;
+  static constexpr int MINB = WARPS_ / (NT / 32) > 0 ? WARPS_ / (NT / 32) : 1;
   static constexpr int PX = TX + 4, PY = TY + 4, NPT = PX * PY;   // primitives with a 2-cell halo
   static constexpr int NXF = TY * (TX + 1), NRF = (TY + 1) * TX;  // x- and r-faces of a tile
   static constexpr int TW = TX + 2, NTT = (TX + 2) * (TY + 2);    // vcell ring (tile + 1)
 };
-using Tile0 = TileT<TILE_TX[0], TILE_TY[0], TILE_NT[0]>;
-using Tile1 = TileT<TILE_TX[1], TILE_TY[1], TILE_NT[1]>;
-using Tile2 = TileT<TILE_TX[2], TILE_TY[2], TILE_NT[2]>;
-using Tile3 = TileT<TILE_TX[3], TILE_TY[3], TILE_NT[3]>;
-using Tile4 = TileT<TILE_TX[4], TILE_TY[4], TILE_NT[4]>;
+using Tile0 = TileT<TILE_TX[0], TILE_TY[0], TILE_NT[0], TILE_WARPS[0]>;
+using Tile1 = TileT<TILE_TX[1], TILE_TY[1], TILE_NT[1], TILE_WARPS[1]>;
+using Tile2 = TileT<TILE_TX[2], TILE_TY[2], TILE_NT[2], TILE_WARPS[2]>;
+using Tile3 = TileT<TILE_TX[3], TILE_TY[3], TILE_NT[3], TILE_WARPS[3]>;
+using Tile4 = TileT<TILE_TX[4], TILE_TY[4], TILE_NT[4], TILE_WARPS[4]>;
 static_assert(Tile0::NC <= Tile0::NT && Tile1::NC <= Tile1::NT && Tile2::NC <= Tile2::NT && Tile3::NC <= Tile3::NT &&
                   Tile4::NC <= Tile4::NT,
               "a thread per cell");

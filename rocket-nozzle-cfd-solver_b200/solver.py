@@ -580,7 +580,8 @@ class GPUSolver:
         return {b: a for a, b in PRECISION.items()}[v.value]
 
     def setTile(self, shape):
-        """Tile shape of the stage/physics kernels: '16x15' (default), '16x16', '16x8', '32x15' or '14x16'."""
+        """Tile shape of the stage/physics kernels: '16x15', '16x16', '16x8', '32x15' or '14x16' (a new handle
+        starts with '14x16' when its tiles number at most 3 per SM, else '16x15')."""
         _check(lib().rn_set_tile(self.h, TILES[shape]))
 
     @property

@@ -123,6 +123,17 @@ def test_readbacks_agree(rn):
     assert np.array_equal(res["data"]["colA"].reshape(-1, 4), A[:, s.iExit])
     assert np.array_equal(res["data"]["blkB"].reshape(3, 5, 4), B[1:4, 2:7])
     assert g.pollAsync() is None
+    # more rectangles than one gather launch takes, an empty one among them
+    cells = [{"name": f"c{k}", "tex": st["A"], "x": 3 * k, "y": k % s.Nr, "w": 1 + k % 2, "h": 1 + k % 3}
+             for k in range(11)] + [{"name": "none", "tex": st["B"], "x": 0, "y": 0, "w": 0, "h": 4}]
+    assert g.requestAsync(cells, 10)
+    res = None
+    while res is None:
+        res = g.pollAsync()
+    for k in range(11):
+        x, y, w, h = 3 * k, k % s.Nr, 1 + k % 2, 1 + k % 3
+        assert np.array_equal(res["data"][f"c{k}"].reshape(h, w, 4), A[y:y + h, x:x + w])
+    assert res["data"]["none"].size == 0
     assert g.requestAsync(reqs[:1], 9)
     g.cancelAsync()
     assert g.pollAsync() is None
