@@ -321,6 +321,11 @@ int rn_destroy(rn_handle h) {
   rn_batch_detach(h);
   cudaStreamSynchronize(h->stream);
   free_buffers(h);
+  if (h->copyStream) {
+    cudaStreamSynchronize(h->copyStream);
+    cudaStreamDestroy(h->copyStream);
+    cudaEventDestroy(h->evGathered);
+  }
   if (h->pinned) cudaFreeHost(h->pinned);
   if (h->asyncDev) cudaFree(h->asyncDev);
   for (auto& p : h->evPending) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
@@ -631,13 +636,24 @@ int rn_request_async(rn_handle h, const rn_read_req* reqs, int nreq, int tag) {
     CK(cudaMalloc(&h->asyncDev, sizeof(float4) * (total > 0 ? total : 1)));
     h->asyncDevCap = total > 0 ? total : 1;
   }
+  if (!h->copyStream) {
+    CK(cudaStreamCreateWithFlags(&h->copyStream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&h->evGathered, cudaEventDisableTiming));
+  }
   if (!rects.empty()) {
+    // the snapshot is taken in stream order; its copy to the host runs on the
+    // copy stream, so the steps queued after it do not wait for the copy
     int rc = rn_gather_rects(rects.data(), int(rects.size()), h->asyncDev, h->stream);
     if (rc != RN_OK) return rc;
     h->launches++;
-    CK(cudaMemcpyAsync(h->pinned, h->asyncDev, sizeof(float4) * total, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaEventRecord(h->evGathered, h->stream));
+    CK(cudaStreamWaitEvent(h->copyStream, h->evGathered, 0));
+    CK(cudaMemcpyAsync(h->pinned, h->asyncDev, sizeof(float4) * total, cudaMemcpyDeviceToHost, h->copyStream));
+  } else {
+    CK(cudaEventRecord(h->evGathered, h->stream));
+    CK(cudaStreamWaitEvent(h->copyStream, h->evGathered, 0));
   }
-  CK(cudaEventRecord(h->asyncEv, h->stream));
+  CK(cudaEventRecord(h->asyncEv, h->copyStream));
   h->asyncBusy = true;
   h->asyncTag = tag;
   h->asyncFloats = 4 * total;

@@ -37,6 +37,8 @@ struct rn_solver {
   cudaEvent_t asyncEv = nullptr;
   float4* asyncDev = nullptr;      // device staging of the gathered rectangles
   size_t asyncDevCap = 0;          // float4 capacity of asyncDev
+  cudaStream_t copyStream = nullptr;   // the staging buffer's copy to the host
+  cudaEvent_t evGathered = nullptr;
   bool asyncBusy = false;
   int asyncTag = 0;
   double* dInt = nullptr;

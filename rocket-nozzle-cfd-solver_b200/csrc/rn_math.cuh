@@ -124,8 +124,11 @@ RN_DEV void ghost_prim(const Grid& g, const float4* __restrict__ A, const float4
       else q.w.y = fmaxf(q.w.y, 0.0f);
     }
   } else {
-    if (solid_at(g, i, j)) wall = true;
-    else q = to_prim(A[j * Nx + i], B[j * Nx + i]);
+    // the state is loaded with the mask (not after it), so the two loads overlap
+    const int k = j * Nx + i;
+    const float4 a = A[k], b = B[k];
+    if (g.mask[k] != 0) wall = true;
+    else q = to_prim(a, b);
   }
   if (wall) {
     W = make_float4(-1.0f, 0.0f, 0.0f, 1.0f);

@@ -230,19 +230,27 @@ __device__ __forceinline__ bool update_cell(const StageArgs& a, const rn_params&
   const Grid& g = a.g;
   const int Nx = g.Nx;
   const int k = j * Nx + i;
-  if (g.mask[k]) {
+  // the cell's own operands in one round of loads; a slave cell (host kh != k)
+  // then loads its host's
+  const uint8_t solid = g.mask[k];
+  const float4 gm = g.geoM[k], gg = g.geoG[k];
+  float4 A = a.A[k], B = a.B[k], A0 = STAGE == 2 ? a.A0[k] : A, B0 = STAGE == 2 ? a.B0[k] : B;
+  if (solid) {
     oA = make_float4(P.ambCons[0], P.ambCons[1], P.ambCons[2], P.ambCons[3]);
     oB = make_float4(P.ambB[0], P.ambB[1], P.ambB[2], P.ambB[3]);
     return false;
   }
-  float4 gm = g.geoM[k];
   const int Hx = i + iround(gm.x), Hy = j + iround(gm.y), kh = Hy * Nx + Hx;
-  float4 gg = g.geoG[k];
-  float4 A = a.A[kh], B = a.B[kh];
+  float ghz = gm.z;
+  if (kh != k) {
+    A = a.A[kh]; B = a.B[kh];
+    if (STAGE == 2) { A0 = a.A0[kh]; B0 = a.B0[kh]; }
+    ghz = g.geoM[kh].z;
+  }
   Prim q = to_prim(A, B);
   float4 L = make_float4(0.f, 0.f, 0.f, 0.f), LY = L;
   float LO = 0.0f;
-  const int sm_ = iround(g.geoM[kh].z);
+  const int sm_ = iround(ghz);
   for (int m = 0; m < 5; m++) {
     int cx = Hx, cy = Hy;
     if (m == 1) { if (!(sm_ & 1)) continue; cx -= 1; }
@@ -280,7 +288,6 @@ __device__ __forceinline__ bool update_cell(const StageArgs& a, const rn_params&
     U = make_float4(A.x + f * L.x, A.y + f * L.y, A.z + f * L.z, A.w + f * L.w);
     UY = make_float4(B.x + f * LB.x, B.y + f * LB.y, B.z + f * LB.z, B.w + f * LB.w);
   } else {
-    float4 A0 = a.A0[kh], B0 = a.B0[kh];
     U = make_float4(0.5f * (A0.x + A.x + f * L.x), 0.5f * (A0.y + A.y + f * L.y), 0.5f * (A0.z + A.z + f * L.z),
                     0.5f * (A0.w + A.w + f * L.w));
     UY = make_float4(0.5f * (B0.x + B.x + f * LB.x), 0.5f * (B0.y + B.y + f * LB.y),
@@ -407,10 +414,10 @@ __device__ __forceinline__ void vcells(const Grid& g, const rn_params& P, float 
 // FS_VFLUX_X/R: viscous faces of the tile and of the members.
 template <class T>
 __device__ __forceinline__ void viscous_faces(const Grid& g, int x0, int y0, const int* xc, int NF, const float4* sW,
-                                              const float4* sWb, const float4* sT1, const float4* sT2, float4* sF,
-                                              float4* sY) {
+                                              const float4* sWb, const float4* sT1, const float4* sT2,
+                                              const float* sAr, float4* sF, float4* sY) {
   constexpr int TX = T::TX, PX = T::PX, TW = T::TW;
-  const int Nx = g.Nx, Nr = g.Nr, W1 = Nx + 1;
+  const int Nx = g.Nx, Nr = g.Nr;
   for (int k = threadIdx.x; k < NF; k += T::NT) {
     float4 F = make_float4(0.f, 0.f, 0.f, 0.f), FY = F;
     bool dirR, ok;
@@ -437,8 +444,9 @@ __device__ __forceinline__ void viscous_faces(const Grid& g, int x0, int y0, con
       ok = dirR ? (i < Nx && j > 0 && j < Nr) : (i > 0 && i < Nx && j < Nr);
     }
     if (ok) {
-      float4 geo = g.geoA[j * W1 + i];
-      float area = dirR ? geo.w : geo.z;
+      // face k is face k of the inviscid phase, whose open area sAr[k] holds
+      // (every face drawn here was drawn there)
+      float area = sAr[k];
       float4 w1 = sW[p1], w2 = sW[p2];
       if (area != 0.0f && !(w1.x < 0.0f || w2.x < 0.0f))
         visc_flux(dirR, w1, sWb[p1], sT1[v1], sT2[v1], w2, sWb[p2], sT1[v2], sT2[v2], j, F, FY);
@@ -461,14 +469,14 @@ __device__ __forceinline__ bool source_cell(const Grid& g, const float4* __restr
   constexpr int TW = T::TW;
   const int Nx = g.Nx, Nr = g.Nr;
   const int k = j * Nx + i;
-  if (g.mask[k]) {
+  const uint8_t solid = g.mask[k];
+  const float4 gmij = g.geoM[k], gg = g.geoG[k];
+  if (solid) {
     oA = make_float4(P.ambCons[0], P.ambCons[1], P.ambCons[2], P.ambCons[3]);
     oB = make_float4(P.ambB[0], P.ambB[1], P.ambB[2], P.ambB[3]);
     return false;
   }
-  float4 gmij = g.geoM[k];
   const int Hx = i + iround(gmij.x), Hy = j + iround(gmij.y), kh = Hy * Nx + Hx;
-  float4 gg = g.geoG[k];
   Prim q = to_prim(A, B);
   float rho = q.w.x, p = q.w.w, G = q.s.z;
   float velx = q.w.y, vely = q.w.z;
@@ -478,7 +486,7 @@ __device__ __forceinline__ bool source_cell(const Grid& g, const float4* __restr
   const int vh = (Hy - y0 + 1) * TW + (Hx - x0 + 1);
   float4 T1h = sT1[vh], T2h = sT2[vh];
   if (P.visc) {
-    const int sm_ = iround(g.geoM[kh].z);
+    const int sm_ = iround(kh == k ? gmij.z : g.geoM[kh].z);
     for (int m = 0; m < 5; m++) {
       int cx = Hx, cy = Hy;
       if (m == 1) { if (!(sm_ & 1)) continue; cx -= 1; }
@@ -649,7 +657,7 @@ __device__ __forceinline__ void stage2_physics_body(const StageArgs& a, const Ph
   float4* sY = sF + NFV;
   vcells<T>(g, P, dt, x0, y0, xc, NV, sW, sWb, sT1, sT2);
   __syncthreads();
-  if (P.visc) viscous_faces<T>(g, x0, y0, xc, NFV, sW, sWb, sT1, sT2, sF, sY);
+  if (P.visc) viscous_faces<T>(g, x0, y0, xc, NFV, sW, sWb, sT1, sT2, sAr, sF, sY);
   __syncthreads();
 
   const int i = x0 + tid % TX, j = y0 + tid / TX;
