@@ -280,23 +280,31 @@ def run_ours(args, rank, world, local_rank):
         torch.distributed.barrier()
     # The app's frame loop: queue the next step(n, P) before waiting for the
     # previous read-back, then turn that read-back into the read-outs while
-    # the GPU runs (requestAsync / pollAsync keep one read in flight).
-    t0 = time.perf_counter()
-    perf = None
-    g.step(SOLVER_STEPS, setup.P)              # parameter block converted and passed every call
-    g.requestAsync(reqs, 0)
-    for k in range(args.steps):
-        if k + 1 < args.steps:
-            g.step(SOLVER_STEPS, setup.P)
-        res = None
-        while res is None:
-            res = g.pollAsync()
-        d = res["data"]
-        perf = rn.exit_performance(setup, {"A": d["colA"], "B": d["colB"]})
-        if k + 1 < args.steps:
-            g.requestAsync(reqs, k + 1)
-    g.sync()
-    e2e_s = replicas.max_over_ranks(time.perf_counter() - t0, dev)
+    # the GPU runs (requestAsync / pollAsync keep one read in flight). Run 3
+    # times; the median run is reported, all three are listed.
+    def frame_loop():
+        t0 = time.perf_counter()
+        perf, iters = None, []
+        g.step(SOLVER_STEPS, setup.P)              # parameter block converted and passed every call
+        g.requestAsync(reqs, 0)
+        for k in range(args.steps):
+            ta = time.perf_counter()
+            if k + 1 < args.steps:
+                g.step(SOLVER_STEPS, setup.P)
+            res = None
+            while res is None:
+                res = g.pollAsync()
+            d = res["data"]
+            perf = rn.exit_performance(setup, {"A": d["colA"], "B": d["colB"]})
+            if k + 1 < args.steps:
+                g.requestAsync(reqs, k + 1)
+            iters.append(time.perf_counter() - ta)
+        g.sync()
+        return replicas.max_over_ranks(time.perf_counter() - t0, dev), perf, iters
+
+    runs = [frame_loop() for _ in range(3)]
+    e2e_runs = [world * cells * SOLVER_STEPS * args.steps / r[0] for r in runs]
+    e2e_s, perf, iters = sorted(runs, key=lambda r: r[0])[1]
     e2e = world * cells * SOLVER_STEPS * args.steps / e2e_s
     g.close()
     del flush
@@ -330,7 +338,8 @@ def run_ours(args, rank, world, local_rank):
                        "tile": tile_name},
             "roofline": roofline, "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "exit_thrust_N": perf["F"] if perf else None},
+                    "exit_thrust_N": perf["F"] if perf else None, "runs": e2e_runs,
+                    "frame_ms_median": 1e3 * float(np.median(iters)), "frame_ms_max": 1e3 * float(max(iters))},
             "steady_state_value": steady,
             "gpu_launches": launches, "clocks": clk.summary(), "fp64_error": fp64, "spray": spray, "large_grid": large,
             "batched": batched, "serving": serving}
