@@ -179,13 +179,28 @@ __host__ __device__ constexpr size_t stage_smem_t(int maxX) {
 // Phases shared by the stage, physics and fused kernels. Each loops its slots
 // over the block's threads; the caller puts the barriers between phases.
 
+// Open area of face slot k as the reference reads it from geoA (0 where the
+// face is not drawn).
+template <class T>
+__device__ __forceinline__ float face_area(const Grid& g, int k, int x0, int y0, const int* xc) {
+  const FaceSlot s = face_slot<T>(k, x0, y0, xc, g.Nx, g.Nr);
+  if (!s.valid) return 0.0f;
+  const float4* p = g.geoA + (s.j * (g.Nx + 1) + s.i);
+  return s.dirR ? p->w : p->z;
+}
+
 // FS_PRIM: ghost-cell primitives of the tile + 2-cell halo, then the listed
-// members' 5x5 blocks.
+// members' 5x5 blocks. The open areas of the NF faces go to sAr on the way:
+// a thread's first two are loaded before its primitives and stored after
+// them, so their latency hides behind the primitive phase.
 template <class T>
 __device__ __forceinline__ void load_prims(const Grid& g, const float4* __restrict__ A, const float4* __restrict__ B,
                                            float t, const rn_params& P, int x0, int y0, const int* xc, int NP,
-                                           float4* sW, float4* sWb) {
+                                           float4* sW, float4* sWb, int NF, float* sAr) {
   const int Nx = g.Nx, Nr = g.Nr;
+  const int f0 = threadIdx.x, f1 = threadIdx.x + T::NT;
+  const float ar0 = f0 < NF ? face_area<T>(g, f0, x0, y0, xc) : 0.0f;
+  const float ar1 = f1 < NF ? face_area<T>(g, f1, x0, y0, xc) : 0.0f;
   for (int k = threadIdx.x; k < NP; k += T::NT) {
     int i, j;
     prim_slot<T>(k, x0, y0, xc, Nx, i, j);
@@ -195,28 +210,26 @@ __device__ __forceinline__ void load_prims(const Grid& g, const float4* __restri
     sW[k] = W;
     sWb[k] = Wb;
   }
+  if (f0 < NF) sAr[f0] = ar0;
+  if (f1 < NF) sAr[f1] = ar1;
+  for (int k = f1 + T::NT; k < NF; k += T::NT) sAr[k] = face_area<T>(g, k, x0, y0, xc);
 }
 
 // FS_FLUX_X/R: tile x-faces, tile r-faces, members' faces.
 template <class T>
 __device__ __forceinline__ void inviscid_faces(const Grid& g, const rn_params& P, int x0, int y0, const int* xc,
                                                int NF, const float4* sW, const float4* sWb, float4* sF, float4* sY,
-                                               float* sO, float* sAr) {
-  const int Nx = g.Nx, Nr = g.Nr, W1 = Nx + 1;
+                                               float* sO, const float* sAr) {
+  const int Nx = g.Nx, Nr = g.Nr;
   for (int k = threadIdx.x; k < NF; k += T::NT) {
     const FaceSlot s = face_slot<T>(k, x0, y0, xc, Nx, Nr);
     Flux f;
     f.F = make_float4(0.f, 0.f, 0.f, 0.f); f.Y = f.F; f.O = 0.f;
-    float area = 0.0f;
-    if (s.valid) {
-      float4 geo = g.geoA[s.j * W1 + s.i];
-      area = s.dirR ? geo.w : geo.z;
-      if (area != 0.0f)
-        f = face_flux(s.dirR, area, sW[s.c[0]], sWb[s.c[0]], sW[s.c[1]], sWb[s.c[1]], sW[s.c[2]], sWb[s.c[2]],
-                      sW[s.c[3]], sWb[s.c[3]], sW[s.s[0]], sW[s.s[1]], sW[s.s[2]], sW[s.s[3]], P);
-    }
+    const float area = sAr[k];   // the face's open area, 0 where it is not drawn (load_prims)
+    if (area != 0.0f)
+      f = face_flux(s.dirR, area, sW[s.c[0]], sWb[s.c[0]], sW[s.c[1]], sWb[s.c[1]], sW[s.c[2]], sWb[s.c[2]],
+                    sW[s.c[3]], sWb[s.c[3]], sW[s.s[0]], sW[s.s[1]], sW[s.s[2]], sW[s.s[3]], P);
     sF[k] = f.F; sY[k] = f.Y; sO[k] = f.O;
-    sAr[k] = area;   // the face's (signed) open area, for the group sums
   }
 }
 
@@ -356,7 +369,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const rn_params& 
     t = st.z;                                     // inlet ramp at t_new
   }
   __syncthreads();
-  load_prims<T>(g, a.A, a.B, t, P, x0, y0, xc, NP, sW, sWb);
+  load_prims<T>(g, a.A, a.B, t, P, x0, y0, xc, NP, sW, sWb, NF, sAr);
   __syncthreads();
   inviscid_faces<T>(g, P, x0, y0, xc, NF, sW, sWb, sF, sY, sO, sAr);
   __syncthreads();
@@ -627,7 +640,7 @@ __device__ __forceinline__ void stage2_physics_body(const StageArgs& a, const Ph
   const float4 st = *a.stNew;
   const float dt = st.x, t = st.z;
   __syncthreads();
-  load_prims<T>(g, a.A, a.B, t, P, x0, y0, xc, NP, sW, sWb);
+  load_prims<T>(g, a.A, a.B, t, P, x0, y0, xc, NP, sW, sWb, NF, sAr);
   __syncthreads();
   {
     float4* sF = R;
