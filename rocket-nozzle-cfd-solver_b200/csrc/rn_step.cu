@@ -201,14 +201,42 @@ __device__ __forceinline__ void load_prims(const Grid& g, const float4* __restri
   const int f0 = threadIdx.x, f1 = threadIdx.x + T::NT;
   const float ar0 = f0 < NF ? face_area<T>(g, f0, x0, y0, xc) : 0.0f;
   const float ar1 = f1 < NF ? face_area<T>(g, f1, x0, y0, xc) : 0.0f;
-  for (int k = threadIdx.x; k < NP; k += T::NT) {
-    int i, j;
-    prim_slot<T>(k, x0, y0, xc, Nx, i, j);
-    float4 W, Wb;
-    if (i <= Nx + 1 && j <= Nr + 1) ghost_prim(g, A, B, i, j, t, P, W, Wb);
-    else { W = make_float4(-1.f, 0.f, 0.f, 1.f); Wb = make_float4(0.f, 0.f, 0.f, 0.f); }
-    sW[k] = W;
-    sWb[k] = Wb;
+  // Two slots per round: the state and mask of both (where they are grid
+  // cells) are loaded before either is converted, so the two rounds' loads
+  // overlap. Ghost slots outside the grid take ghost_prim's boundary branches.
+  for (int k0 = threadIdx.x; k0 < NP; k0 += 2 * T::NT) {
+    const int k1 = k0 + T::NT;
+    int i0, j0, i1 = -1, j1 = -1;
+    prim_slot<T>(k0, x0, y0, xc, Nx, i0, j0);
+    if (k1 < NP) prim_slot<T>(k1, x0, y0, xc, Nx, i1, j1);
+    const bool in0 = i0 >= 0 && i0 < Nx && j0 >= 0 && j0 < Nr;
+    const bool in1 = k1 < NP && i1 >= 0 && i1 < Nx && j1 >= 0 && j1 < Nr;
+    float4 a0, b0, a1, b1;
+    uint8_t m0 = 0, m1 = 0;
+    if (in0) { const int c = j0 * Nx + i0; a0 = A[c]; b0 = B[c]; m0 = g.mask[c]; }
+    if (in1) { const int c = j1 * Nx + i1; a1 = A[c]; b1 = B[c]; m1 = g.mask[c]; }
+#pragma unroll
+    for (int u = 0; u < 2; u++) {
+      const int k = u ? k1 : k0, i = u ? i1 : i0, j = u ? j1 : j0;
+      if (k >= NP) break;
+      float4 W, Wb;
+      if (u ? in1 : in0) {                       // ghost_prim's interior branch
+        if (u ? m1 : m0) {
+          W = make_float4(-1.0f, 0.0f, 0.0f, 1.0f);
+          Wb = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        } else {
+          const Prim q = to_prim(u ? a1 : a0, u ? b1 : b0);
+          W = q.w;
+          Wb = q.s;
+        }
+      } else if (i <= Nx + 1 && j <= Nr + 1) {
+        ghost_prim(g, A, B, i, j, t, P, W, Wb);
+      } else {
+        W = make_float4(-1.f, 0.f, 0.f, 1.f); Wb = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+      sW[k] = W;
+      sWb[k] = Wb;
+    }
   }
   if (f0 < NF) sAr[f0] = ar0;
   if (f1 < NF) sAr[f1] = ar1;
