@@ -49,6 +49,12 @@ template <int TX_, int TY_, int NT_, int WARPS_>
 struct TileT {
   static constexpr int TX = TX_, TY = TY_, NT = NT_, NC = TX * TY;   // NT threads, NC cells (NC <= NT)
   static constexpr int MINB = WARPS_ / (NT / 32) > 0 ? WARPS_ / (NT / 32) : 1;
+  // Shapes compiled for fewer than 32 warps run the fused kernel's stage-2
+  // update and FS_VCELL as one work list, with T1/T2 in shared memory of their
+  // own (viscous plume 512x192 with 14x16 tiles: 3.00 -> 3.18 G
+  // cell-updates/s); at 4 blocks per SM that memory and the longer loop body
+  // cost more than they save (64 batched instances, 16x15: 4.37 -> 4.18 G).
+  static constexpr bool MERGED = WARPS_ < 32;
   static constexpr int PX = TX + 4, PY = TY + 4, NPT = PX * PY;   // primitives with a 2-cell halo
   static constexpr int NXF = TY * (TX + 1), NRF = (TY + 1) * TX;  // x- and r-faces of a tile
   static constexpr int TW = TX + 2, NTT = (TX + 2) * (TY + 2);    // vcell ring (tile + 1)
@@ -436,20 +442,18 @@ __device__ __forceinline__ void vcell_slot(int k, int x0, int y0, const int* xc,
   }
 }
 
-// FS_VCELL over the tile + 1 ring and the members' cells.
+// FS_VCELL of vcell slot k (the tile + 1 ring, then the members' cells).
 template <class T>
-__device__ __forceinline__ void vcells(const Grid& g, const rn_params& P, float dt, int x0, int y0, const int* xc,
-                                       int NV, const float4* sW, const float4* sWb, float4* sT1, float4* sT2) {
+__device__ __forceinline__ void vcell_at(const Grid& g, const rn_params& P, float dt, int x0, int y0, const int* xc,
+                                         int k, const float4* sW, const float4* sWb, float4* sT1, float4* sT2) {
   const int Nx = g.Nx, Nr = g.Nr;
-  for (int k = threadIdx.x; k < NV; k += T::NT) {
-    int i, j, c, e_, w_, n_, s_;
-    vcell_slot<T>(k, x0, y0, xc, Nx, i, j, c, e_, w_, n_, s_);
-    float4 T1 = make_float4(0.f, 0.f, 0.f, 0.f), T2 = T1;
-    if (i >= 0 && i < Nx && j >= 0 && j < Nr)
-      vcell(sW[c], sWb[c], sW[e_], sW[w_], sW[n_], sW[s_], i, j, g.geoM[j * Nx + i].w, dt, P, T1, T2);
-    sT1[k] = T1;
-    sT2[k] = T2;
-  }
+  int i, j, c, e_, w_, n_, s_;
+  vcell_slot<T>(k, x0, y0, xc, Nx, i, j, c, e_, w_, n_, s_);
+  float4 T1 = make_float4(0.f, 0.f, 0.f, 0.f), T2 = T1;
+  if (i >= 0 && i < Nx && j >= 0 && j < Nr)
+    vcell(sW[c], sWb[c], sW[e_], sW[w_], sW[n_], sW[s_], i, j, g.geoM[j * Nx + i].w, dt, P, T1, T2);
+  sT1[k] = T1;
+  sT2[k] = T2;
 }
 
 // FS_VFLUX_X/R: viscous faces of the tile and of the members.
@@ -635,16 +639,19 @@ __device__ __forceinline__ bool source_cell(const Grid& g, const float4* __restr
 // tile cell can have) stay in shared memory and feed FS_SOURCE directly.
 template <class T>
 __host__ __device__ constexpr size_t fused_region_t(int maxX) {
-  // float4 slots of the region that holds first the inviscid faces, then
-  // the vcell ring and the viscous faces
-  return (2 * (T::NXF + T::NRF + 4 * maxX) + ((T::NXF + T::NRF + 4 * maxX) + 3) / 4) >
-                 (2 * (T::NTT + 5 * maxX) + 2 * (T::NXF + T::NRF + 4 * maxX))
+  // float4 slots of the region that holds first the inviscid faces' F, Y and
+  // O, then (T::MERGED) the viscous faces' F and Y, which need less, or the
+  // vcell ring's T1/T2 and the viscous faces
+  return T::MERGED || (2 * (T::NXF + T::NRF + 4 * maxX) + ((T::NXF + T::NRF + 4 * maxX) + 3) / 4) >
+                          (2 * (T::NTT + 5 * maxX) + 2 * (T::NXF + T::NRF + 4 * maxX))
              ? (2 * (T::NXF + T::NRF + 4 * maxX) + ((T::NXF + T::NRF + 4 * maxX) + 3) / 4)
              : (2 * (T::NTT + 5 * maxX) + 2 * (T::NXF + T::NRF + 4 * maxX));
 }
 template <class T>
 __host__ __device__ constexpr size_t fused_smem_t(int maxX) {
-  return sizeof(float4) * (2 * (T::NPT + 25 * maxX) + fused_region_t<T>(maxX) + 2 * (T::NT + maxX)) +
+  // primitives, face region, vcell T1/T2 (T::MERGED), stage-2 results, face areas
+  return sizeof(float4) * (2 * (T::NPT + 25 * maxX) + fused_region_t<T>(maxX) +
+                           (T::MERGED ? 2 * (T::NTT + 5 * maxX) : 0) + 2 * (T::NT + maxX)) +
          sizeof(float) * (T::NXF + T::NRF + 4 * maxX);
 }
 template <class T>
@@ -661,7 +668,9 @@ __device__ __forceinline__ void stage2_physics_body(const StageArgs& a, const Ph
   float4* sW = sm;
   float4* sWb = sW + NP;
   float4* R = sWb + NP;
-  float4* sA2 = R + fused_region_t<T>(xn);
+  float4* sT1 = T::MERGED ? R + fused_region_t<T>(xn) : R;
+  float4* sT2 = sT1 + (T::MERGED ? T::NTT + 5 * xn : NV);
+  float4* sA2 = T::MERGED ? sT2 + (T::NTT + 5 * xn) : R + fused_region_t<T>(xn);
   float4* sB2 = sA2 + NT + xn;
   float* sAr = reinterpret_cast<float*>(sB2 + NT + xn);   // face areas, kept for FS_SOURCE
   for (int q = tid; q < xn; q += NT) xc[q] = a.xcell[xb + q];
@@ -676,28 +685,39 @@ __device__ __forceinline__ void stage2_physics_body(const StageArgs& a, const Ph
     float* sO = reinterpret_cast<float*>(sY + NF);
     inviscid_faces<T>(g, P, x0, y0, xc, NF, sW, sWb, sF, sY, sO, sAr);
     __syncthreads();
-    const int i = x0 + tid % TX, j = y0 + tid / TX;
-    if (tid < T::NC && i < Nx && j < Nr) {
-      float4 oA, oB;
-      update_cell<T, 2>(a, P, i, j, dt, t, x0, y0, xc, xn, sF, sY, sO, sAr, oA, oB);
-      sA2[tid] = oA;
-      sB2[tid] = oB;
-    }
-    for (int q = tid; q < xn; q += NT) {
-      const int m = xc[q];
-      float4 oA, oB;
-      update_cell<T, 2>(a, P, m % Nx, m / Nx, dt, t, x0, y0, xc, xn, sF, sY, sO, sAr, oA, oB);
-      sA2[NT + q] = oA;
-      sB2[NT + q] = oB;
+    // One flat list (T::MERGED): the stage-2 update of the tile's cells and of
+    // its listed members, then FS_VCELL of the vcell slots. FS_VCELL reads only
+    // the stage-2 input primitives, so it needs no barrier after the update,
+    // and the list fills whole passes of the block. Otherwise FS_VCELL follows
+    // in a phase of its own, its T1/T2 taking the faces' place.
+    const int NU = T::NC + xn;
+    for (int q = tid; q < NU + (T::MERGED ? NV : 0); q += NT) {
+      if (q < T::NC) {                            // q == tid here (NC <= NT)
+        const int i = x0 + q % TX, j = y0 + q / TX;
+        if (i < Nx && j < Nr) {
+          float4 oA, oB;
+          update_cell<T, 2>(a, P, i, j, dt, t, x0, y0, xc, xn, sF, sY, sO, sAr, oA, oB);
+          sA2[q] = oA;
+          sB2[q] = oB;
+        }
+      } else if (q < NU) {
+        const int e = q - T::NC, m = xc[e];
+        float4 oA, oB;
+        update_cell<T, 2>(a, P, m % Nx, m / Nx, dt, t, x0, y0, xc, xn, sF, sY, sO, sAr, oA, oB);
+        sA2[NT + e] = oA;
+        sB2[NT + e] = oB;
+      } else {
+        vcell_at<T>(g, P, dt, x0, y0, xc, q - NU, sW, sWb, sT1, sT2);
+      }
     }
   }
   __syncthreads();
-  float4* sT1 = R;
-  float4* sT2 = sT1 + NV;
-  float4* sF = sT2 + NV;
+  float4* sF = T::MERGED ? R : sT2 + NV;
   float4* sY = sF + NFV;
-  vcells<T>(g, P, dt, x0, y0, xc, NV, sW, sWb, sT1, sT2);
-  __syncthreads();
+  if (!T::MERGED) {
+    for (int k = tid; k < NV; k += NT) vcell_at<T>(g, P, dt, x0, y0, xc, k, sW, sWb, sT1, sT2);
+    __syncthreads();
+  }
   if (P.visc) viscous_faces<T>(g, x0, y0, xc, NFV, sW, sWb, sT1, sT2, sAr, sF, sY);
   __syncthreads();
 
