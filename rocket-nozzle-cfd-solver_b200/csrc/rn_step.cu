@@ -49,12 +49,14 @@ template <int TX_, int TY_, int NT_, int WARPS_>
 struct TileT {
   static constexpr int TX = TX_, TY = TY_, NT = NT_, NC = TX * TY;   // NT threads, NC cells (NC <= NT)
   static constexpr int MINB = WARPS_ / (NT / 32) > 0 ? WARPS_ / (NT / 32) : 1;
-  // Shapes compiled for fewer than 32 warps run the fused kernel's stage-2
-  // update and FS_VCELL as one work list, with T1/T2 in shared memory of their
-  // own (viscous plume 512x192 with 14x16 tiles: 3.00 -> 3.18 G
-  // cell-updates/s); at 4 blocks per SM that memory and the longer loop body
-  // cost more than they save (64 batched instances, 16x15: 4.37 -> 4.18 G).
-  static constexpr bool MERGED = WARPS_ < 32;
+  // Shapes compiled for fewer than 32 warps (more registers per thread) run
+  // the fused kernel's stage-2 update and FS_VCELL as one work list, with
+  // T1/T2 in shared memory of their own (viscous plume 512x192 with 14x16
+  // tiles: 3.00 -> 3.10-3.18 G cell-updates/s), and load their first
+  // primitives before the member list (prefetch_prims). At 4 blocks per SM
+  // the extra memory, loop body and live registers cost more than they save
+  // (64 batched instances, 16x15: 4.37 -> 4.18 G).
+  static constexpr bool WIDE = WARPS_ < 32;
   static constexpr int PX = TX + 4, PY = TY + 4, NPT = PX * PY;   // primitives with a 2-cell halo
   static constexpr int NXF = TY * (TX + 1), NRF = (TY + 1) * TX;  // x- and r-faces of a tile
   static constexpr int TW = TX + 2, NTT = (TX + 2) * (TY + 2);    // vcell ring (tile + 1)
@@ -195,6 +197,39 @@ __device__ __forceinline__ float face_area(const Grid& g, int k, int x0, int y0,
   return s.dirR ? p->w : p->z;
 }
 
+// State and mask of a thread's first two primitive slots (tid, tid + NT) where
+// they are tile slots and grid cells: loads that need neither the member list
+// nor the step info, so a block issues them first and they overlap those.
+struct PrimPair {
+  float4 a[2], b[2];
+  uint8_t m[2];
+  bool in[2];
+};
+template <class T>
+__device__ __forceinline__ PrimPair prefetch_prims(const Grid& g, const float4* __restrict__ A,
+                                                   const float4* __restrict__ B, int x0, int y0) {
+  PrimPair p;
+  if (!T::WIDE) return p;                        // load_prims loads them itself
+#pragma unroll
+  for (int u = 0; u < 2; u++) {
+    const int k = threadIdx.x + u * T::NT;
+    p.in[u] = false;
+    p.m[u] = 0;
+    if (k < T::NPT) {
+      int i, j;
+      prim_slot<T>(k, x0, y0, nullptr, g.Nx, i, j);   // a tile slot: the member list is not read
+      p.in[u] = i >= 0 && i < g.Nx && j >= 0 && j < g.Nr;
+      if (p.in[u]) {
+        const int c = j * g.Nx + i;
+        p.a[u] = A[c];
+        p.b[u] = B[c];
+        p.m[u] = g.mask[c];
+      }
+    }
+  }
+  return p;
+}
+
 // FS_PRIM: ghost-cell primitives of the tile + 2-cell halo, then the listed
 // members' 5x5 blocks. The open areas of the NF faces go to sAr on the way:
 // a thread's first two are loaded before its primitives and stored after
@@ -202,7 +237,7 @@ __device__ __forceinline__ float face_area(const Grid& g, int k, int x0, int y0,
 template <class T>
 __device__ __forceinline__ void load_prims(const Grid& g, const float4* __restrict__ A, const float4* __restrict__ B,
                                            float t, const rn_params& P, int x0, int y0, const int* xc, int NP,
-                                           float4* sW, float4* sWb, int NF, float* sAr) {
+                                           float4* sW, float4* sWb, int NF, float* sAr, const PrimPair& pf) {
   const int Nx = g.Nx, Nr = g.Nr;
   const int f0 = threadIdx.x, f1 = threadIdx.x + T::NT;
   const float ar0 = f0 < NF ? face_area<T>(g, f0, x0, y0, xc) : 0.0f;
@@ -219,8 +254,11 @@ __device__ __forceinline__ void load_prims(const Grid& g, const float4* __restri
     const bool in1 = k1 < NP && i1 >= 0 && i1 < Nx && j1 >= 0 && j1 < Nr;
     float4 a0, b0, a1, b1;
     uint8_t m0 = 0, m1 = 0;
-    if (in0) { const int c = j0 * Nx + i0; a0 = A[c]; b0 = B[c]; m0 = g.mask[c]; }
-    if (in1) { const int c = j1 * Nx + i1; a1 = A[c]; b1 = B[c]; m1 = g.mask[c]; }
+    const bool first = T::WIDE && k0 == int(threadIdx.x);   // the round prefetch_prims loaded (tile slots)
+    if (first && k0 < T::NPT) { a0 = pf.a[0]; b0 = pf.b[0]; m0 = pf.m[0]; }
+    else if (in0) { const int c = j0 * Nx + i0; a0 = A[c]; b0 = B[c]; m0 = g.mask[c]; }
+    if (first && k1 < T::NPT) { a1 = pf.a[1]; b1 = pf.b[1]; m1 = pf.m[1]; }
+    else if (in1) { const int c = j1 * Nx + i1; a1 = A[c]; b1 = B[c]; m1 = g.mask[c]; }
 #pragma unroll
     for (int u = 0; u < 2; u++) {
       const int k = u ? k1 : k0, i = u ? i1 : i0, j = u ? j1 : j0;
@@ -376,6 +414,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const rn_params& 
   const int Nx = g.Nx, Nr = g.Nr;
   const int tid = threadIdx.x;
   const int x0 = bx * TX, y0 = by * T::TY;
+  const PrimPair pf = prefetch_prims<T>(g, a.A, a.B, x0, y0);
   const int xb = a.xoff[tileId], xn = a.xoff[tileId + 1] - xb;
   const int NP = T::NPT + 25 * xn, NF = T::NXF + T::NRF + 4 * xn;
   float4* sW = sm;
@@ -403,7 +442,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const rn_params& 
     t = st.z;                                     // inlet ramp at t_new
   }
   __syncthreads();
-  load_prims<T>(g, a.A, a.B, t, P, x0, y0, xc, NP, sW, sWb, NF, sAr);
+  load_prims<T>(g, a.A, a.B, t, P, x0, y0, xc, NP, sW, sWb, NF, sAr, pf);
   __syncthreads();
   inviscid_faces<T>(g, P, x0, y0, xc, NF, sW, sWb, sF, sY, sO, sAr);
   __syncthreads();
@@ -640,18 +679,18 @@ __device__ __forceinline__ bool source_cell(const Grid& g, const float4* __restr
 template <class T>
 __host__ __device__ constexpr size_t fused_region_t(int maxX) {
   // float4 slots of the region that holds first the inviscid faces' F, Y and
-  // O, then (T::MERGED) the viscous faces' F and Y, which need less, or the
+  // O, then (T::WIDE) the viscous faces' F and Y, which need less, or the
   // vcell ring's T1/T2 and the viscous faces
-  return T::MERGED || (2 * (T::NXF + T::NRF + 4 * maxX) + ((T::NXF + T::NRF + 4 * maxX) + 3) / 4) >
+  return T::WIDE || (2 * (T::NXF + T::NRF + 4 * maxX) + ((T::NXF + T::NRF + 4 * maxX) + 3) / 4) >
                           (2 * (T::NTT + 5 * maxX) + 2 * (T::NXF + T::NRF + 4 * maxX))
              ? (2 * (T::NXF + T::NRF + 4 * maxX) + ((T::NXF + T::NRF + 4 * maxX) + 3) / 4)
              : (2 * (T::NTT + 5 * maxX) + 2 * (T::NXF + T::NRF + 4 * maxX));
 }
 template <class T>
 __host__ __device__ constexpr size_t fused_smem_t(int maxX) {
-  // primitives, face region, vcell T1/T2 (T::MERGED), stage-2 results, face areas
+  // primitives, face region, vcell T1/T2 (T::WIDE), stage-2 results, face areas
   return sizeof(float4) * (2 * (T::NPT + 25 * maxX) + fused_region_t<T>(maxX) +
-                           (T::MERGED ? 2 * (T::NTT + 5 * maxX) : 0) + 2 * (T::NT + maxX)) +
+                           (T::WIDE ? 2 * (T::NTT + 5 * maxX) : 0) + 2 * (T::NT + maxX)) +
          sizeof(float) * (T::NXF + T::NRF + 4 * maxX);
 }
 template <class T>
@@ -662,22 +701,23 @@ __device__ __forceinline__ void stage2_physics_body(const StageArgs& a, const Ph
   const int Nx = g.Nx, Nr = g.Nr;
   const int tid = threadIdx.x;
   const int x0 = bx * TX, y0 = by * T::TY;
+  const PrimPair pf = prefetch_prims<T>(g, a.A, a.B, x0, y0);
   const int xb = a.xoff[tileId], xn = a.xoff[tileId + 1] - xb, xnP = P.visc ? xn : 0;
   const int NP = T::NPT + 25 * xn, NF = T::NXF + T::NRF + 4 * xn;
   const int NV = T::NTT + 5 * xnP, NFV = T::NXF + T::NRF + 4 * xnP;
   float4* sW = sm;
   float4* sWb = sW + NP;
   float4* R = sWb + NP;
-  float4* sT1 = T::MERGED ? R + fused_region_t<T>(xn) : R;
-  float4* sT2 = sT1 + (T::MERGED ? T::NTT + 5 * xn : NV);
-  float4* sA2 = T::MERGED ? sT2 + (T::NTT + 5 * xn) : R + fused_region_t<T>(xn);
+  float4* sT1 = T::WIDE ? R + fused_region_t<T>(xn) : R;
+  float4* sT2 = sT1 + (T::WIDE ? T::NTT + 5 * xn : NV);
+  float4* sA2 = T::WIDE ? sT2 + (T::NTT + 5 * xn) : R + fused_region_t<T>(xn);
   float4* sB2 = sA2 + NT + xn;
   float* sAr = reinterpret_cast<float*>(sB2 + NT + xn);   // face areas, kept for FS_SOURCE
   for (int q = tid; q < xn; q += NT) xc[q] = a.xcell[xb + q];
   const float4 st = *a.stNew;
   const float dt = st.x, t = st.z;
   __syncthreads();
-  load_prims<T>(g, a.A, a.B, t, P, x0, y0, xc, NP, sW, sWb, NF, sAr);
+  load_prims<T>(g, a.A, a.B, t, P, x0, y0, xc, NP, sW, sWb, NF, sAr, pf);
   __syncthreads();
   {
     float4* sF = R;
@@ -685,13 +725,13 @@ __device__ __forceinline__ void stage2_physics_body(const StageArgs& a, const Ph
     float* sO = reinterpret_cast<float*>(sY + NF);
     inviscid_faces<T>(g, P, x0, y0, xc, NF, sW, sWb, sF, sY, sO, sAr);
     __syncthreads();
-    // One flat list (T::MERGED): the stage-2 update of the tile's cells and of
+    // One flat list (T::WIDE): the stage-2 update of the tile's cells and of
     // its listed members, then FS_VCELL of the vcell slots. FS_VCELL reads only
     // the stage-2 input primitives, so it needs no barrier after the update,
     // and the list fills whole passes of the block. Otherwise FS_VCELL follows
     // in a phase of its own, its T1/T2 taking the faces' place.
     const int NU = T::NC + xn;
-    for (int q = tid; q < NU + (T::MERGED ? NV : 0); q += NT) {
+    for (int q = tid; q < NU + (T::WIDE ? NV : 0); q += NT) {
       if (q < T::NC) {                            // q == tid here (NC <= NT)
         const int i = x0 + q % TX, j = y0 + q / TX;
         if (i < Nx && j < Nr) {
@@ -712,9 +752,9 @@ __device__ __forceinline__ void stage2_physics_body(const StageArgs& a, const Ph
     }
   }
   __syncthreads();
-  float4* sF = T::MERGED ? R : sT2 + NV;
+  float4* sF = T::WIDE ? R : sT2 + NV;
   float4* sY = sF + NFV;
-  if (!T::MERGED) {
+  if (!T::WIDE) {
     for (int k = tid; k < NV; k += NT) vcell_at<T>(g, P, dt, x0, y0, xc, k, sW, sWb, sT1, sT2);
     __syncthreads();
   }
