@@ -31,18 +31,37 @@ struct Grid {
 struct Prim { float4 w, s; };        // w = (rho, u, v, p), s = (Z, F, G, O)   solver.js:29
 struct Flux { float4 F, Y; float O; };   // face flux: F(4), (FZ, FF, u_f G_f, u_f), FO
 
-// Division of the time-step arithmetic. The fast variant (RN_FAST_DIV) takes
+// Division of the time-step arithmetic. The fast variant (RN_FAST) takes
 // the hardware's reciprocal-based quotient (div.approx, within 2 ulp for
 // divisors of magnitude 2^-126 .. 2^126, which every divisor here is: densities,
 // pressures, wave speeds, face areas and volumes, all floored well above
 // 2^-126 and far below 2^126); the exact variant divides as IEEE does.
 RN_DEV float fdiv(float a, float b) {
-#ifdef RN_FAST_DIV
+#ifdef RN_FAST
   return __fdividef(a, b);
 #else
   return a / b;
 #endif
 }
+
+// Pairs of lanes through Blackwell's packed FP32 instructions (two IEEE
+// round-to-nearest operations per instruction, each lane rounding as the
+// scalar operation does). madd2 is a*b + c: one fused multiply-add per lane in
+// the fast variant, a multiply then an add in the exact one.
+RN_DEV float2 lo2(float4 v) { return make_float2(v.x, v.y); }
+RN_DEV float2 hi2(float4 v) { return make_float2(v.z, v.w); }
+RN_DEV float4 cat4(float2 l, float2 h) { return make_float4(l.x, l.y, h.x, h.y); }
+RN_DEV float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+RN_DEV float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }   // a + (-b) == a - b
+RN_DEV float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+RN_DEV float2 madd2(float2 a, float2 b, float2 c) {
+#ifdef RN_FAST
+  return __ffma2_rn(a, b, c);
+#else
+  return __fadd2_rn(__fmul2_rn(a, b), c);
+#endif
+}
+RN_DEV float4 diff4(float4 a, float4 b) { return cat4(sub2(lo2(a), lo2(b)), sub2(hi2(a), hi2(b))); }
 
 RN_DEV float clampf(float x, float a, float b) { return fminf(fmaxf(x, a), b); }
 RN_DEV float mixf(float x, float y, float a) { return x * (1.0f - a) + y * a; }
@@ -161,10 +180,24 @@ RN_DEV void interior_prim(const Grid& g, const float4* __restrict__ A, const flo
 // 2 max(ab, 0) / den with den = a + b, or 1 where |den| <= 1e-30. For ab <= 0
 // the quotient is a zero carrying den's sign, so the division is skipped; the
 // result is the same float for every input that is not NaN.
-RN_DEV float van_leer(float a, float b) {
-  float ab = a * b, den = a + b;
-  den = mixf(den, 1.0f, (1e-30f < fabsf(den)) ? 0.0f : 1.0f);   // step(abs(den), 1e-30)
+// mix(den, 1, step(abs(den), 1e-30)) is den or 1 exactly for every finite den
+// (a select); ab and den come in packed (van_leer4).
+RN_DEV float van_leer_of(float ab, float den) {
+  den = (1e-30f < fabsf(den)) ? den : 1.0f;
   return ab > 0.0f ? fdiv(2.0f * ab, den) : copysignf(0.0f, den);
+}
+RN_DEV float van_leer(float a, float b) { return van_leer_of(a * b, a + b); }
+// Componentwise van_leer(a, b) of two float4 slopes.
+RN_DEV float4 van_leer4(float4 a, float4 b) {
+  const float2 ab0 = mul2(lo2(a), lo2(b)), ab1 = mul2(hi2(a), hi2(b));
+  const float2 dn0 = add2(lo2(a), lo2(b)), dn1 = add2(hi2(a), hi2(b));
+  return make_float4(van_leer_of(ab0.x, dn0.x), van_leer_of(ab0.y, dn0.y), van_leer_of(ab1.x, dn1.x),
+                     van_leer_of(ab1.y, dn1.y));
+}
+// w + h * d per component (h = +-0.5: the MUSCL face values).
+RN_DEV float4 step4(float4 w, float h, float4 d) {
+  const float2 hh = make_float2(h, h);
+  return cat4(madd2(hh, lo2(d), lo2(w)), madd2(hh, hi2(d), hi2(w)));
 }
 RN_DEV float jump_ratio(float a, float b) { return fdiv(fabsf(a - b), fminf(a, b)); }
 
@@ -209,23 +242,20 @@ RN_DEV Flux face_flux(bool DIR_R, float area, float4 w0, float4 b0, float4 w1, f
     if (s3) { w3 = w2; w3.y = -w3.y; b3 = b2; }
     WLw = w1; WLs = b1; WRw = w2; WRs = b2;
     if (P.order2 && area > 0.0f) {
-      float4 dL = make_float4(van_leer(w1.x - w0.x, w2.x - w1.x), van_leer(w1.y - w0.y, w2.y - w1.y),
-                              van_leer(w1.z - w0.z, w2.z - w1.z), van_leer(w1.w - w0.w, w2.w - w1.w));
-      float4 dR = make_float4(van_leer(w2.x - w1.x, w3.x - w2.x), van_leer(w2.y - w1.y, w3.y - w2.y),
-                              van_leer(w2.z - w1.z, w3.z - w2.z), van_leer(w2.w - w1.w, w3.w - w2.w));
-      float4 tL = make_float4(w1.x + 0.5f * dL.x, w1.y + 0.5f * dL.y, w1.z + 0.5f * dL.z, w1.w + 0.5f * dL.w);
-      float4 tR = make_float4(w2.x - 0.5f * dR.x, w2.y - 0.5f * dR.y, w2.z - 0.5f * dR.z, w2.w - 0.5f * dR.w);
+      const float4 d12 = diff4(w2, w1);
+      const float4 dL = van_leer4(diff4(w1, w0), d12), dR = van_leer4(d12, diff4(w3, w2));
+      // w - 0.5 d == w + (-0.5) d in every rounding
+      const float4 tL = step4(w1, 0.5f, dL), tR = step4(w2, -0.5f, dR);
       if (tL.x > 0.0f && tL.w > 0.0f && tR.x > 0.0f && tR.w > 0.0f) {
-        float4 yL = make_float4(van_leer(b1.x - b0.x, b2.x - b1.x), van_leer(b1.y - b0.y, b2.y - b1.y),
-                                van_leer(b1.z - b0.z, b2.z - b1.z), van_leer(b1.w - b0.w, b2.w - b1.w));
-        float4 yR = make_float4(van_leer(b2.x - b1.x, b3.x - b2.x), van_leer(b2.y - b1.y, b3.y - b2.y),
-                                van_leer(b2.z - b1.z, b3.z - b2.z), van_leer(b2.w - b1.w, b3.w - b2.w));
+        const float4 e12 = diff4(b2, b1);
+        const float4 yL = van_leer4(diff4(b1, b0), e12), yR = van_leer4(e12, diff4(b3, b2));
+        const float4 sL = step4(b1, 0.5f, yL), sR = step4(b2, -0.5f, yR);
         WLw = tL;
-        WLs = make_float4(clampf(b1.x + 0.5f * yL.x, 0.0f, 1.0f), clampf(b1.y + 0.5f * yL.y, 0.0f, 1.0f),
-                          clampf(b1.z + 0.5f * yL.z, 0.5f, 100.0f), clampf(b1.w + 0.5f * yL.w, 0.0f, 1.0f));
+        WLs = make_float4(clampf(sL.x, 0.0f, 1.0f), clampf(sL.y, 0.0f, 1.0f), clampf(sL.z, 0.5f, 100.0f),
+                          clampf(sL.w, 0.0f, 1.0f));
         WRw = tR;
-        WRs = make_float4(clampf(b2.x - 0.5f * yR.x, 0.0f, 1.0f), clampf(b2.y - 0.5f * yR.y, 0.0f, 1.0f),
-                          clampf(b2.z - 0.5f * yR.z, 0.5f, 100.0f), clampf(b2.w - 0.5f * yR.w, 0.0f, 1.0f));
+        WRs = make_float4(clampf(sR.x, 0.0f, 1.0f), clampf(sR.y, 0.0f, 1.0f), clampf(sR.z, 0.5f, 100.0f),
+                          clampf(sR.w, 0.0f, 1.0f));
       }
     }
   }

@@ -208,22 +208,21 @@ struct PrimPair {
 template <class T>
 __device__ __forceinline__ PrimPair prefetch_prims(const Grid& g, const float4* __restrict__ A,
                                                    const float4* __restrict__ B, int x0, int y0) {
-  PrimPair p;
-  if (!T::WIDE) return p;                        // load_prims loads them itself
+  PrimPair p = {};
+  if constexpr (T::WIDE) {                       // otherwise load_prims loads them itself
 #pragma unroll
-  for (int u = 0; u < 2; u++) {
-    const int k = threadIdx.x + u * T::NT;
-    p.in[u] = false;
-    p.m[u] = 0;
-    if (k < T::NPT) {
-      int i, j;
-      prim_slot<T>(k, x0, y0, nullptr, g.Nx, i, j);   // a tile slot: the member list is not read
-      p.in[u] = i >= 0 && i < g.Nx && j >= 0 && j < g.Nr;
-      if (p.in[u]) {
-        const int c = j * g.Nx + i;
-        p.a[u] = A[c];
-        p.b[u] = B[c];
-        p.m[u] = g.mask[c];
+    for (int u = 0; u < 2; u++) {
+      const int k = threadIdx.x + u * T::NT;
+      if (k < T::NPT) {
+        int i, j;
+        prim_slot<T>(k, x0, y0, nullptr, g.Nx, i, j);   // a tile slot: the member list is not read
+        p.in[u] = i >= 0 && i < g.Nx && j >= 0 && j < g.Nr;
+        if (p.in[u]) {
+          const int c = j * g.Nx + i;
+          p.a[u] = A[c];
+          p.b[u] = B[c];
+          p.m[u] = g.mask[c];
+        }
       }
     }
   }
