@@ -57,6 +57,8 @@ void free_buffers(rn_solver* h) {
   cudaFree(h->PA[0]);   // base of the 6-plane parcel ring
   for (int p = 0; p < 2; p++) h->PA[p] = h->PB[p] = h->PC[p] = nullptr;
   cudaFree(h->src); cudaFree(h->tab); cudaFree(h->dep); cudaFree(h->key); cudaFree(h->sortTemp);
+  cudaFree(h->acc);
+  h->acc = nullptr;
   cudaFree(h->xoff); cudaFree(h->xcell); cudaFree(h->heavy);
   h->xoff = h->xcell = nullptr;
   h->heavy = nullptr;
@@ -83,6 +85,7 @@ int spray_reset_dev(rn_solver* h) {
     CK(cudaMemsetAsync(h->PB[p], 0, sizeof(float4) * SPRAY_N, h->stream));
     CK(cudaMemsetAsync(h->PC[p], 0, sizeof(float4) * SPRAY_N, h->stream));
   }
+  CK(cudaMemsetAsync(h->acc, 0, sizeof(unsigned long long) * 8 * size_t(h->Nx) * h->Nr, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   h->head = 0;
   h->scur = 0;
@@ -126,6 +129,8 @@ int alloc_buffers(rn_solver* h, int Nx, int Nr) {
   }
   CK(cudaMalloc(&h->src, sizeof(float4) * N));
   CK(cudaMemsetAsync(h->src, 0, sizeof(float4) * N, h->stream));
+  CK(cudaMalloc(&h->acc, sizeof(unsigned long long) * 8 * N));
+  CK(cudaMemsetAsync(h->acc, 0, sizeof(unsigned long long) * 8 * N, h->stream));
   CK(cudaMalloc(&h->tab, sizeof(float4) * 768));
   CK(cudaMemsetAsync(h->tab, 0, sizeof(float4) * 768, h->stream));
   CK(cudaMalloc(&h->dep, sizeof(float4) * SPRAY_N));
@@ -469,6 +474,7 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
       sp.oPA = h->PA[1 - h->scur]; sp.oPB = h->PB[1 - h->scur]; sp.oPC = h->PC[1 - h->scur];
       sp.tab = h->tab; sp.st = stNew;
       sp.key = h->key; sp.val = h->val; sp.dep = h->dep;
+      sp.acc = h->acc + size_t(4) * g.Nx * g.Nr * h->scur;
       sp.head = int(h->head); sp.seed = int(h->seed);
       int launched = 0;
       ProfScope ps(h, RN_K_PARCELS);
@@ -518,6 +524,8 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
       ApplyArgs ap;
       ap.g = g;
       ap.A = h->SA[h->cur]; ap.B = h->SB[h->cur]; ap.src = h->src;
+      ap.acc = h->acc + size_t(4) * g.Nx * g.Nr * h->scur;
+      ap.accNext = h->acc + size_t(4) * g.Nx * g.Nr * (1 - h->scur);
       ap.oA = h->SA[out]; ap.oB = h->SB[out];
       ap.wOut = wOut; ap.finalCfl = 1;
       {
@@ -839,6 +847,9 @@ int rn_autotune(rn_handle h, const rn_params* P, int steps, int* chosen) {
     if (e == cudaSuccess) e = copy_all(false);
     h->cur = cur; h->stepIdx = stepIdx; h->wslot = wslot; h->scur = scur; h->wvalid = wvalid;
     h->stepCount = stepCount; h->head = head; h->seed = seed;
+    // the spray's deposit sums start each step at zero whatever parity it has
+    if (e == cudaSuccess)
+      e = cudaMemsetAsync(h->acc, 0, sizeof(unsigned long long) * 8 * size_t(h->Nx) * h->Nr, h->stream);
   }
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);

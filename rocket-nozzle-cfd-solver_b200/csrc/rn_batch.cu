@@ -254,6 +254,7 @@ int launch_step(rn_batch_t* b, int c, bool withSpray) {
       sp.oPA = h->PA[1 - h->scur]; sp.oPB = h->PB[1 - h->scur]; sp.oPC = h->PC[1 - h->scur];
       sp.tab = h->tab; sp.st = h->stepTex + (1 - si);
       sp.key = h->key; sp.val = h->val; sp.dep = h->dep;
+      sp.acc = h->acc + size_t(4) * h->Nx * h->Nr * h->scur;
       sp.head = int(h->head); sp.seed = int(h->seed);
       int launched = 0;
       if (b->K->spray(sp, b->params[m], h->sortTemp, h->sortTempBytes, h->keyS, h->valS, h->src, b->stream,
@@ -290,6 +291,8 @@ int launch_step(rn_batch_t* b, int c, bool withSpray) {
       ApplyArgs ap;
       ap.g = h->grid();
       ap.A = h->SA[cur]; ap.B = h->SB[cur]; ap.src = h->src;
+      ap.acc = h->acc + size_t(4) * h->Nx * h->Nr * h->scur;
+      ap.accNext = h->acc + size_t(4) * h->Nx * h->Nr * (1 - h->scur);
       ap.oA = h->SA[out]; ap.oB = h->SB[out];
       ap.wOut = h->wmax + (1 - ws);
       ap.finalCfl = 1;
@@ -599,6 +602,10 @@ int rn_batch_autotune(rn_batch b, int steps, int* chosen) {
       if (!toSave) {
         h->cur = s.cur; h->stepIdx = s.stepIdx; h->wslot = s.wslot; h->scur = s.scur; h->wvalid = s.wvalid;
         h->stepCount = s.stepCount; h->head = s.head; h->seed = s.seed;
+        // the spray's deposit sums start each step at zero whatever parity it has
+        cudaError_t e = cudaMemsetAsync(h->acc, 0, sizeof(unsigned long long) * 8 * size_t(h->Nx) * h->Nr,
+                                        h->stream);
+        if (e != cudaSuccess) return e;
       }
     }
     return cudaSuccess;

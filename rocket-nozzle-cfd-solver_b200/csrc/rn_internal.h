@@ -35,6 +35,7 @@ struct rn_solver {
   float* pinned = nullptr;
   size_t pinnedCap = 0, asyncFloats = 0;
   cudaEvent_t asyncEv = nullptr;
+  unsigned long long* acc = nullptr;   // 2 x N x 4 fixed-point spray deposit sums (by step parity scur)
   float4* asyncDev = nullptr;      // device staging of the gathered rectangles
   size_t asyncDevCap = 0;          // float4 capacity of asyncDev
   cudaStream_t copyStream = nullptr;   // the staging buffer's copy to the host

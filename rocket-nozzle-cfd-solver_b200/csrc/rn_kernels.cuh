@@ -75,6 +75,7 @@ struct SprayArgs {
   const float4* tab;                    // 256 x 3 injector table
   const float4* st;
   unsigned* key; unsigned* val; float4* dep;   // deposit records (cell key, parcel index, source)
+  unsigned long long* acc;              // fixed-point deposit sums of this step, 4 per cell (fast variant)
   int head, seed;
 };
 
@@ -82,6 +83,8 @@ struct ApplyArgs {
   Grid g;
   const float4* A; const float4* B;
   const float4* src;
+  const unsigned long long* acc;        // this step's fixed-point deposit sums (fast variant)
+  unsigned long long* accNext;          // the next step's, cleared here cell by cell
   float4* oA; float4* oB;
   unsigned* wOut;
   int finalCfl;

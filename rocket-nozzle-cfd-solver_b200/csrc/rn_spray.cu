@@ -14,6 +14,14 @@
 //   sequentially by one thread: the same order, deterministic, no float atomics.
 // k_apply: FS_SPRAY_APPLY (spray.js:150-179) per cell, with the step's CFL
 //   epilogue when it is the step's last kernel.
+// Fast variant: the deposits go instead into 64-bit fixed-point sums per cell
+//   (integer atomics, so the sums do not depend on the order the parcels
+//   arrive in: deterministic, with no sort). A component is quantised in
+//   steps of 2^-40 of a bound no deposit reaches (mass: the largest parcel
+//   mass mhat * dtMax / 4; momentum: that times 4 vMax), after the float
+//   product x * 2^40 / bound, so each deposit keeps float precision and the
+//   sums hold up to 2^22 bounds. The exact variant keeps the sort and the
+//   float sum in parcel-index order.
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
 #include "rn_kernels.cuh"
@@ -36,6 +44,20 @@ __device__ __forceinline__ bool wall_at(const Grid& g, const float4* A1, const f
   int cx = int(floorf(x)), cy = int(floorf(y));
   if (cx < 0 || cy < 0 || cx >= g.Nx || cy >= g.Nr) return false;
   return g.mask[cy * g.Nx + cx] != 0;          // padded W.x < 0 exactly at solid cells
+}
+
+// Fixed-point scales of the deposit sums (fast variant): 2^40 / bound.
+__device__ __forceinline__ float dep_scale_mass(const rn_params& P) {
+  return ldexpf(1.0f / fmaxf(P.mhat * P.dtMax * 0.25f, 1e-30f), 40);
+}
+__device__ __forceinline__ float dep_scale_mom(const rn_params& P) {
+  return ldexpf(1.0f / fmaxf(P.mhat * P.dtMax * fmaxf(P.vMax, 1.0f), 1e-30f), 40);
+}
+__device__ __forceinline__ unsigned long long to_fixed(float x, float scale) {
+  return (unsigned long long)__float2ll_rn(x * scale);
+}
+__device__ __forceinline__ float from_fixed(unsigned long long v, float scale) {
+  return float(double((long long)v) / double(scale));
 }
 
 __global__ void __launch_bounds__(256) k_parcels(SprayArgs a, rn_params P) {
@@ -145,9 +167,20 @@ __global__ void __launch_bounds__(256) k_parcels(SprayArgs a, rn_params P) {
     key = unsigned(gy * g.Nx + gx);
     dep = make_float4(oC.x * (1.0f - type), oC.x * type, oC.y, oC.z);
   }
+#ifdef RN_FAST
+  if (key != none) {
+    const float sm = dep_scale_mass(P), sp = dep_scale_mom(P);
+    unsigned long long* c = a.acc + 4 * size_t(key);
+    atomicAdd(c + 0, to_fixed(dep.x, sm));
+    atomicAdd(c + 1, to_fixed(dep.y, sm));
+    atomicAdd(c + 2, to_fixed(dep.z, sp));
+    atomicAdd(c + 3, to_fixed(dep.w, sp));
+  }
+#else
   a.key[idx] = key;
   a.val[idx] = unsigned(idx);
   a.dep[idx] = dep;
+#endif
 }
 
 // one thread per run of equal keys: sum in parcel-index order. The run is read
@@ -189,13 +222,24 @@ __global__ void __launch_bounds__(256) k_apply(ApplyArgs a, rn_params P) {
     const int i = k % g.Nx, j = k / g.Nx;
     float4 oA, oB;
     bool fluid = !g.mask[k];
+    // the next step's deposit sums start at zero (both variants keep this up)
+    reinterpret_cast<ulonglong2*>(a.accNext)[2 * k] = make_ulonglong2(0ull, 0ull);
+    reinterpret_cast<ulonglong2*>(a.accNext)[2 * k + 1] = make_ulonglong2(0ull, 0ull);
     if (!fluid) {
       oA = make_float4(P.ambCons[0], P.ambCons[1], P.ambCons[2], P.ambCons[3]);
       oB = make_float4(P.ambB[0], P.ambB[1], P.ambB[2], P.ambB[3]);
     } else {
       float4 gm = g.geoM[k];
       const int kh = (j + iround(gm.y)) * g.Nx + (i + iround(gm.x));
+#ifdef RN_FAST
+      const ulonglong2* c = reinterpret_cast<const ulonglong2*>(a.acc) + 2 * size_t(kh);
+      const ulonglong2 c01 = c[0], c23 = c[1];
+      const float sm = dep_scale_mass(P), sp = dep_scale_mom(P);
+      float4 s = make_float4(from_fixed(c01.x, sm), from_fixed(c01.y, sm), from_fixed(c23.x, sp),
+                             from_fixed(c23.y, sp));
+#else
       float4 s = a.src[kh];
+#endif
       float4 A = a.A[kh], B = a.B[kh];
       float invV = 1.0f / fmaxf(g.geoG[k].x, 1e-6f);
       float dm = s.x + s.y;
@@ -249,6 +293,11 @@ int launch_spray(const SprayArgs& a, const rn_params& P, void* sortTemp, size_t 
                  unsigned* valOut, float4* src, cudaStream_t s, int* launches) {
   const int Ncells = a.g.Nx * a.g.Nr;
   k_parcels<<<SPRAY_N / 256, 256, 0, s>>>(a, P);
+#ifdef RN_FAST
+  (void)sortTemp; (void)sortTempBytes; (void)keyOut; (void)valOut; (void)src; (void)Ncells;
+  *launches += 1;   // the deposits are summed in k_parcels itself
+  return 0;
+#endif
   size_t bytes = sortTempBytes;
   cudaError_t e = cub::DeviceRadixSort::SortPairs(sortTemp, bytes, a.key, keyOut, a.val, valOut, SPRAY_N, 0,
                                                   key_bits(Ncells), s);
