@@ -47,7 +47,7 @@ RN_DEV float fdiv(float a, float b) {
 // Pairs of lanes through Blackwell's packed FP32 instructions (two IEEE
 // round-to-nearest operations per instruction, each lane rounding as the
 // scalar operation does). madd2 is a*b + c: one fused multiply-add per lane in
-// the fast variant, a multiply then an add in the exact one.
+// the fast variant, a multiply then an add (scalar) in the exact one.
 RN_DEV float2 lo2(float4 v) { return make_float2(v.x, v.y); }
 RN_DEV float2 hi2(float4 v) { return make_float2(v.z, v.w); }
 RN_DEV float4 cat4(float2 l, float2 h) { return make_float4(l.x, l.y, h.x, h.y); }
@@ -58,7 +58,9 @@ RN_DEV float2 madd2(float2 a, float2 b, float2 c) {
 #ifdef RN_FAST
   return __ffma2_rn(a, b, c);
 #else
-  return __fadd2_rn(__fmul2_rn(a, b), c);
+  // scalar lanes: a packed multiply followed by a packed add may be fused,
+  // which the exact variant must not do (it is built with -fmad=false)
+  return make_float2(c.x + a.x * b.x, c.y + a.y * b.y);
 #endif
 }
 RN_DEV float4 diff4(float4 a, float4 b) { return cat4(sub2(lo2(a), lo2(b)), sub2(hi2(a), hi2(b))); }
