@@ -167,12 +167,17 @@ int rn_wait(rn_handle h, int timeout_ms);
 /* number of kernels this handle has launched (for launch accounting) */
 int rn_kernel_launches(rn_handle h, long long* out);
 /* Arithmetic of the step kernels. The reference's shaders run in GLSL highp,
- * whose division and square root may be off by up to a few ulp.
+ * whose division and square root may be off by up to a few ulp and whose
+ * compilers may fuse multiply-adds.
  *   RN_PRECISION_FAST (default): the hardware's approximate division and
- *     square root (within 2 ulp), the same latitude;
- *   RN_PRECISION_EXACT: IEEE-rounded division and square root, so the state
- *     reproduces the CPU oracle of the shader passes bit for bit except where
- *     pow/exp/log/sin/cos differ in the last bit. About 1.7x slower.
+ *     square root (within 2 ulp) and fused multiply-adds, the same latitude;
+ *     spray deposits summed per cell in 64-bit fixed point (order-independent);
+ *   RN_PRECISION_EXACT: IEEE-rounded division and square root, no fusion, and
+ *     spray deposits summed in parcel-index order as the reference's blending
+ *     does, so the state reproduces the CPU oracle of the shader passes bit
+ *     for bit except where pow/exp/log/sin/cos differ in the last bit. About
+ *     1.7x slower.
+ * Both are deterministic: the same inputs give the same bits, run to run.
  * No reference counterpart (the reference has one shader build). */
 #define RN_PRECISION_FAST 0
 #define RN_PRECISION_EXACT 1
