@@ -336,6 +336,12 @@ int rn_destroy(rn_handle h) {
   for (auto& p : h->evPending) { cudaEventDestroy(p.second.first); cudaEventDestroy(p.second.second); }
   for (auto e : h->evPool) cudaEventDestroy(e);
   cudaEventDestroy(h->asyncEv);
+  if (h->sprayStream) {
+    cudaStreamSynchronize(h->sprayStream);
+    cudaEventDestroy(h->evSprayFork);
+    cudaEventDestroy(h->evSprayJoin);
+    cudaStreamDestroy(h->sprayStream);
+  }
   if (h->side) {
     cudaStreamSynchronize(h->side);
     cudaEventDestroy(h->evFork);
@@ -477,9 +483,27 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
       sp.acc = h->acc + size_t(4) * g.Nx * g.Nr * h->scur;
       sp.head = int(h->head); sp.seed = int(h->seed);
       int launched = 0;
-      ProfScope ps(h, RN_K_PARCELS);
-      if (h->K->spray(sp, *P, h->sortTemp, h->sortTempBytes, h->keyS, h->valS, h->src, h->stream, &launched) != 0)
-        return fail(RN_ERR_CUDA, "rn_step: deposit sort failed");
+      // The parcel step reads the stage-1 state and writes only the parcel
+      // ring and the deposit sums, which stage 2 + the split step do not
+      // touch: it runs on a stream of its own, beside them, and the apply
+      // waits for it. (Profiling times it on the main stream instead.)
+      cudaStream_t ss = h->stream;
+      if (!h->prof) {
+        if (!h->sprayStream) {
+          CK(cudaStreamCreateWithFlags(&h->sprayStream, cudaStreamNonBlocking));
+          CK(cudaEventCreateWithFlags(&h->evSprayFork, cudaEventDisableTiming));
+          CK(cudaEventCreateWithFlags(&h->evSprayJoin, cudaEventDisableTiming));
+        }
+        CK(cudaEventRecord(h->evSprayFork, h->stream));
+        CK(cudaStreamWaitEvent(h->sprayStream, h->evSprayFork, 0));
+        ss = h->sprayStream;
+      }
+      {
+        ProfScope ps(h, RN_K_PARCELS);
+        if (h->K->spray(sp, *P, h->sortTemp, h->sortTempBytes, h->keyS, h->valS, h->src, ss, &launched) != 0)
+          return fail(RN_ERR_CUDA, "rn_step: deposit sort failed");
+      }
+      if (ss != h->stream) CK(cudaEventRecord(h->evSprayJoin, ss));
       h->launches += launched;
     }
     StageArgs b = a;
@@ -520,6 +544,7 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
     h->launches++;
     h->cur = s2;
     if (inj) {
+      if (!h->prof) CK(cudaStreamWaitEvent(h->stream, h->evSprayJoin, 0));   // the parcel step is done
       const int out = (h->cur + 1) % 3;
       ApplyArgs ap;
       ap.g = g;

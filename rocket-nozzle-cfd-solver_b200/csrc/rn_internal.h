@@ -62,6 +62,8 @@ struct rn_solver {
   int numSMs = 148;
   cudaStream_t side = nullptr;          // runs the heavy tiles' launch beside the main one
   cudaEvent_t evFork = nullptr, evJoin = nullptr;
+  cudaStream_t sprayStream = nullptr;   // runs the parcel step beside stage 2 + the split step
+  cudaEvent_t evSprayFork = nullptr, evSprayJoin = nullptr;
   std::vector<uint8_t> hostMask;
   std::vector<float> hostGeoM;
   // kernels of the selected precision (rn_set_precision)
