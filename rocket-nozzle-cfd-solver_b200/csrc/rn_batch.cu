@@ -75,6 +75,8 @@ struct rn_batch_t {
   int numSMs = 148;
   cudaStream_t side = nullptr;
   cudaEvent_t evFork = nullptr, evJoin = nullptr;
+  cudaStream_t sprayStream = nullptr;   // the members' parcel steps, beside stage 2 + the split step
+  cudaEvent_t evSprayFork = nullptr, evSprayJoin = nullptr;
   const KernelSet* K = nullptr;
   // the graph of one period
   cudaGraphExec_t graph = nullptr;
@@ -241,7 +243,17 @@ int launch_step(rn_batch_t* b, int c, bool withSpray) {
   b->K->batchStage1(b->dInst, b->dBlock, nb, ph, b->tile, b->stream);
   b->launches++;
   if (f.inj && withSpray) {
-    // GPUSpray.step between the two stages (solver.js:865-871), per member
+    // GPUSpray.step between the two stages (solver.js:865-871), per member, on
+    // a stream of its own: the parcel steps read the stage-1 states and write
+    // only the parcel rings and deposit sums, which stage 2 + the split step
+    // do not touch; the applies wait for them
+    if (!b->sprayStream) {
+      BCK(cudaStreamCreateWithFlags(&b->sprayStream, cudaStreamNonBlocking));
+      BCK(cudaEventCreateWithFlags(&b->evSprayFork, cudaEventDisableTiming));
+      BCK(cudaEventCreateWithFlags(&b->evSprayJoin, cudaEventDisableTiming));
+    }
+    BCK(cudaEventRecord(b->evSprayFork, b->stream));
+    BCK(cudaStreamWaitEvent(b->sprayStream, b->evSprayFork, 0));
     for (size_t m = 0; m < b->members.size(); m++) {
       rn_solver* h = b->members[m];
       const BatchInst& d = b->uploaded[m];
@@ -257,11 +269,12 @@ int launch_step(rn_batch_t* b, int c, bool withSpray) {
       sp.acc = h->acc + size_t(4) * h->Nx * h->Nr * h->scur;
       sp.head = int(h->head); sp.seed = int(h->seed);
       int launched = 0;
-      if (b->K->spray(sp, b->params[m], h->sortTemp, h->sortTempBytes, h->keyS, h->valS, h->src, b->stream,
+      if (b->K->spray(sp, b->params[m], h->sortTemp, h->sortTempBytes, h->keyS, h->valS, h->src, b->sprayStream,
                       &launched) != 0)
         return bfail(RN_ERR_CUDA, "rn_batch_step: deposit sort failed");
       b->launches += launched;
     }
+    BCK(cudaEventRecord(b->evSprayJoin, b->sprayStream));
   }
   ph.finalCfl = f.inj ? 0 : 1;
   if (f.phys()) {
@@ -282,6 +295,7 @@ int launch_step(rn_batch_t* b, int c, bool withSpray) {
   }
   b->launches++;
   if (f.inj && withSpray) {
+    BCK(cudaStreamWaitEvent(b->stream, b->evSprayJoin, 0));   // the parcel steps are done
     for (size_t m = 0; m < b->members.size(); m++) {
       rn_solver* h = b->members[m];
       const BatchInst& d = b->uploaded[m];
@@ -388,6 +402,12 @@ int rn_batch_destroy(rn_batch b) {
   cudaEventDestroy(b->evFork);
   cudaEventDestroy(b->evJoin);
   cudaStreamDestroy(b->side);
+  if (b->sprayStream) {
+    cudaStreamSynchronize(b->sprayStream);
+    cudaEventDestroy(b->evSprayFork);
+    cudaEventDestroy(b->evSprayJoin);
+    cudaStreamDestroy(b->sprayStream);
+  }
   cudaStreamDestroy(b->stream);
   delete b;
   return RN_OK;
