@@ -239,3 +239,15 @@ def test_heavy_tiles_run_in_their_own_launch(rn):
     batch.close()
     for g in bigs + [little, ref]:
         g.close()
+
+
+def test_default_tile_by_grid_size(rn):
+    """A new handle takes 14x16 tiles (compiled for 3 blocks per SM) when the
+    grid's 14x16 tiles number at most 3 per SM, and 16x15 otherwise."""
+    import torch
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    for Nx, Nr in ((128, 48), (512, 192), (1024, 384), (2048, 768)):
+        g = rn.GPUSolver(Nx, Nr)
+        tiles = -(-Nx // 14) * -(-Nr // 16)
+        assert g.tile == ("14x16" if tiles <= 3 * sms else "16x15"), (Nx, Nr, g.tile)
+        g.close()
