@@ -153,7 +153,10 @@ int rn_spray_set_parcels(rn_handle h, const float* PA, const float* PB, int head
 /* GPUSpray.reset() (spray.js:242-254) */
 int rn_spray_reset(rn_handle h);
 /* GPUSpray.stats(P) (spray.js:312-320): out = (fuel mass, oxidiser mass,
- * live parcels, mean diameter) */
+ * live parcels, mean diameter). Returns RN_ERR_STATE (once, then clears it) if
+ * a fast-precision deposit since the last call fell outside the fixed-point
+ * range of the deposit sums (a parcel far heavier or faster than
+ * mhat*dtMax/4 and vMax allow) and was clamped. */
 int rn_spray_stats(rn_handle h, double out[4]);
 /* The read-outs the reference computes in JavaScript from column read-backs
  * (exitPerformance simsetup.js:314-337, chamberPerformance 239-250,

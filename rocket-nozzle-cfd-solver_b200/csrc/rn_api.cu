@@ -59,6 +59,8 @@ void free_buffers(rn_solver* h) {
   cudaFree(h->src); cudaFree(h->tab); cudaFree(h->dep); cudaFree(h->key); cudaFree(h->sortTemp);
   cudaFree(h->acc);
   h->acc = nullptr;
+  cudaFree(h->depFlag);
+  h->depFlag = nullptr;
   cudaFree(h->xoff); cudaFree(h->xcell); cudaFree(h->heavy);
   h->xoff = h->xcell = nullptr;
   h->heavy = nullptr;
@@ -110,6 +112,8 @@ int alloc_buffers(rn_solver* h, int Nx, int Nr) {
   CK(cudaMalloc(&h->wallRow, sizeof(float4) * Nx));
   CK(cudaMalloc(&h->stepTex, sizeof(float4) * 2));
   CK(cudaMalloc(&h->wmax, sizeof(unsigned) * 2));
+  CK(cudaMalloc(&h->depFlag, sizeof(unsigned)));
+  CK(cudaMemsetAsync(h->depFlag, 0, sizeof(unsigned), h->stream));
   CK(cudaMalloc(&h->dInt, sizeof(double) * 16));
   CK(cudaMemsetAsync(h->geoA, 0, sizeof(float4) * NF, h->stream));
   CK(cudaMemsetAsync(h->geoG, 0, sizeof(float4) * N, h->stream));
@@ -481,6 +485,7 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
       sp.tab = h->tab; sp.st = stNew;
       sp.key = h->key; sp.val = h->val; sp.dep = h->dep;
       sp.acc = h->acc + size_t(4) * g.Nx * g.Nr * h->scur;
+      sp.depFlag = h->depFlag;
       sp.head = int(h->head); sp.seed = int(h->seed);
       int launched = 0;
       // The parcel step reads the stage-1 state and writes only the parcel
@@ -739,7 +744,15 @@ int rn_spray_stats(rn_handle h, double out[4]) {
   if (!valid(h) || !out) return fail(RN_ERR_ARG, "rn_spray_stats: bad argument");
   std::vector<float4> b(SPRAY_N);
   CK(cudaMemcpyAsync(b.data(), h->PB[h->scur], sizeof(float4) * SPRAY_N, cudaMemcpyDeviceToHost, h->stream));
+  unsigned flag = 0;
+  CK(cudaMemcpyAsync(&flag, h->depFlag, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream));
   CK(cudaStreamSynchronize(h->stream));
+  if (flag) {
+    CK(cudaMemsetAsync(h->depFlag, 0, sizeof(unsigned), h->stream));
+    return fail(RN_ERR_STATE, "rn_spray_stats: a spray deposit left the fixed-point range of the fast "
+                              "precision (a parcel far heavier or faster than mhat*dtMax/4 and vMax allow); "
+                              "the deposits were clamped");
+  }
   double f = 0, o = 0, dS = 0;
   long long n = 0;
   for (int k = 0; k < SPRAY_N; k++) {

@@ -267,6 +267,7 @@ int launch_step(rn_batch_t* b, int c, bool withSpray) {
       sp.tab = h->tab; sp.st = h->stepTex + (1 - si);
       sp.key = h->key; sp.val = h->val; sp.dep = h->dep;
       sp.acc = h->acc + size_t(4) * h->Nx * h->Nr * h->scur;
+      sp.depFlag = h->depFlag;
       sp.head = int(h->head); sp.seed = int(h->seed);
       int launched = 0;
       if (b->K->spray(sp, b->params[m], h->sortTemp, h->sortTempBytes, h->keyS, h->valS, h->src, b->sprayStream,

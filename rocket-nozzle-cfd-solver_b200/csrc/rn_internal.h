@@ -20,6 +20,7 @@ struct rn_solver {
   uint8_t* mask = nullptr;
   float4* stepTex = nullptr;      // [2]
   unsigned* wmax = nullptr;       // [2]
+  unsigned* depFlag = nullptr;    // set when a fast deposit left the fixed-point range
   int stepIdx = 0, wslot = 0;
   bool wvalid = false;
   long long stepCount = 0, launches = 0;

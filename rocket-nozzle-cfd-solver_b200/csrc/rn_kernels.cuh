@@ -76,6 +76,7 @@ struct SprayArgs {
   const float4* st;
   unsigned* key; unsigned* val; float4* dep;   // deposit records (cell key, parcel index, source)
   unsigned long long* acc;              // fixed-point deposit sums of this step, 4 per cell (fast variant)
+  unsigned* depFlag;                    // set when a deposit left the fixed-point range (fast variant)
   int head, seed;
 };
 

@@ -53,8 +53,16 @@ __device__ __forceinline__ float dep_scale_mass(const rn_params& P) {
 __device__ __forceinline__ float dep_scale_mom(const rn_params& P) {
   return ldexpf(1.0f / fmaxf(P.mhat * P.dtMax * fmaxf(P.vMax, 1.0f), 1e-30f), 40);
 }
-__device__ __forceinline__ unsigned long long to_fixed(float x, float scale) {
-  return (unsigned long long)__float2ll_rn(x * scale);
+// |x * scale| stays below 2^46 (64 bounds) or is clamped there and flagged:
+// 65,536 deposits of that size still sum within the 63 bits.
+__device__ __forceinline__ unsigned long long to_fixed(float x, float scale, bool& over) {
+  constexpr float LIM = 70368744177664.0f;   // 2^46
+  float y = x * scale;
+  if (!(fabsf(y) < LIM)) {
+    over = true;
+    y = y < 0.0f ? -LIM : (y > 0.0f ? LIM : 0.0f);   // NaN -> 0
+  }
+  return (unsigned long long)__float2ll_rn(y);
 }
 __device__ __forceinline__ float from_fixed(unsigned long long v, float scale) {
   return float(double((long long)v) / double(scale));
@@ -171,10 +179,12 @@ __global__ void __launch_bounds__(256) k_parcels(SprayArgs a, rn_params P) {
   if (key != none) {
     const float sm = dep_scale_mass(P), sp = dep_scale_mom(P);
     unsigned long long* c = a.acc + 4 * size_t(key);
-    atomicAdd(c + 0, to_fixed(dep.x, sm));
-    atomicAdd(c + 1, to_fixed(dep.y, sm));
-    atomicAdd(c + 2, to_fixed(dep.z, sp));
-    atomicAdd(c + 3, to_fixed(dep.w, sp));
+    bool over = false;
+    atomicAdd(c + 0, to_fixed(dep.x, sm, over));
+    atomicAdd(c + 1, to_fixed(dep.y, sm, over));
+    atomicAdd(c + 2, to_fixed(dep.z, sp, over));
+    atomicAdd(c + 3, to_fixed(dep.w, sp, over));
+    if (over) atomicOr(a.depFlag, 1u);
   }
 #else
   a.key[idx] = key;

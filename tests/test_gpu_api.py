@@ -341,3 +341,27 @@ def test_fast_deposit_sums_are_deterministic(rn):
         out.append(g.readAll())
         g.close()
     assert np.array_equal(out[0]["A"], out[1]["A"]) and np.array_equal(out[0]["B"], out[1]["B"])
+
+
+def test_fast_deposit_out_of_range_is_reported(rn):
+    """A deposit beyond the fixed-point range of the fast deposit sums (here
+    parcels a million times heavier than mhat*dtMax/4) is clamped and reported
+    once by the spray statistics; the next call is clean again."""
+    from rocket_nozzle_cfd_solver_b200 import configs
+    s = rn.build_sim_setup(configs.injector_spray(128, 48)[0])
+    PA, PB, head = configs.prepopulated_parcels(s, 1024)
+    PB = np.array(PB, dtype=np.float32).reshape(-1, 4)
+    live = PB[:, 1] > 0
+    PB[live, 1] = np.float32(1e6 * s.P["spray"]["mhat"] * s.P["dtMax"] / 4)
+    g = rn.GPUSolver(s.Nx, s.Nr)
+    g.setGeometry(s.geo)
+    init = s.initialState()
+    g.setState(init["A"], init["B"])
+    rn.GPUSpray(g).resize()
+    g.spray.setInjector(s.injector)
+    g.spray.setParcels(PA, PB.ravel(), head)
+    g.step(3, s.P)
+    with pytest.raises(rn.RnError, match="fixed-point range"):
+        g.spray.stats()
+    g.spray.stats()                                  # reported once
+    g.close()
