@@ -301,13 +301,14 @@ size_t spray_sort_temp_bytes(int Ncells) {
 
 int launch_spray(const SprayArgs& a, const rn_params& P, void* sortTemp, size_t sortTempBytes, unsigned* keyOut,
                  unsigned* valOut, float4* src, cudaStream_t s, int* launches) {
-  const int Ncells = a.g.Nx * a.g.Nr;
   k_parcels<<<SPRAY_N / 256, 256, 0, s>>>(a, P);
 #ifdef RN_FAST
-  (void)sortTemp; (void)sortTempBytes; (void)keyOut; (void)valOut; (void)src; (void)Ncells;
-  *launches += 1;   // the deposits are summed in k_parcels itself
-  return 0;
-#endif
+  // the deposits are summed in k_parcels itself (fixed point)
+  (void)sortTemp; (void)sortTempBytes; (void)keyOut; (void)valOut; (void)src;
+  *launches += 1;
+#else
+  // the deposit records sorted by cell, each cell's run summed in parcel order
+  const int Ncells = a.g.Nx * a.g.Nr;
   size_t bytes = sortTempBytes;
   cudaError_t e = cub::DeviceRadixSort::SortPairs(sortTemp, bytes, a.key, keyOut, a.val, valOut, SPRAY_N, 0,
                                                   key_bits(Ncells), s);
@@ -315,6 +316,7 @@ int launch_spray(const SprayArgs& a, const rn_params& P, void* sortTemp, size_t 
   cudaMemsetAsync(src, 0, sizeof(float4) * size_t(Ncells), s);
   k_segsum<<<SPRAY_N / 256, 256, 0, s>>>(keyOut, valOut, a.dep, src, unsigned(Ncells));
   *launches += 2;   // own kernels: parcels and segsum (the radix sort's kernels are library code)
+#endif
   return 0;
 }
 
