@@ -50,6 +50,8 @@ int rn_record_cuda(cudaError_t e, const char* what) { return cuda_fail(e, what);
 namespace {
 
 void free_buffers(rn_solver* h) {
+  if (h->stepGraph) cudaGraphExecDestroy(h->stepGraph);   // its launches name these buffers
+  h->stepGraph = nullptr;
   cudaFree(h->SA[0]);   // base of the 6-plane state ring
   for (int s = 0; s < 3; s++) h->SA[s] = h->SB[s] = nullptr;
   cudaFree(h->geoA); cudaFree(h->geoG); cudaFree(h->geoM); cudaFree(h->jw); cudaFree(h->wallRow);
@@ -162,6 +164,8 @@ bool valid(rn_solver* h) { return h != nullptr && h->SA[0] != nullptr; }
 // inside it (a sliver merged across the tile edge). Groups are a host plus the
 // slaves of its slave mask (geoM.z bits 1/2/4/8, cutcell.js:168-174).
 int rn_build_member_lists(rn_solver* h) {
+  if (h->stepGraph) cudaGraphExecDestroy(h->stepGraph);   // its launches name the old lists
+  h->stepGraph = nullptr;
   const int TX = TILE_TX[h->tile], TY = TILE_TY[h->tile];
   const int Nx = h->Nx, Nr = h->Nr, tx = (Nx + TX - 1) / TX, nT = tx * ((Nr + TY - 1) / TY);
   const uint8_t* mask = h->hostMask.data();
@@ -449,130 +453,210 @@ int rn_get_state(rn_handle h, float* A, float* B) {
   return RN_OK;
 }
 
+}  // extern "C"
+
+namespace {
+constexpr int STEP_PERIOD = 6;   // 3 ring shifts x 2 step-info parities
+
+// One time step of handle h (the body of step(n, P), solver.js:849-891).
+int step_once(rn_solver* h, const rn_params* P) {
+  const Grid g = h->grid();
+  const bool phys = P->visc || P->chem, inj = P->inj != 0;
+  const int s0 = h->cur, s1 = (h->cur + 1) % 3, s2 = (h->cur + 2) % 3;
+  unsigned* wIn = h->wmax + h->wslot;
+  unsigned* wOut = h->wmax + (1 - h->wslot);
+  if (!h->wvalid) {
+    int rc = rn_ensure_wave_speed(h);
+    if (rc != RN_OK) return rc;
+  }
+  float4* stPrev = h->stepTex + h->stepIdx;
+  float4* stNew = h->stepTex + (1 - h->stepIdx);
+  StageArgs a;
+  a.g = g;
+  a.A = h->SA[s0]; a.B = h->SB[s0]; a.A0 = h->SA[s0]; a.B0 = h->SB[s0];
+  a.oA = h->SA[s1]; a.oB = h->SB[s1];
+  a.stPrev = stPrev; a.stNew = stNew; a.wIn = wIn; a.wOut = wOut;
+  a.finalCfl = 0;
+  a.xoff = h->xoff; a.xcell = h->xcell; a.maxX = h->maxX;
+  {
+    ProfScope ps(h, RN_K_STAGE1);
+    h->K->stage1(a, *P, h->tile, h->stream);
+  }
+  h->launches++;
+  if (inj) {
+    SprayArgs sp;
+    sp.g = g;
+    sp.A1 = h->SA[s1]; sp.B1 = h->SB[s1];
+    sp.PA = h->PA[h->scur]; sp.PB = h->PB[h->scur];
+    sp.oPA = h->PA[1 - h->scur]; sp.oPB = h->PB[1 - h->scur]; sp.oPC = h->PC[1 - h->scur];
+    sp.tab = h->tab; sp.st = stNew;
+    sp.key = h->key; sp.val = h->val; sp.dep = h->dep;
+    sp.acc = h->acc + size_t(4) * g.Nx * g.Nr * h->scur;
+    sp.depFlag = h->depFlag;
+    sp.head = int(h->head); sp.seed = int(h->seed);
+    int launched = 0;
+    // The parcel step reads the stage-1 state and writes only the parcel
+    // ring and the deposit sums, which stage 2 + the split step do not
+    // touch: it runs on a stream of its own, beside them, and the apply
+    // waits for it. (Profiling times it on the main stream instead.)
+    cudaStream_t ss = h->stream;
+    if (!h->prof) {
+      if (!h->sprayStream) {
+        CK(cudaStreamCreateWithFlags(&h->sprayStream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&h->evSprayFork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&h->evSprayJoin, cudaEventDisableTiming));
+      }
+      CK(cudaEventRecord(h->evSprayFork, h->stream));
+      CK(cudaStreamWaitEvent(h->sprayStream, h->evSprayFork, 0));
+      ss = h->sprayStream;
+    }
+    {
+      ProfScope ps(h, RN_K_PARCELS);
+      if (h->K->spray(sp, *P, h->sortTemp, h->sortTempBytes, h->keyS, h->valS, h->src, ss, &launched) != 0)
+        return fail(RN_ERR_CUDA, "rn_step: deposit sort failed");
+    }
+    if (ss != h->stream) CK(cudaEventRecord(h->evSprayJoin, ss));
+    h->launches += launched;
+  }
+  StageArgs b = a;
+  b.A = h->SA[s1]; b.B = h->SB[s1]; b.A0 = h->SA[s0]; b.B0 = h->SB[s0];
+  b.oA = h->SA[s2]; b.oB = h->SB[s2];
+  b.finalCfl = (!phys && !inj) ? 1 : 0;
+  if (phys) {
+    // stage 2 + split step in one kernel; its output replaces the stage-2 slot
+    PhysArgs p;
+    p.g = g;
+    p.A1 = h->SA[s1]; p.B1 = h->SB[s1]; p.A2 = h->SA[s2]; p.B2 = h->SB[s2];
+    p.oA = h->SA[s2]; p.oB = h->SB[s2];
+    p.st = stNew; p.wOut = wOut; p.finalCfl = inj ? 0 : 1;
+    p.xoff = h->xoff; p.xcell = h->xcell; p.maxX = h->maxX;
+    ProfScope ps(h, RN_K_STAGE2_PHYSICS);
+    const int nTiles = int(h->hostXoff.size()) - 1;
+    if (h->nHeavy > 0 && nTiles > SPLIT_BLOCKS_PER_SM * h->numSMs) {
+      // the few tiles with long member lists on the side stream, at the same time
+      if (!h->side) {
+        CK(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&h->evFork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&h->evJoin, cudaEventDisableTiming));
+      }
+      CK(cudaEventRecord(h->evFork, h->stream));
+      CK(cudaStreamWaitEvent(h->side, h->evFork, 0));
+      h->K->stage2phys(b, p, *P, h->tile, h->heavy, h->nHeavy, false, h->side);
+      CK(cudaEventRecord(h->evJoin, h->side));
+      h->K->stage2phys(b, p, *P, h->tile, nullptr, h->nHeavy, true, h->stream);
+      CK(cudaStreamWaitEvent(h->stream, h->evJoin, 0));
+      h->launches++;
+    } else {
+      h->K->stage2phys(b, p, *P, h->tile, nullptr, 0, false, h->stream);
+    }
+  } else {
+    ProfScope ps(h, RN_K_STAGE2);
+    h->K->stage2(b, *P, h->tile, h->stream);
+  }
+  h->launches++;
+  h->cur = s2;
+  if (inj) {
+    if (!h->prof) CK(cudaStreamWaitEvent(h->stream, h->evSprayJoin, 0));   // the parcel step is done
+    const int out = (h->cur + 1) % 3;
+    ApplyArgs ap;
+    ap.g = g;
+    ap.A = h->SA[h->cur]; ap.B = h->SB[h->cur]; ap.src = h->src;
+    ap.acc = h->acc + size_t(4) * g.Nx * g.Nr * h->scur;
+    ap.accNext = h->acc + size_t(4) * g.Nx * g.Nr * (1 - h->scur);
+    ap.oA = h->SA[out]; ap.oB = h->SB[out];
+    ap.wOut = wOut; ap.finalCfl = 1;
+    {
+      ProfScope ps(h, RN_K_APPLY);
+      h->K->apply(ap, *P, h->stream);
+    }
+    h->launches++;
+    h->cur = out;
+    h->scur = 1 - h->scur;
+    h->head = (h->head + 4) % SPRAY_N;
+    h->seed = h->seed + 1u;
+  }
+  h->stepIdx = 1 - h->stepIdx;
+  h->wslot = 1 - h->wslot;
+  h->wvalid = true;
+  h->s1last = s1;
+  h->stepCount++;
+  return RN_OK;
+}
+
+// Whether the handle's 6-step graph can replay the next steps with P: the
+// kernels, launch shapes, buffers and parameter block it was captured with.
+bool graph_matches(const rn_solver* h, const rn_params* P) {
+  return h->stepGraph && h->graphK == h->K && h->graphTile == h->tile && h->graphMaxX == h->maxX &&
+         h->graphHeavy == h->nHeavy && h->graphBase == h->SA[0] && h->graphXoff == h->xoff &&
+         std::memcmp(&h->graphP, P, sizeof(rn_params)) == 0;
+}
+void drop_step_graph(rn_solver* h) {
+  if (h->stepGraph) cudaGraphExecDestroy(h->stepGraph);
+  h->stepGraph = nullptr;
+}
+}  // namespace
+
+extern "C" {
+
 int rn_step(rn_handle h, int n, const rn_params* P) {
   if (!valid(h) || !P || n < 0) return fail(RN_ERR_ARG, "rn_step: bad argument");
   if (h->batch) return fail(RN_ERR_STATE, "rn_step: the handle is stepped by a batch");
-  const Grid g = h->grid();
-  const bool phys = P->visc || P->chem, inj = P->inj != 0;
-  for (int k = 0; k < n; k++) {
-    const int s0 = h->cur, s1 = (h->cur + 1) % 3, s2 = (h->cur + 2) % 3;
-    unsigned* wIn = h->wmax + h->wslot;
-    unsigned* wOut = h->wmax + (1 - h->wslot);
-    if (!h->wvalid) {
-      int rc = rn_ensure_wave_speed(h);
+  const bool inj = P->inj != 0;
+  int done = 0;
+  // Without sprays the launch sequence repeats every 6 steps (3 ring shifts x
+  // 2 step-info parities): whole periods replay from a CUDA graph captured
+  // from the handle's own launches (not while profiling, which brackets each
+  // kernel with events).
+  if (!inj && !h->prof && n >= 2 * STEP_PERIOD) {
+    while (done < n && (!h->wvalid || (h->stepGraph && graph_matches(h, P) &&
+                                       (h->cur != h->graphCur || h->stepIdx != h->graphStepIdx ||
+                                        h->wslot != h->graphWslot)))) {
+      int rc = step_once(h, P);
       if (rc != RN_OK) return rc;
+      done++;
     }
-    float4* stPrev = h->stepTex + h->stepIdx;
-    float4* stNew = h->stepTex + (1 - h->stepIdx);
-    StageArgs a;
-    a.g = g;
-    a.A = h->SA[s0]; a.B = h->SB[s0]; a.A0 = h->SA[s0]; a.B0 = h->SB[s0];
-    a.oA = h->SA[s1]; a.oB = h->SB[s1];
-    a.stPrev = stPrev; a.stNew = stNew; a.wIn = wIn; a.wOut = wOut;
-    a.finalCfl = 0;
-    a.xoff = h->xoff; a.xcell = h->xcell; a.maxX = h->maxX;
-    {
-      ProfScope ps(h, RN_K_STAGE1);
-      h->K->stage1(a, *P, h->tile, h->stream);
-    }
-    h->launches++;
-    if (inj) {
-      SprayArgs sp;
-      sp.g = g;
-      sp.A1 = h->SA[s1]; sp.B1 = h->SB[s1];
-      sp.PA = h->PA[h->scur]; sp.PB = h->PB[h->scur];
-      sp.oPA = h->PA[1 - h->scur]; sp.oPB = h->PB[1 - h->scur]; sp.oPC = h->PC[1 - h->scur];
-      sp.tab = h->tab; sp.st = stNew;
-      sp.key = h->key; sp.val = h->val; sp.dep = h->dep;
-      sp.acc = h->acc + size_t(4) * g.Nx * g.Nr * h->scur;
-      sp.depFlag = h->depFlag;
-      sp.head = int(h->head); sp.seed = int(h->seed);
-      int launched = 0;
-      // The parcel step reads the stage-1 state and writes only the parcel
-      // ring and the deposit sums, which stage 2 + the split step do not
-      // touch: it runs on a stream of its own, beside them, and the apply
-      // waits for it. (Profiling times it on the main stream instead.)
-      cudaStream_t ss = h->stream;
-      if (!h->prof) {
-        if (!h->sprayStream) {
-          CK(cudaStreamCreateWithFlags(&h->sprayStream, cudaStreamNonBlocking));
-          CK(cudaEventCreateWithFlags(&h->evSprayFork, cudaEventDisableTiming));
-          CK(cudaEventCreateWithFlags(&h->evSprayJoin, cudaEventDisableTiming));
-        }
-        CK(cudaEventRecord(h->evSprayFork, h->stream));
-        CK(cudaStreamWaitEvent(h->sprayStream, h->evSprayFork, 0));
-        ss = h->sprayStream;
+    if (n - done >= STEP_PERIOD && !graph_matches(h, P)) {
+      drop_step_graph(h);
+      if (h->nHeavy > 0 && !h->side) {   // the heavy tiles' stream exists before the capture
+        CK(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&h->evFork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&h->evJoin, cudaEventDisableTiming));
       }
-      {
-        ProfScope ps(h, RN_K_PARCELS);
-        if (h->K->spray(sp, *P, h->sortTemp, h->sortTempBytes, h->keyS, h->valS, h->src, ss, &launched) != 0)
-          return fail(RN_ERR_CUDA, "rn_step: deposit sort failed");
-      }
-      if (ss != h->stream) CK(cudaEventRecord(h->evSprayJoin, ss));
-      h->launches += launched;
+      const int cur = h->cur, stepIdx = h->stepIdx, wslot = h->wslot, s1last = h->s1last;
+      const long long stepCount = h->stepCount, launches = h->launches;
+      cudaGraph_t gr = nullptr;
+      CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+      int rc = RN_OK;
+      for (int k = 0; k < STEP_PERIOD && rc == RN_OK; k++) rc = step_once(h, P);
+      cudaError_t e = cudaStreamEndCapture(h->stream, &gr);
+      const long long perPeriod = h->launches - launches;
+      h->cur = cur; h->stepIdx = stepIdx; h->wslot = wslot; h->s1last = s1last;
+      h->stepCount = stepCount; h->launches = launches;
+      if (rc != RN_OK) { if (gr) cudaGraphDestroy(gr); return rc; }
+      if (e != cudaSuccess) { if (gr) cudaGraphDestroy(gr); return cuda_fail(e, "rn_step: graph capture"); }
+      e = cudaGraphInstantiate(&h->stepGraph, gr, 0);
+      cudaGraphDestroy(gr);
+      if (e != cudaSuccess) { h->stepGraph = nullptr; return cuda_fail(e, "rn_step: graph instantiate"); }
+      h->graphK = h->K; h->graphTile = h->tile; h->graphMaxX = h->maxX; h->graphHeavy = h->nHeavy;
+      h->graphBase = h->SA[0]; h->graphXoff = h->xoff; h->graphP = *P;
+      h->graphCur = cur; h->graphStepIdx = stepIdx; h->graphWslot = wslot;
+      h->graphLaunches = perPeriod;
     }
-    StageArgs b = a;
-    b.A = h->SA[s1]; b.B = h->SB[s1]; b.A0 = h->SA[s0]; b.B0 = h->SB[s0];
-    b.oA = h->SA[s2]; b.oB = h->SB[s2];
-    b.finalCfl = (!phys && !inj) ? 1 : 0;
-    if (phys) {
-      // stage 2 + split step in one kernel; its output replaces the stage-2 slot
-      PhysArgs p;
-      p.g = g;
-      p.A1 = h->SA[s1]; p.B1 = h->SB[s1]; p.A2 = h->SA[s2]; p.B2 = h->SB[s2];
-      p.oA = h->SA[s2]; p.oB = h->SB[s2];
-      p.st = stNew; p.wOut = wOut; p.finalCfl = inj ? 0 : 1;
-      p.xoff = h->xoff; p.xcell = h->xcell; p.maxX = h->maxX;
-      ProfScope ps(h, RN_K_STAGE2_PHYSICS);
-      const int nTiles = int(h->hostXoff.size()) - 1;
-      if (h->nHeavy > 0 && nTiles > SPLIT_BLOCKS_PER_SM * h->numSMs) {
-        // the few tiles with long member lists on the side stream, at the same time
-        if (!h->side) {
-          CK(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
-          CK(cudaEventCreateWithFlags(&h->evFork, cudaEventDisableTiming));
-          CK(cudaEventCreateWithFlags(&h->evJoin, cudaEventDisableTiming));
-        }
-        CK(cudaEventRecord(h->evFork, h->stream));
-        CK(cudaStreamWaitEvent(h->side, h->evFork, 0));
-        h->K->stage2phys(b, p, *P, h->tile, h->heavy, h->nHeavy, false, h->side);
-        CK(cudaEventRecord(h->evJoin, h->side));
-        h->K->stage2phys(b, p, *P, h->tile, nullptr, h->nHeavy, true, h->stream);
-        CK(cudaStreamWaitEvent(h->stream, h->evJoin, 0));
-        h->launches++;
-      } else {
-        h->K->stage2phys(b, p, *P, h->tile, nullptr, 0, false, h->stream);
+    if (graph_matches(h, P) && h->wvalid && h->cur == h->graphCur && h->stepIdx == h->graphStepIdx &&
+        h->wslot == h->graphWslot) {
+      while (n - done >= STEP_PERIOD) {
+        CK(cudaGraphLaunch(h->stepGraph, h->stream));
+        // a period leaves the ring, step info and wave-speed slot where they were
+        h->s1last = (h->cur + 1 + 2 * (STEP_PERIOD - 1)) % 3;
+        h->stepCount += STEP_PERIOD;
+        h->launches += h->graphLaunches;
+        done += STEP_PERIOD;
       }
-    } else {
-      ProfScope ps(h, RN_K_STAGE2);
-      h->K->stage2(b, *P, h->tile, h->stream);
     }
-    h->launches++;
-    h->cur = s2;
-    if (inj) {
-      if (!h->prof) CK(cudaStreamWaitEvent(h->stream, h->evSprayJoin, 0));   // the parcel step is done
-      const int out = (h->cur + 1) % 3;
-      ApplyArgs ap;
-      ap.g = g;
-      ap.A = h->SA[h->cur]; ap.B = h->SB[h->cur]; ap.src = h->src;
-      ap.acc = h->acc + size_t(4) * g.Nx * g.Nr * h->scur;
-      ap.accNext = h->acc + size_t(4) * g.Nx * g.Nr * (1 - h->scur);
-      ap.oA = h->SA[out]; ap.oB = h->SB[out];
-      ap.wOut = wOut; ap.finalCfl = 1;
-      {
-        ProfScope ps(h, RN_K_APPLY);
-        h->K->apply(ap, *P, h->stream);
-      }
-      h->launches++;
-      h->cur = out;
-      h->scur = 1 - h->scur;
-      h->head = (h->head + 4) % SPRAY_N;
-      h->seed = h->seed + 1u;
-    }
-    h->stepIdx = 1 - h->stepIdx;
-    h->wslot = 1 - h->wslot;
-    h->wvalid = true;
-    h->s1last = s1;
-    h->stepCount++;
+  }
+  for (; done < n; done++) {
+    int rc = step_once(h, P);
+    if (rc != RN_OK) return rc;
   }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail(e, "rn_step launch");

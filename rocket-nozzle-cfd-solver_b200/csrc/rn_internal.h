@@ -63,6 +63,15 @@ struct rn_solver {
   int numSMs = 148;
   cudaStream_t side = nullptr;          // runs the heavy tiles' launch beside the main one
   cudaEvent_t evFork = nullptr, evJoin = nullptr;
+  // the 6-step period of non-spray steps as a CUDA graph, and what it was
+  // captured with (rn_step replays it only while all of that still holds)
+  cudaGraphExec_t stepGraph = nullptr;
+  const void* graphK = nullptr;
+  int graphTile = -1, graphMaxX = -1, graphHeavy = -1, graphCur = -1, graphStepIdx = -1, graphWslot = -1;
+  const void* graphBase = nullptr;
+  const void* graphXoff = nullptr;
+  rn_params graphP;
+  long long graphLaunches = 0;
   cudaStream_t sprayStream = nullptr;   // runs the parcel step beside stage 2 + the split step
   cudaEvent_t evSprayFork = nullptr, evSprayJoin = nullptr;
   std::vector<uint8_t> hostMask;
