@@ -63,6 +63,8 @@ void free_buffers(rn_solver* h) {
   h->acc = nullptr;
   cudaFree(h->depFlag);
   h->depFlag = nullptr;
+  cudaFree(h->dHS);
+  h->dHS = nullptr;
   cudaFree(h->xoff); cudaFree(h->xcell); cudaFree(h->heavy);
   h->xoff = h->xcell = nullptr;
   h->heavy = nullptr;
@@ -115,6 +117,7 @@ int alloc_buffers(rn_solver* h, int Nx, int Nr) {
   CK(cudaMalloc(&h->stepTex, sizeof(float4) * 2));
   CK(cudaMalloc(&h->wmax, sizeof(unsigned) * 2));
   CK(cudaMalloc(&h->depFlag, sizeof(unsigned)));
+  CK(cudaMalloc(&h->dHS, sizeof(unsigned) * 2));
   CK(cudaMemsetAsync(h->depFlag, 0, sizeof(unsigned), h->stream));
   CK(cudaMalloc(&h->dInt, sizeof(double) * 16));
   CK(cudaMemsetAsync(h->geoA, 0, sizeof(float4) * NF, h->stream));
@@ -494,6 +497,7 @@ int step_once(rn_solver* h, const rn_params* P) {
     sp.acc = h->acc + size_t(4) * g.Nx * g.Nr * h->scur;
     sp.depFlag = h->depFlag;
     sp.head = int(h->head); sp.seed = int(h->seed);
+    sp.hs = h->hsOnDevice ? h->dHS : nullptr;
     int launched = 0;
     // The parcel step reads the stage-1 state and writes only the parcel
     // ring and the deposit sums, which stage 2 + the split step do not
@@ -565,6 +569,7 @@ int step_once(rn_solver* h, const rn_params* P) {
     ap.accNext = h->acc + size_t(4) * g.Nx * g.Nr * (1 - h->scur);
     ap.oA = h->SA[out]; ap.oB = h->SB[out];
     ap.wOut = wOut; ap.finalCfl = 1;
+    ap.hsNext = h->hsOnDevice ? h->dHS : nullptr;
     {
       ProfScope ps(h, RN_K_APPLY);
       h->K->apply(ap, *P, h->stream);
@@ -598,39 +603,58 @@ void drop_step_graph(rn_solver* h) {
 
 extern "C" {
 
+__global__ void k_set_hs(unsigned* hs, unsigned head, unsigned seed) {
+  hs[0] = head;
+  hs[1] = seed;
+}
+
 int rn_step(rn_handle h, int n, const rn_params* P) {
   if (!valid(h) || !P || n < 0) return fail(RN_ERR_ARG, "rn_step: bad argument");
   if (h->batch) return fail(RN_ERR_STATE, "rn_step: the handle is stepped by a batch");
   const bool inj = P->inj != 0;
   int done = 0;
-  // Without sprays the launch sequence repeats every 6 steps (3 ring shifts x
-  // 2 step-info parities): whole periods replay from a CUDA graph captured
-  // from the handle's own launches (not while profiling, which brackets each
-  // kernel with events).
-  if (!inj && !h->prof && n >= 2 * STEP_PERIOD) {
-    while (done < n && (!h->wvalid || (h->stepGraph && graph_matches(h, P) &&
-                                       (h->cur != h->graphCur || h->stepIdx != h->graphStepIdx ||
-                                        h->wslot != h->graphWslot)))) {
+  // The launch sequence repeats: every 6 steps without sprays (3 ring shifts x
+  // 2 step-info parities), every 2 with them (the state ring stays put, the
+  // step info, wave-speed slot and parcel ring alternate; the ring head and
+  // seed are then read and advanced on the device). Whole periods replay from
+  // a CUDA graph captured from the handle's own launches (not while
+  // profiling, which brackets each kernel with events).
+  const int period = inj ? 2 : STEP_PERIOD;
+  auto at_start = [&]() {
+    return h->cur == h->graphCur && h->stepIdx == h->graphStepIdx && h->wslot == h->graphWslot &&
+           (!inj || h->scur == h->graphScur);
+  };
+  if (!h->prof && n >= 2 * period) {
+    while (done < n && (!h->wvalid || (graph_matches(h, P) && !at_start()))) {
       int rc = step_once(h, P);
       if (rc != RN_OK) return rc;
       done++;
     }
-    if (n - done >= STEP_PERIOD && !graph_matches(h, P)) {
+    if (n - done >= period && !graph_matches(h, P)) {
       drop_step_graph(h);
-      if (h->nHeavy > 0 && !h->side) {   // the heavy tiles' stream exists before the capture
+      if (h->nHeavy > 0 && !h->side) {   // the helper streams exist before the capture
         CK(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
         CK(cudaEventCreateWithFlags(&h->evFork, cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&h->evJoin, cudaEventDisableTiming));
       }
-      const int cur = h->cur, stepIdx = h->stepIdx, wslot = h->wslot, s1last = h->s1last;
+      if (inj && !h->sprayStream) {
+        CK(cudaStreamCreateWithFlags(&h->sprayStream, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&h->evSprayFork, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&h->evSprayJoin, cudaEventDisableTiming));
+      }
+      const int cur = h->cur, stepIdx = h->stepIdx, wslot = h->wslot, s1last = h->s1last, scur = h->scur;
+      const uint32_t head = h->head, seed = h->seed;
       const long long stepCount = h->stepCount, launches = h->launches;
       cudaGraph_t gr = nullptr;
+      h->hsOnDevice = inj;
       CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
       int rc = RN_OK;
-      for (int k = 0; k < STEP_PERIOD && rc == RN_OK; k++) rc = step_once(h, P);
+      for (int k = 0; k < period && rc == RN_OK; k++) rc = step_once(h, P);
       cudaError_t e = cudaStreamEndCapture(h->stream, &gr);
+      h->hsOnDevice = false;
       const long long perPeriod = h->launches - launches;
-      h->cur = cur; h->stepIdx = stepIdx; h->wslot = wslot; h->s1last = s1last;
+      h->cur = cur; h->stepIdx = stepIdx; h->wslot = wslot; h->s1last = s1last; h->scur = scur;
+      h->head = head; h->seed = seed;
       h->stepCount = stepCount; h->launches = launches;
       if (rc != RN_OK) { if (gr) cudaGraphDestroy(gr); return rc; }
       if (e != cudaSuccess) { if (gr) cudaGraphDestroy(gr); return cuda_fail(e, "rn_step: graph capture"); }
@@ -639,18 +663,26 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
       if (e != cudaSuccess) { h->stepGraph = nullptr; return cuda_fail(e, "rn_step: graph instantiate"); }
       h->graphK = h->K; h->graphTile = h->tile; h->graphMaxX = h->maxX; h->graphHeavy = h->nHeavy;
       h->graphBase = h->SA[0]; h->graphXoff = h->xoff; h->graphP = *P;
-      h->graphCur = cur; h->graphStepIdx = stepIdx; h->graphWslot = wslot;
+      h->graphCur = cur; h->graphStepIdx = stepIdx; h->graphWslot = wslot; h->graphScur = scur;
       h->graphLaunches = perPeriod;
+      h->graphPeriod = period;
     }
-    if (graph_matches(h, P) && h->wvalid && h->cur == h->graphCur && h->stepIdx == h->graphStepIdx &&
-        h->wslot == h->graphWslot) {
-      while (n - done >= STEP_PERIOD) {
+    if (graph_matches(h, P) && h->graphPeriod == period && h->wvalid && at_start() && n - done >= period) {
+      if (inj) {   // the ring head and seed the graph's parcel kernels read
+        k_set_hs<<<1, 1, 0, h->stream>>>(h->dHS, h->head, h->seed);
+        h->launches++;
+      }
+      while (n - done >= period) {
         CK(cudaGraphLaunch(h->stepGraph, h->stream));
-        // a period leaves the ring, step info and wave-speed slot where they were
-        h->s1last = (h->cur + 1 + 2 * (STEP_PERIOD - 1)) % 3;
-        h->stepCount += STEP_PERIOD;
+        // a period leaves the rings, step info and wave-speed slot where they were
+        h->s1last = inj ? (h->cur + 1) % 3 : (h->cur + 1 + 2 * (period - 1)) % 3;
+        if (inj) {
+          h->head = (h->head + 4u * uint32_t(period)) % SPRAY_N;
+          h->seed = h->seed + uint32_t(period);
+        }
+        h->stepCount += period;
         h->launches += h->graphLaunches;
-        done += STEP_PERIOD;
+        done += period;
       }
     }
   }

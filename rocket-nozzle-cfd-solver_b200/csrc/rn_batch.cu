@@ -269,6 +269,7 @@ int launch_step(rn_batch_t* b, int c, bool withSpray) {
       sp.acc = h->acc + size_t(4) * h->Nx * h->Nr * h->scur;
       sp.depFlag = h->depFlag;
       sp.head = int(h->head); sp.seed = int(h->seed);
+      sp.hs = nullptr;
       int launched = 0;
       if (b->K->spray(sp, b->params[m], h->sortTemp, h->sortTempBytes, h->keyS, h->valS, h->src, b->sprayStream,
                       &launched) != 0)
@@ -311,6 +312,7 @@ int launch_step(rn_batch_t* b, int c, bool withSpray) {
       ap.oA = h->SA[out]; ap.oB = h->SB[out];
       ap.wOut = h->wmax + (1 - ws);
       ap.finalCfl = 1;
+      ap.hsNext = nullptr;
       b->K->apply(ap, b->params[m], b->stream);
       b->launches++;
       h->scur = 1 - h->scur;

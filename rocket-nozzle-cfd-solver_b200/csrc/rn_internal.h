@@ -72,6 +72,9 @@ struct rn_solver {
   const void* graphXoff = nullptr;
   rn_params graphP;
   long long graphLaunches = 0;
+  int graphScur = -1, graphPeriod = 0;
+  unsigned* dHS = nullptr;   // the spray ring's (head, seed) on the device, for graph-replayed spray steps
+  bool hsOnDevice = false;   // step_once launches read and advance dHS (while capturing)
   cudaStream_t sprayStream = nullptr;   // runs the parcel step beside stage 2 + the split step
   cudaEvent_t evSprayFork = nullptr, evSprayJoin = nullptr;
   std::vector<uint8_t> hostMask;

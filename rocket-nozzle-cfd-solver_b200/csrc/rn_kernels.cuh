@@ -78,6 +78,7 @@ struct SprayArgs {
   unsigned long long* acc;              // fixed-point deposit sums of this step, 4 per cell (fast variant)
   unsigned* depFlag;                    // set when a deposit left the fixed-point range (fast variant)
   int head, seed;
+  const unsigned* hs;                   // if set: (head, seed) read here instead (graph replay)
 };
 
 struct ApplyArgs {
@@ -89,6 +90,7 @@ struct ApplyArgs {
   float4* oA; float4* oB;
   unsigned* wOut;
   int finalCfl;
+  unsigned* hsNext;                     // if set: (head, seed) advanced by one step here (graph replay)
 };
 
 // One instance of a batch: its buffers, where it stood in its state ring and

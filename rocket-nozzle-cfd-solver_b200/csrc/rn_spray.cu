@@ -74,10 +74,11 @@ __global__ void __launch_bounds__(256) k_parcels(SprayArgs a, rn_params P) {
   const Grid g = a.g;
   const float dt = a.st->x;
   float4 pa = a.PA[idx], pb = a.PB[idx];
-  int rel = idx - a.head;
+  const int head = a.hs ? int(a.hs[0]) : a.head;
+  int rel = idx - head;
   if (rel < 0) rel += SPRAY_N;
   float4 oA, oB, oC;
-  const uint32_t seed = uint32_t(a.seed);
+  const uint32_t seed = a.hs ? a.hs[1] : uint32_t(a.seed);
   if (rel < SPRAY_PER_STEP) {
     // new parcel; whatever the old one still carried goes to the gas
     uint32_t id = uint32_t(idx) ^ (seed * 2654435761u);
@@ -228,6 +229,13 @@ __global__ void __launch_bounds__(256) k_apply(ApplyArgs a, rn_params P) {
   const int N = g.Nx * g.Nr;
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   float wcell = 0.0f;
+  // the ring head and seed of the next step (GPUSpray.step's bookkeeping,
+  // spray.js:295-296), when they live on the device; k_parcels of this step
+  // has read them (it runs before this kernel)
+  if (a.hsNext && k == 0) {
+    a.hsNext[0] = (a.hsNext[0] + unsigned(SPRAY_PER_STEP)) % unsigned(SPRAY_N);
+    a.hsNext[1] = a.hsNext[1] + 1u;
+  }
   if (k < N) {
     const int i = k % g.Nx, j = k / g.Nx;
     float4 oA, oB;
