@@ -365,3 +365,30 @@ def test_fast_deposit_out_of_range_is_reported(rn):
         g.spray.stats()
     g.spray.stats()                                  # reported once
     g.close()
+
+
+@pytest.mark.parametrize("name", ["viscous", "spray"])
+def test_graph_replay_matches_single_steps(rn, name):
+    """step(n, P) replays a captured period of its launches (6 steps, 2 with
+    sprays) as a CUDA graph for n >= 2 periods; stepping one step per call never
+    does. Both reach the same bits, across an ambient rescale (which moves the
+    ring phase) and a changed parameter block (which re-captures)."""
+    s, _ = golden_case(rn, name)
+    P2 = dict(s.P)
+    P2["cfl"] = s.P["cfl"] * 0.9
+    outs = []
+    for graphed in (False, True):
+        g = gpu(rn, s, 0)
+        plan = [(13, s.P), (17, P2)]
+        for i, (n, P) in enumerate(plan):
+            if graphed:
+                g.step(n, P)
+            else:
+                for _ in range(n):
+                    g.step(1, P)
+            if i == 0:
+                g.rescaleAmbient(0.9, 1.0, 0.0, P2)
+        outs.append((g.readAll(), g.readStepInfo()))
+        g.close()
+    (a, sa), (b, sb) = outs
+    assert np.array_equal(a["A"], b["A"]) and np.array_equal(a["B"], b["B"]) and np.array_equal(sa, sb)
