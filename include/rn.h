@@ -114,7 +114,11 @@ int rn_set_state(rn_handle h, const float* A, const float* B);
 /* readAll() (solver.js:1075) */
 int rn_get_state(rn_handle h, float* A, float* B);
 /* step(n, P) (solver.js:849-891), including GPUSpray.step (spray.js:256-297)
- * when P->inj is set: queued on the handle's stream */
+ * when P->inj is set: queued on the handle's stream. For n of two periods or
+ * more (12 steps, 4 with sprays) the handle captures one period of its
+ * launches into a CUDA graph and replays it (the same kernels, the same
+ * bits); not while profiling, and not while the caller is itself capturing
+ * the handle's stream. */
 int rn_step(rn_handle h, int n, const rn_params* P);
 /* rescaleAmbient(fp, fT, du, P) (solver.js:998-1010) */
 int rn_rescale_ambient(rn_handle h, float fp, float fT, float du, const rn_params* P);

@@ -624,7 +624,11 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
     return h->cur == h->graphCur && h->stepIdx == h->graphStepIdx && h->wslot == h->graphWslot &&
            (!inj || h->scur == h->graphScur);
   };
-  if (!h->prof && n >= 2 * period) {
+  // (nor when the caller is capturing the handle's stream into a graph of its
+  // own: the launches then go into that graph as they are)
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(h->stream, &cs) != cudaSuccess) cs = cudaStreamCaptureStatusNone;
+  if (!h->prof && cs == cudaStreamCaptureStatusNone && n >= 2 * period) {
     while (done < n && (!h->wvalid || (graph_matches(h, P) && !at_start()))) {
       int rc = step_once(h, P);
       if (rc != RN_OK) return rc;
