@@ -207,7 +207,7 @@ def test_spray_parcels_match_oracle(rn, oracle):
 
 
 def test_full_size_viscous_plume(rn, oracle):
-    """BASELINE's viscous plume grid (512 x 192), 100 steps."""
+    """The bench's viscous plume grid (512 x 192), 100 steps."""
     from rocket_nozzle_cfd_solver_b200 import configs
     s = rn.build_sim_setup(configs.viscous_plume()[0])
     g = gpu(rn, s, 100)
