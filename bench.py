@@ -127,8 +127,9 @@ def make_setup(rn):
     return rn.build_sim_setup(cfg)
 
 
-def cpu_sample(setup, seconds=12.0, threads=None):
-    """Oracle (FP32 port of the shader passes) on the host cores: cell-updates/s."""
+def cpu_sample(setup, seconds=12.0, threads=None, start=2):
+    """Oracle (FP32 port of the shader passes) on the host cores: cell-updates/s,
+    timed from time step `start` (reached untimed) of the solve."""
     oracle = ge.load_oracle()
     threads = threads or os.cpu_count() or 1
     oracle.set_threads(threads)
@@ -136,7 +137,7 @@ def cpu_sample(setup, seconds=12.0, threads=None):
     o.setGeometry(setup.geo)
     init = setup.initialState()
     o.setState(init["A"], init["B"])
-    o.step(2, setup.P)
+    o.step(start, setup.P)
     steps, t0 = 0, time.perf_counter()
     while True:
         o.step(1, setup.P)
@@ -149,6 +150,12 @@ def cpu_sample(setup, seconds=12.0, threads=None):
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the CPU oracle on all host cores, timed over the
+    stretch of the solve where our arm's timed region starts (our arm times
+    time steps W*SOLVER_STEPS .. (W+K)*SOLVER_STEPS after W warm-up bench
+    steps; the oracle steps untimed to W*SOLVER_STEPS, then times K steps,
+    one per bench step: the per-step cost drifts a few percent as the plume
+    develops)."""
     if rank != 0:
         return
     rn = ge.load_package()
@@ -160,19 +167,21 @@ def run_reference(args, rank, world):
     o.setGeometry(setup.geo)
     init = setup.initialState()
     o.setState(init["A"], init["B"])
-    for _ in range(args.warmup):
-        o.step(1, setup.P)
+    start = args.warmup * SOLVER_STEPS
+    o.step(start, setup.P)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         o.step(1, setup.P)
     el = time.perf_counter() - t0
     cells = setup.Nx * setup.Nr
     value = cells * args.steps / el
-    sample = f"{args.steps} time steps of the {setup.Nx}x{setup.Nr} viscous plume, one per bench step"
+    sample = (f"time steps {start}..{start + args.steps} of the {setup.Nx}x{setup.Nr} viscous plume (the start of "
+              f"our arm's timed window, steps {start}..{start + args.steps * SOLVER_STEPS}), one per bench step")
     line = {"impl": "reference", "metric": "cell-updates/s", "value": value, "unit": "cell-updates/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "solver_steps_per_bench_step": 1,
+                       "window": [start, start + args.steps],
                        "implementation": "CPU oracle: C++ restatement of the reference's WebGL2 passes "
                                          "(the reference itself needs a graphics stack)"},
             "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": threads, "kind": "port",
@@ -327,10 +336,11 @@ def run_ours(args, rank, world, local_rank):
     cpu = None
     fp64 = run_fp64_check(args) if world == 1 and not args.no_cpu else None
     if world == 1 and not args.no_cpu:
-        cv, threads, nst, el = cpu_sample(setup)
+        start = args.warmup * SOLVER_STEPS
+        cv, threads, nst, el = cpu_sample(setup, start=start)
         cpu = {"value": cv, "unit": "cell-updates/s", "cores": threads, "kind": "port",
-               "sample": f"{nst} time steps of the {setup.Nx}x{setup.Nr} viscous plume from its initial state "
-                         f"({el:.1f} s, FP32 oracle, OpenMP over rows)"}
+               "sample": f"{nst} time steps of the {setup.Nx}x{setup.Nr} viscous plume from step {start}, the "
+                         f"start of the timed window ({el:.1f} s, FP32 oracle, OpenMP over rows)"}
     line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -437,6 +447,10 @@ def run_batched(args, local_rank, rank=0, world=1):
     peak, src = measured_peak()
     bpc = BYTES_PER_CELL["stage1"] + BYTES_PER_CELL["stage2_physics"]
     instances = int(replicas.sum_over_ranks(len(setups), dev))
+    classes = None
+    if world == 1:
+        classes = [class_solves(rn, size, n, fp64_samples=(2 if size[0] <= 256 else 0))
+                   for size, n in CLASS_COUNTS.items()]
     return {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "instances": instances,
             "ranks": world, "cells_this_rank": my_cells,
             "achieved_gbs": value * bpc / 1e9, "bytes_per_cell_step": bpc, "frac": value * bpc / 1e9 / peak,
@@ -447,7 +461,98 @@ def run_batched(args, local_rank, rank=0, world=1):
             "one_at_a_time": {"value": single, "unit": "cell-updates/s", "wall_value":
                               cells * nsteps * rounds / single_wall, "rounds": rounds},
             "speedup_vs_one_at_a_time": value / single, "fp64_readouts_finite": finite,
-            "setup_s": t_setup, "l2": "state ~1 GB > L2: no flush"}
+            "setup_s": t_setup, "l2": "state ~1 GB > L2: no flush",
+            "solves_per_class": classes}
+
+
+CLASS_COUNTS = {(128, 48): 64, (256, 96): 64, (512, 192): 8, (1024, 384): 4}
+
+
+def class_solves(rn, size, count, t_end_s=2e-3, K=60, seed=64, fp64_samples=0):
+    """Solves/s of `count` seeded nozzles of one grid class (configs.
+    batched_instance: expansion 4-40, p0 10-100 bar, gamma 1.2/1.4, altitude
+    0-30 km, viscous), each run to 2 ms of simulated time (checked every K
+    steps), one at a time (rn_step per solve, in turn) and batched (one
+    SolverBatch; a member leaves the batch when it reaches 2 ms). Host clock
+    around the stepping, setups excluded; final exit thrust and mass flow of
+    every solve; the first `fp64_samples` solves checked against the oracle
+    run in FP64 for the same steps (the FP64-scheme error)."""
+    import torch
+    from rocket_nozzle_cfd_solver_b200 import configs
+    rng = np.random.default_rng(seed + size[0])
+    setups = [rn.build_sim_setup(configs.batched_instance(rng, size)) for _ in range(count)]
+
+    def start(s):
+        g = rn.GPUSolver(s.Nx, s.Nr)
+        g.setGeometry(s.geo)
+        init = s.initialState()
+        g.setState(init["A"], init["B"])
+        return g
+
+    def finish(g, s):
+        col = g.readColumn(s.iExit)
+        perf = rn.exit_performance(s, col)
+        return {"steps": g.stepCount, "F": perf["F"], "mdot": perf["mdot"], "A": g.readAll()}
+
+    # one at a time
+    hs = [start(s) for s in setups]
+    ps = [rn.params_from_P(s.P) for s in setups]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    single = []
+    for g, s, p in zip(hs, setups, ps):
+        t_end = t_end_s / s.tScale
+        while float(g.readStepInfo()[2]) < t_end:
+            g.step(K, p)
+        single.append(g.stepCount)
+    t_single = time.perf_counter() - t0
+    single_res = [finish(g, s) for g, s in zip(hs, setups)]
+    for g in hs:
+        g.close()
+    # batched
+    hs = [start(s) for s in setups]
+    batch = rn.SolverBatch()
+    for g, s in zip(hs, setups):
+        batch.add(g, s.P)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    left = list(range(count))
+    while left:
+        batch.step(K)
+        batch.sync()
+        for q in list(left):
+            if float(hs[q].readStepInfo()[2]) >= t_setups_end(setups[q], t_end_s):
+                batch.remove(hs[q])
+                left.remove(q)
+    t_batch = time.perf_counter() - t0
+    batch.close()
+    batch_res = [finish(g, s) for g, s in zip(hs, setups)]
+    for g in hs:
+        g.close()
+    same = all(a["steps"] == b["steps"] and np.array_equal(a["A"]["A"], b["A"]["A"])
+               for a, b in zip(single_res, batch_res))
+    fp64 = []
+    if fp64_samples:
+        oracle = ge.load_oracle()
+        oracle.set_threads(os.cpu_count() or 1)
+        for s, r in list(zip(setups, batch_res))[:fp64_samples]:
+            o = oracle.OracleSolver(s.Nx, s.Nr, fp64=True)
+            o.setGeometry(s.geo)
+            init = s.initialState()
+            o.setState(init["A"], init["B"])
+            o.step(r["steps"], s.P)
+            op = rn.exit_performance(s, exit_column(o.readAll(), s))
+            o.close()
+            fp64.append({"steps": r["steps"], "thrust_rel_err": abs(r["F"] - op["F"]) / max(abs(op["F"]), 1e-30),
+                         "mdot_rel_err": abs(r["mdot"] - op["mdot"]) / max(abs(op["mdot"]), 1e-30)})
+    steps = [r["steps"] for r in batch_res]
+    return {"grid": f"{size[0]}x{size[1]}", "solves": count, "steps_to_2ms": [min(steps), max(steps)],
+            "one_at_a_time_solves_per_s": count / t_single, "batched_solves_per_s": count / t_batch,
+            "speedup": t_single / t_batch, "results_identical": same, "fp64_error": fp64}
+
+
+def t_setups_end(s, t_end_s):
+    return t_end_s / s.tScale
 
 
 def run_large_grid(args):
@@ -500,49 +605,61 @@ def run_large_grid(args):
             "frac": rate * bpc / 1e9 / peak, "kernels": kern, "tile": tile}
 
 
-def run_spray(args, local_rank):
-    """Injector + spray chamber (coaxial methalox at 70 bar, 512 x 192, the
-    65,536-parcel ring spawning 4 parcels per step from the injector table):
-    device time per step with the parcel update, the deterministic deposit
-    sort, the two stages + split step and the source apply; parcel-steps/s
-    counts every ring slot each step (the reference's spray pass draws all
-    65,536 fragments)."""
+def run_spray(args, local_rank, t_end_s=2e-3, chunk=50):
+    """Injector + spray chamber, the configuration as stated: coaxial methalox
+    at 70 bar (preset injCoax), 512 x 192, the 65,536-slot parcel ring
+    pre-populated with 65,536 seeded parcels (configs.prepopulated_parcels:
+    lognormal diameters, median 60 um, sigma 0.4, on the injector elements,
+    30 / 120 m/s +-10 %) and spawning 4 per step from the injector table, run
+    to about 2 ms of simulated time. Device time of the stepping (CUDA events
+    around each chunk of steps; the chunk boundaries read the step info to
+    stop at 2 ms). Reported beside each other: live parcel-steps/s (live
+    parcels summed over the steps, counted on the device, per second) and
+    slot-steps/s (all 65,536 ring slots every step, what the reference's spray
+    pass draws)."""
     import torch
     rn = ge.load_package()
-    from rocket_nozzle_cfd_solver_b200.configs import injector_spray
-    s = rn.build_sim_setup(injector_spray(512, 192)[0])
+    from rocket_nozzle_cfd_solver_b200 import configs
+    s = rn.build_sim_setup(configs.injector_spray(512, 192)[0])
+    PA, PB, head = configs.prepopulated_parcels(s, 65536)
     g = rn.GPUSolver(s.Nx, s.Nr)
     g.setGeometry(s.geo)
     init = s.initialState()
     g.setState(init["A"], init["B"])
     rn.GPUSpray(g).resize()
     g.spray.setInjector(s.injector)
+    g.spray.setParcels(PA, PB, head)
+    live0 = g.spray.stats()["parcels"]
     p = rn.params_from_P(s.P)
-    n = 50
-    for _ in range(max(args.warmup, 1)):
-        g.step(n, p)
-    g.sync()
     st = torch.cuda.ExternalStream(g.stream())
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with torch.cuda.stream(st):
-        e0.record(st)
-    g.step(n * args.steps, p)
-    with torch.cuda.stream(st):
-        e1.record(st)
-    g.sync()
-    ms = e0.elapsed_time(e1)
-    steps = n * args.steps
+    t_end = t_end_s / s.tScale
+    ms, steps, t = 0.0, 0, 0.0
+    while t < t_end:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(st):
+            e0.record(st)
+        g.step(chunk, p)
+        with torch.cuda.stream(st):
+            e1.record(st)
+        t = float(g.readStepInfo()[2])
+        ms += e0.elapsed_time(e1)
+        steps += chunk
+    live_steps = g.spray.parcelSteps()
+    live = g.spray.stats()["parcels"]
     g.profile(True)
-    g.step(n, p)
+    g.step(chunk, p)
     prof = g.profileRead()
     g.profile(False)
     total = sum(v[0] for v in prof.values())
-    live = g.spray.stats()["parcels"]
     g.close()
-    return {"workload": "injector + spray chamber 512x192 (injCoax, methalox 70 bar), 65,536-parcel ring",
-            "cell_updates_per_s": s.Nx * s.Nr * steps / (ms * 1e-3),
-            "parcel_steps_per_s": 65536 * steps / (ms * 1e-3), "steps_per_s": steps / (ms * 1e-3),
-            "live_parcels_at_end": live, "ms_per_step": ms / steps,
+    sec = ms * 1e-3
+    return {"workload": "injector + spray chamber 512x192 (injCoax, methalox 70 bar), ring pre-populated with "
+                        "65,536 parcels (lognormal d, median 60 um, sigma 0.4), about 2 ms simulated",
+            "steps": steps, "simulated_ms": t * s.tScale * 1e3, "ms_per_step": ms / steps,
+            "steps_per_s": steps / sec, "cell_updates_per_s": s.Nx * s.Nr * steps / sec,
+            "live_parcel_steps_per_s": live_steps / sec, "slot_steps_per_s": 65536 * steps / sec,
+            "live_parcel_steps": live_steps, "live_parcels_at_start": live0, "live_parcels_at_end": live,
+            "deposit": "fixed-point sums per cell (fast precision; scale from the ring's largest mass and speed)",
             "share": {k: round(v[0] / total, 4) for k, v in prof.items() if v[1]}}
 
 
@@ -634,33 +751,38 @@ def run_serving(args):
     """Serving: Poisson arrivals of whole solves (stop at a density-residual
     drop of 1e-4 or 2 ms of simulated time) into the continuous-batching
     SolveServer, against the same arrivals served one solve at a time
-    (max_active=1, the plain form)."""
+    (max_active=1, the plain form), at every rate of --serve-rates (the
+    configuration's 1-50 req/s). The same seeded request mix at every rate."""
     rn = ge.load_package()
     t0 = time.perf_counter()
     reqs = serving_requests(rn, args.serve_requests)
     t_setup = time.perf_counter() - t0
-    rng = np.random.default_rng(11)
-    rate = args.serve_rate
-    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
-    arrivals -= arrivals[0]
     K, drop, t_end = 60, 1e-4, 2e-3
-    served, st = serve_once(rn, reqs, arrivals, 0, K, drop, t_end, args.serve_max_cells)
-    plain, _ = serve_once(rn, reqs, arrivals, 1, K, drop, t_end)
-    same = all(a["integrals"] == b["integrals"] and a["steps"] == b["steps"] for a, b in zip(served, plain))
-    status = {}
-    for r in served:
-        status[r["status"]] = status.get(r["status"], 0) + 1
-    cells = sum(s.Nx * s.Nr * r["steps"] for (_, s, _), r in zip(reqs, served))
-    sv, pl = latency_summary(served), latency_summary(plain)
-    return {"metric": "solves/s", "value": sv["solves_per_s"], "unit": "solves/s", "rate_per_s": rate,
+    sweep = []
+    for rate in (float(r) for r in args.serve_rates.split(",")):
+        rng = np.random.default_rng(11)
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
+        arrivals -= arrivals[0]
+        served, st = serve_once(rn, reqs, arrivals, 0, K, drop, t_end, args.serve_max_cells)
+        plain, _ = serve_once(rn, reqs, arrivals, 1, K, drop, t_end)
+        same = all(a["integrals"] == b["integrals"] and a["steps"] == b["steps"] for a, b in zip(served, plain))
+        status = {}
+        for r in served:
+            status[r["status"]] = status.get(r["status"], 0) + 1
+        cells = sum(s.Nx * s.Nr * r["steps"] for (_, s, _), r in zip(reqs, served))
+        sv, pl = latency_summary(served), latency_summary(plain)
+        sweep.append({"rate_per_s": rate, "solves_per_s": sv["solves_per_s"], "p50_ms": sv["p50_ms"],
+                      "p99_ms": sv["p99_ms"], "makespan_s": sv["makespan_s"],
+                      "cell_updates_per_s": cells / sv["makespan_s"], "status": status, "ticks": st["ticks"],
+                      "one_at_a_time": pl, "speedup_solves_per_s": sv["solves_per_s"] / pl["solves_per_s"],
+                      "results_identical_in_mix_and_alone": same})
+    top = max(sweep, key=lambda e: e["rate_per_s"])
+    return {"metric": "solves/s", "value": top["solves_per_s"], "unit": "solves/s", "rate_per_s": top["rate_per_s"],
             "requests": len(reqs), "spray_requests": sum(1 for k, _, _ in reqs if k == "spray"),
             "spray_parcels": [int((np.asarray(pc[1]).reshape(-1, 4)[:, 1] > 0).sum()) for k, _, pc in reqs if pc],
+            "grids": [f"{s.Nx}x{s.Nr}" for _, s, _ in reqs],
             "stop": "density residual drop 1e-4 or 2 ms simulated", "check_every": K,
-            "max_active_cells": args.serve_max_cells,
-            "p50_ms": sv["p50_ms"], "p99_ms": sv["p99_ms"], "makespan_s": sv["makespan_s"],
-            "cell_updates_per_s": cells / sv["makespan_s"], "status": status, "ticks": st["ticks"],
-            "one_at_a_time": pl, "speedup_solves_per_s": sv["solves_per_s"] / pl["solves_per_s"],
-            "results_identical_in_mix_and_alone": same, "setup_s": t_setup}
+            "max_active_cells": args.serve_max_cells, "sweep": sweep, "setup_s": t_setup}
 
 
 def main():
@@ -683,8 +805,10 @@ def main():
                     help="skip the 4096x1536 HBM-resident sweep point and the spray chamber leg")
     ap.add_argument("--only-spray", action="store_true",
                     help="run only the spray chamber leg and print its JSON object (for profiling)")
-    ap.add_argument("--serve-requests", type=int, default=24, help="requests of the serving leg (0: skip)")
-    ap.add_argument("--serve-rate", type=float, default=5.0, help="Poisson arrival rate of the serving leg (1/s)")
+    ap.add_argument("--serve-requests", type=int, default=12,
+                    help="requests of the serving leg at each arrival rate (0: skip)")
+    ap.add_argument("--serve-rates", default="1,2,5,10,20,50",
+                    help="Poisson arrival rates of the serving leg (1/s), comma-separated")
     ap.add_argument("--serve-max-cells", type=int, default=2000000,
                     help="admission cap on the grid cells the server steps at once (0: memory budget only)")
     args = ap.parse_args()

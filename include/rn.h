@@ -156,6 +156,11 @@ int rn_spray_build_injector(rn_handle h, const rn_injector_element* el, int n);
 int rn_spray_set_parcels(rn_handle h, const float* PA, const float* PB, int head);
 /* GPUSpray.reset() (spray.js:242-254) */
 int rn_spray_reset(rn_handle h);
+/* Live parcels summed over every spray step since the ring was last set
+ * (rn_spray_reset, rn_spray_set_parcels, rn_set_state): the parcel-steps the
+ * handle has simulated. Counted on the device by the parcel kernel; blocks
+ * until the handle's queued steps are done. No reference counterpart. */
+int rn_spray_parcel_steps(rn_handle h, long long* out);
 /* GPUSpray.stats(P) (spray.js:312-320): out = (fuel mass, oxidiser mass,
  * live parcels, mean diameter). Returns RN_ERR_STATE (once, then clears it) if
  * a fast-precision deposit since the last call fell outside the fixed-point
@@ -383,7 +388,9 @@ typedef struct {
   rn_integrals_out integrals;       /* FP64 read-outs of the final state */
 } rn_solve_result;
 typedef struct {
-  long long queued, active, finished, bytes_used, bytes_budget, ticks, admitted, failed;
+  long long queued, active, finished, bytes_used, bytes_budget, ticks, admitted;
+  long long failed;     /* 1 once the CUDA context broke: every solve then failed and submit refuses */
+  long long evicted;    /* solves that failed alone (setup, allocation, a non-finite residual) */
 } rn_serve_status;
 int rn_server_default_opts(rn_server_opts* opts);
 int rn_server_create(const rn_server_opts* opts, rn_server* out);
@@ -398,6 +405,18 @@ int rn_serve_wait(rn_server s, long long id, int timeout_ms, rn_solve_result* re
 int rn_serve_stats(rn_server s, rn_serve_status* out);
 /* device bytes the server charges a solve of an Nx x Nr grid against its budget */
 int rn_solve_bytes(int Nx, int Nr, long long* bytes);
+/* Failure isolation: a solve whose own work fails (its setup or upload at
+ * admission, an allocation, a non-finite residual) is evicted alone with
+ * RN_SOLVE_FAILED, its memory freed, and every other solve carries on
+ * unchanged. A class batch whose step fails while the CUDA context stays
+ * usable evicts that class's solves. Only a broken context (a sticky CUDA
+ * error) fails every solve and latches `failed`.
+ * Host-side fault injection for tests (nothing faults on the GPU): the next
+ * request submitted to s fails as a device allocation would (RN_ERR_NOMEM)
+ * at its admission (RN_INJECT_ADMIT) or in its first tick (RN_INJECT_TICK). */
+#define RN_INJECT_ADMIT 1
+#define RN_INJECT_TICK 2
+int rn_serve_inject(rn_server s, int where);
 
 /* the handle's CUDA stream (a cudaStream_t), so a caller can order its own
  * work (timing events, cache flushes) with the handle's kernels */
@@ -431,8 +450,12 @@ int rn_profile_read(rn_handle h, double ms[RN_NKERNELS], long long launches[RN_N
  * array (per-row terms of up to RN_STATIC_MAX_ROWS rows, 256 KiB, held by
  * every GPU that loads the library until exit); Nr above that limit is
  * rejected with RN_ERR_ARG. The first call on a device looks up the array's
- * device address; make it before any stream capture. Calls share the array:
- * calls that overlap on the GPU race. Blocks until `out` is filled. */
+ * device address; make it before any stream capture. The call cannot be made
+ * while its stream is being captured (it ends with a blocking read-back):
+ * it then returns RN_ERR_ARG and queues nothing. The looked-up address does
+ * not survive cudaDeviceReset: do not call it after a reset in the same
+ * process. Calls share the array: calls that overlap on the GPU race.
+ * Blocks until `out` is filled. */
 #define RN_STATIC_MAX_ROWS 4096
 int rn_integrals_static(const float* A, const float* B, const float* geoA, const uint8_t* mask, int Nx, int Nr,
                         const float* stepinfo, const rn_integral_spec* spec, rn_integrals_out* out, void* stream);

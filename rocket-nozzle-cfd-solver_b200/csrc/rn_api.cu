@@ -55,6 +55,8 @@ void free_buffers(rn_solver* h) {
   cudaFree(h->SA[0]);   // base of the 6-plane state ring
   for (int s = 0; s < 3; s++) h->SA[s] = h->SB[s] = nullptr;
   cudaFree(h->geoA); cudaFree(h->geoG); cudaFree(h->geoM); cudaFree(h->jw); cudaFree(h->wallRow);
+  cudaFree(h->maskP); cudaFree(h->dMaps); cudaFree(h->errFlag);
+  h->maskP = nullptr; h->dMaps = nullptr; h->errFlag = nullptr;
   cudaFree(h->mask); cudaFree(h->stepTex); cudaFree(h->wmax); cudaFree(h->dInt);
   cudaFree(h->PA[0]);   // base of the 6-plane parcel ring
   for (int p = 0; p < 2; p++) h->PA[p] = h->PB[p] = h->PC[p] = nullptr;
@@ -63,6 +65,10 @@ void free_buffers(rn_solver* h) {
   h->acc = nullptr;
   cudaFree(h->depFlag);
   h->depFlag = nullptr;
+  cudaFree(h->depBound);
+  h->depBound = nullptr;
+  cudaFree(h->liveSteps);
+  h->liveSteps = nullptr;
   cudaFree(h->dHS);
   h->dHS = nullptr;
   cudaFree(h->xoff); cudaFree(h->xcell); cudaFree(h->heavy);
@@ -92,6 +98,8 @@ int spray_reset_dev(rn_solver* h) {
     CK(cudaMemsetAsync(h->PC[p], 0, sizeof(float4) * SPRAY_N, h->stream));
   }
   CK(cudaMemsetAsync(h->acc, 0, sizeof(unsigned long long) * 8 * size_t(h->Nx) * h->Nr, h->stream));
+  if (h->depBound) CK(cudaMemsetAsync(h->depBound, 0, sizeof(unsigned) * 4, h->stream));
+  if (h->liveSteps) CK(cudaMemsetAsync(h->liveSteps, 0, sizeof(unsigned long long), h->stream));
   CK(cudaStreamSynchronize(h->stream));
   h->head = 0;
   h->scur = 0;
@@ -119,6 +127,10 @@ int alloc_buffers(rn_solver* h, int Nx, int Nr) {
   CK(cudaMalloc(&h->depFlag, sizeof(unsigned)));
   CK(cudaMalloc(&h->dHS, sizeof(unsigned) * 2));
   CK(cudaMemsetAsync(h->depFlag, 0, sizeof(unsigned), h->stream));
+  CK(cudaMalloc(&h->depBound, sizeof(unsigned) * 4));
+  CK(cudaMemsetAsync(h->depBound, 0, sizeof(unsigned) * 4, h->stream));
+  CK(cudaMalloc(&h->liveSteps, sizeof(unsigned long long)));
+  CK(cudaMemsetAsync(h->liveSteps, 0, sizeof(unsigned long long), h->stream));
   CK(cudaMalloc(&h->dInt, sizeof(double) * 16));
   CK(cudaMemsetAsync(h->geoA, 0, sizeof(float4) * NF, h->stream));
   CK(cudaMemsetAsync(h->geoG, 0, sizeof(float4) * N, h->stream));
@@ -128,6 +140,17 @@ int alloc_buffers(rn_solver* h, int Nx, int Nr) {
   CK(cudaMemsetAsync(h->wallRow, 0, sizeof(float4) * Nx, h->stream));
   CK(cudaMemsetAsync(h->stepTex, 0, sizeof(float4) * 2, h->stream));
   CK(cudaMemsetAsync(h->wmax, 0, sizeof(unsigned) * 2, h->stream));
+  // halo copies: pitched mask, error word, tensor maps
+  h->maskPitch = (Nx + 15) / 16 * 16;
+  CK(cudaMalloc(&h->maskP, size_t(h->maskPitch) * Nr));
+  CK(cudaMemsetAsync(h->maskP, 0, size_t(h->maskPitch) * Nr, h->stream));
+  CK(cudaMalloc(&h->errFlag, sizeof(unsigned)));
+  CK(cudaMemsetAsync(h->errFlag, 0, sizeof(unsigned), h->stream));
+  CK(cudaMalloc(&h->dMaps, sizeof(TileMaps) * NTILES));
+  {
+    const int rcm = rn_build_tile_maps(h);
+    if (rcm != RN_OK) return rcm;
+  }
   // spray ring and deposit records
   float4* pr = nullptr;
   CK(cudaMalloc(&pr, sizeof(float4) * SPRAY_N * 6));
@@ -161,7 +184,63 @@ int alloc_buffers(rn_solver* h, int Nx, int Nr) {
 
 bool valid(rn_solver* h) { return h != nullptr && h->SA[0] != nullptr; }
 
+// cuTensorMapEncodeTiled from the driver (the library links the runtime only).
+using EncodeTiledFn = decltype(&cuTensorMapEncodeTiled);
+EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
+
 }  // namespace
+
+// The halo copies of a tile shape with PX x PY halo cells: each float4 plane
+// as a (4 Nx) x Nr float32 tensor with a (4 PX) x PY box; the mask as an
+// Nx x Nr byte tensor (rows maskPitch bytes apart) with an MW x PY box.
+// Boxes that reach past the grid read zeros there.
+int rn_build_tile_maps(rn_solver* h) {
+  const EncodeTiledFn enc = encode_tiled();
+  if (!enc) return fail(RN_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the CUDA driver");
+  const int Nx = h->Nx, Nr = h->Nr;
+  std::vector<TileMaps> maps(NTILES);
+  const cuuint32_t estr[2] = {1, 1};
+  for (int t = 0; t < NTILES; t++) {
+    const int PX = TILE_TX[t] + 4, PY = TILE_TY[t] + 4;
+    const cuuint64_t pdim[2] = {cuuint64_t(4) * Nx, cuuint64_t(Nr)};
+    const cuuint64_t pstride[1] = {cuuint64_t(16) * Nx};
+    const cuuint32_t pbox[2] = {cuuint32_t(4 * PX), cuuint32_t(PY)};
+    for (int s = 0; s < 6; s++) {
+      CUtensorMap* m = s < 3 ? &maps[t].a[s] : &maps[t].b[s - 3];
+      void* base = s < 3 ? static_cast<void*>(h->SA[s]) : static_cast<void*>(h->SB[s - 3]);
+      CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, pdim, pstride, pbox, estr,
+                       CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS) return fail(RN_ERR_CUDA, "cuTensorMapEncodeTiled (state plane) failed: " + std::to_string(r));
+    }
+    const cuuint64_t mdim[2] = {cuuint64_t(Nx), cuuint64_t(Nr)};
+    const cuuint64_t mstride[1] = {cuuint64_t(h->maskPitch)};
+    const cuuint32_t mbox[2] = {cuuint32_t(mask_box_width(PX)), cuuint32_t(PY)};
+    CUresult r = enc(&maps[t].mask, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, h->maskP, mdim, mstride, mbox, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(RN_ERR_CUDA, "cuTensorMapEncodeTiled (mask) failed: " + std::to_string(r));
+  }
+  CK(cudaMemcpyAsync(h->dMaps, maps.data(), sizeof(TileMaps) * NTILES, cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return RN_OK;
+}
+
+int rn_mask_refresh(rn_solver* h) {
+  CK(cudaMemcpy2DAsync(h->maskP, size_t(h->maskPitch), h->mask, size_t(h->Nx), size_t(h->Nx), size_t(h->Nr),
+                       cudaMemcpyDeviceToDevice, h->stream));
+  return RN_OK;
+}
 
 // Per tile, the cells outside it that belong to a cut-cell group with a cell
 // inside it (a sliver merged across the tile edge). Groups are a host plus the
@@ -377,6 +456,10 @@ int rn_set_mask(rn_handle h, const uint8_t* mask) {
   std::vector<uint8_t> m(N);
   for (size_t k = 0; k < N; k++) m[k] = mask[k] ? 1 : 0;
   CK(cudaMemcpyAsync(h->mask, m.data(), N, cudaMemcpyHostToDevice, h->stream));
+  {
+    const int rc = rn_mask_refresh(h);
+    if (rc != RN_OK) return rc;
+  }
   CK(cudaStreamSynchronize(h->stream));
   h->wvalid = false;
   return RN_OK;
@@ -481,6 +564,7 @@ int step_once(rn_solver* h, const rn_params* P) {
   a.stPrev = stPrev; a.stNew = stNew; a.wIn = wIn; a.wOut = wOut;
   a.finalCfl = 0;
   a.xoff = h->xoff; a.xcell = h->xcell; a.maxX = h->maxX;
+  a.slotIn = s0; a.tm = h->dMaps; a.err = h->errFlag;
   {
     ProfScope ps(h, RN_K_STAGE1);
     h->K->stage1(a, *P, h->tile, h->stream);
@@ -496,6 +580,9 @@ int step_once(rn_solver* h, const rn_params* P) {
     sp.key = h->key; sp.val = h->val; sp.dep = h->dep;
     sp.acc = h->acc + size_t(4) * g.Nx * g.Nr * h->scur;
     sp.depFlag = h->depFlag;
+    sp.boundIn = h->depBound + 2 * h->scur;
+    sp.boundOut = h->depBound + 2 * (1 - h->scur);
+    sp.liveSteps = h->liveSteps;
     sp.head = int(h->head); sp.seed = int(h->seed);
     sp.hs = h->hsOnDevice ? h->dHS : nullptr;
     int launched = 0;
@@ -525,6 +612,7 @@ int step_once(rn_solver* h, const rn_params* P) {
   StageArgs b = a;
   b.A = h->SA[s1]; b.B = h->SB[s1]; b.A0 = h->SA[s0]; b.B0 = h->SB[s0];
   b.oA = h->SA[s2]; b.oB = h->SB[s2];
+  b.slotIn = s1;
   b.finalCfl = (!phys && !inj) ? 1 : 0;
   if (phys) {
     // stage 2 + split step in one kernel; its output replaces the stage-2 slot
@@ -567,6 +655,7 @@ int step_once(rn_solver* h, const rn_params* P) {
     ap.A = h->SA[h->cur]; ap.B = h->SB[h->cur]; ap.src = h->src;
     ap.acc = h->acc + size_t(4) * g.Nx * g.Nr * h->scur;
     ap.accNext = h->acc + size_t(4) * g.Nx * g.Nr * (1 - h->scur);
+    ap.boundIn = h->depBound + 2 * h->scur;
     ap.oA = h->SA[out]; ap.oB = h->SB[out];
     ap.wOut = wOut; ap.finalCfl = 1;
     ap.hsNext = h->hsOnDevice ? h->dHS : nullptr;
@@ -850,6 +939,22 @@ int rn_spray_set_parcels(rn_handle h, const float* PA, const float* PB, int head
   CK(cudaMemcpyAsync(h->PA[h->scur], PA, sizeof(float4) * SPRAY_N, cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemcpyAsync(h->PB[h->scur], PB, sizeof(float4) * SPRAY_N, cudaMemcpyHostToDevice, h->stream));
   CK(cudaMemsetAsync(h->PC[h->scur], 0, sizeof(float4) * SPRAY_N, h->stream));
+  // the deposit bounds of the loaded ring: its largest live mass and speed
+  float mMax = 0.0f, vMax = 0.0f;
+  for (int k = 0; k < SPRAY_N; k++) {
+    const float m = PB[4 * k + 1];
+    if (!(m > 0.0f)) continue;
+    const float v = std::sqrt(PA[4 * k + 2] * PA[4 * k + 2] + PA[4 * k + 3] * PA[4 * k + 3]);
+    if (m < 3.0e38f) mMax = std::max(mMax, m);
+    if (v < 3.0e38f) vMax = std::max(vMax, v);
+  }
+  unsigned hb[4];
+  std::memcpy(&hb[0], &mMax, 4);
+  std::memcpy(&hb[1], &vMax, 4);
+  hb[2] = hb[0];
+  hb[3] = hb[1];
+  CK(cudaMemcpyAsync(h->depBound, hb, sizeof(hb), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaMemsetAsync(h->liveSteps, 0, sizeof(unsigned long long), h->stream));
   CK(cudaStreamSynchronize(h->stream));
   h->head = uint32_t(((head % SPRAY_N) + SPRAY_N) % SPRAY_N);
   return RN_OK;
@@ -858,6 +963,15 @@ int rn_spray_set_parcels(rn_handle h, const float* PA, const float* PB, int head
 int rn_spray_reset(rn_handle h) {
   if (!valid(h)) return fail(RN_ERR_ARG, "rn_spray_reset: bad handle");
   return spray_reset_dev(h);
+}
+
+int rn_spray_parcel_steps(rn_handle h, long long* out) {
+  if (!valid(h) || !out) return fail(RN_ERR_ARG, "rn_spray_parcel_steps: bad argument");
+  unsigned long long v = 0;
+  CK(cudaMemcpyAsync(&v, h->liveSteps, sizeof(v), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  *out = (long long)v;
+  return RN_OK;
 }
 
 int rn_spray_stats(rn_handle h, double out[4]) {
@@ -870,8 +984,7 @@ int rn_spray_stats(rn_handle h, double out[4]) {
   if (flag) {
     CK(cudaMemsetAsync(h->depFlag, 0, sizeof(unsigned), h->stream));
     return fail(RN_ERR_STATE, "rn_spray_stats: a spray deposit left the fixed-point range of the fast "
-                              "precision (a parcel far heavier or faster than mhat*dtMax/4 and vMax allow); "
-                              "the deposits were clamped");
+                              "precision (a non-finite parcel); the deposits were clamped");
   }
   double f = 0, o = 0, dS = 0;
   long long n = 0;
@@ -907,6 +1020,23 @@ int rn_integrals(rn_handle h, const rn_integral_spec* spec, rn_integrals_out* ou
 int rn_sync(rn_handle h) {
   if (!h) return fail(RN_ERR_ARG, "rn_sync: NULL handle");
   CK(cudaStreamSynchronize(h->stream));
+  if (h->errFlag) {
+    unsigned e = 0;
+    CK(cudaMemcpy(&e, h->errFlag, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (e) {
+      CK(cudaMemset(h->errFlag, 0, sizeof(unsigned)));
+      return fail(RN_ERR_CUDA, "rn_sync: a stage kernel's halo copy did not complete; the step's results are invalid");
+    }
+  }
+  if (h->depFlag) {
+    unsigned e = 0;
+    CK(cudaMemcpy(&e, h->depFlag, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (e) {
+      CK(cudaMemset(h->depFlag, 0, sizeof(unsigned)));
+      return fail(RN_ERR_STATE, "rn_sync: a spray deposit left the fixed-point range of the fast precision (a "
+                                "non-finite parcel); the deposits were clamped");
+    }
+  }
   return RN_OK;
 }
 
@@ -959,7 +1089,7 @@ int rn_autotune(rn_handle h, const rn_params* P, int steps, int* chosen) {
   const size_t N = size_t(h->Nx) * h->Nr;
   const size_t stateBytes = sizeof(float4) * N * 6, sprayBytes = sizeof(float4) * SPRAY_N * 6;
   char* save = nullptr;
-  CK(cudaMalloc(&save, stateBytes + sprayBytes + sizeof(float4) * 2 + sizeof(unsigned) * 2));
+  CK(cudaMalloc(&save, stateBytes + sprayBytes + sizeof(float4) * 2 + sizeof(unsigned) * 6));
   auto copy_all = [&](bool toSave) -> cudaError_t {
     char* p = save;
     cudaError_t e;
@@ -974,6 +1104,10 @@ int rn_autotune(rn_handle h, const rn_params* P, int steps, int* chosen) {
                : cudaMemcpyAsync(h->stepTex, p, sizeof(float4) * 2, k, h->stream);
     if (e != cudaSuccess) return e;
     p += sizeof(float4) * 2;
+    e = toSave ? cudaMemcpyAsync(p, h->depBound, sizeof(unsigned) * 4, k, h->stream)
+               : cudaMemcpyAsync(h->depBound, p, sizeof(unsigned) * 4, k, h->stream);
+    if (e != cudaSuccess) return e;
+    p += sizeof(unsigned) * 4;
     return toSave ? cudaMemcpyAsync(p, h->wmax, sizeof(unsigned) * 2, k, h->stream)
                   : cudaMemcpyAsync(h->wmax, p, sizeof(unsigned) * 2, k, h->stream);
   };

@@ -165,6 +165,8 @@ int refresh(rn_batch_t* b) {
     }
     d.stepTex = h->stepTex;
     d.wmax = h->wmax;
+    d.tm = h->dMaps;
+    d.err = h->errFlag;
     d.xoff = h->xoff;
     d.xcell = h->xcell;
     normalise(b, h, d.cur0, d.stepIdx0, d.wslot0);
@@ -268,6 +270,9 @@ int launch_step(rn_batch_t* b, int c, bool withSpray) {
       sp.key = h->key; sp.val = h->val; sp.dep = h->dep;
       sp.acc = h->acc + size_t(4) * h->Nx * h->Nr * h->scur;
       sp.depFlag = h->depFlag;
+      sp.boundIn = h->depBound + 2 * h->scur;
+      sp.boundOut = h->depBound + 2 * (1 - h->scur);
+      sp.liveSteps = h->liveSteps;
       sp.head = int(h->head); sp.seed = int(h->seed);
       sp.hs = nullptr;
       int launched = 0;
@@ -309,6 +314,7 @@ int launch_step(rn_batch_t* b, int c, bool withSpray) {
       ap.A = h->SA[cur]; ap.B = h->SB[cur]; ap.src = h->src;
       ap.acc = h->acc + size_t(4) * h->Nx * h->Nr * h->scur;
       ap.accNext = h->acc + size_t(4) * h->Nx * h->Nr * (1 - h->scur);
+      ap.boundIn = h->depBound + 2 * h->scur;
       ap.oA = h->SA[out]; ap.oB = h->SB[out];
       ap.wOut = h->wmax + (1 - ws);
       ap.finalCfl = 1;

@@ -449,6 +449,8 @@ int rn_build_geometry(rn_handle h, const rn_cut_spec* sp, rn_cut_stats* stats) {
   std::memcpy(h->hostGeoM.data(), gm.data(), sizeof(float4) * N);
   int rc = rn_build_member_lists(h);
   if (rc != RN_OK) return rc;
+  rc = rn_mask_refresh(h);
+  if (rc != RN_OK) return rc;
   h->wvalid = false;
   if (stats) {
     stats->nCut = int(cnt[0]);

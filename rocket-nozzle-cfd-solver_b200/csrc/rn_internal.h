@@ -18,9 +18,18 @@ struct rn_solver {
   int cur = 0;
   float4 *geoA = nullptr, *geoG = nullptr, *geoM = nullptr, *jw = nullptr, *wallRow = nullptr;
   uint8_t* mask = nullptr;
+  // the mask again with rows padded to 16 bytes (a tensor map's row stride
+  // must be a multiple of 16 bytes), refreshed whenever the mask changes
+  uint8_t* maskP = nullptr;
+  int maskPitch = 0;
+  // tensor maps of the stage kernels' halo copies, one TileMaps per tile shape
+  rn::TileMaps* dMaps = nullptr;
+  unsigned* errFlag = nullptr;    // set by a stage kernel whose halo copy did not complete in time
   float4* stepTex = nullptr;      // [2]
   unsigned* wmax = nullptr;       // [2]
   unsigned* depFlag = nullptr;    // set when a fast deposit left the fixed-point range
+  unsigned* depBound = nullptr;   // [2 step parities] x (largest parcel mass, speed) of the ring, float bits
+  unsigned long long* liveSteps = nullptr;   // live parcels summed over the spray steps since the ring was set
   int stepIdx = 0, wslot = 0;
   bool wvalid = false;
   long long stepCount = 0, launches = 0;
@@ -97,6 +106,10 @@ struct rn_solver {
   rn::Grid grid() const { return rn::Grid{Nx, Nr, mask, geoA, geoG, geoM}; }
 };
 
+// (Re)encode the tensor maps of h's state ring and pitched mask (rn_api.cu).
+int rn_build_tile_maps(rn_solver* h);
+// Copy h->mask into its row-pitched copy (queued on h->stream).
+int rn_mask_refresh(rn_solver* h);
 // Record an error for rn_last_error() and return `code`.
 int rn_record_error(int code, const std::string& msg);
 int rn_record_cuda(cudaError_t e, const char* what);

@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include "rn_math.cuh"
+#include "rn_tma.cuh"
 
 namespace rn {
 
@@ -52,6 +53,9 @@ struct StageArgs {
   const int* xoff;                      // per tile: out-of-tile members of its cut-cell groups (CSR)
   const int* xcell;
   int maxX;                             // largest per-tile list (sizes the dynamic shared memory)
+  int slotIn;                           // ring slot of (A, B): selects the tensor maps of the halo copy
+  const TileMaps* tm;                   // the handle's tensor maps, one TileMaps per tile shape
+  unsigned* err;                        // set when a halo copy did not complete in time
 };
 
 struct PhysArgs {
@@ -77,6 +81,9 @@ struct SprayArgs {
   unsigned* key; unsigned* val; float4* dep;   // deposit records (cell key, parcel index, source)
   unsigned long long* acc;              // fixed-point deposit sums of this step, 4 per cell (fast variant)
   unsigned* depFlag;                    // set when a deposit left the fixed-point range (fast variant)
+  const unsigned* boundIn;              // (mass, speed) bounds of the ring this step reads (float bits)
+  unsigned* boundOut;                   // the same for the ring it writes: max of boundIn and its parcels
+  unsigned long long* liveSteps;        // += live parcels this step writes (parcel-steps counter)
   int head, seed;
   const unsigned* hs;                   // if set: (head, seed) read here instead (graph replay)
 };
@@ -86,6 +93,7 @@ struct ApplyArgs {
   const float4* A; const float4* B;
   const float4* src;
   const unsigned long long* acc;        // this step's fixed-point deposit sums (fast variant)
+  const unsigned* boundIn;              // the (mass, speed) bounds its deposits were scaled by
   unsigned long long* accNext;          // the next step's, cleared here cell by cell
   float4* oA; float4* oB;
   unsigned* wOut;
@@ -105,6 +113,8 @@ struct BatchInst {
   unsigned* wmax;                       // 2 slots
   const int* xoff;
   const int* xcell;
+  const TileMaps* tm;                   // the member's tensor maps, one TileMaps per tile shape
+  unsigned* err;                        // the member's error word (halo copy timeout)
   int cur0, stepIdx0, wslot0;
   int firstBlock, tilesX;
   int pad_;

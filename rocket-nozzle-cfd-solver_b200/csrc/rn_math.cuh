@@ -97,12 +97,25 @@ RN_DEV float wave_speed(float4 a, float4 b) {
   return fabsf(q.w.y) + fabsf(q.w.z) + 2.0f * sound_speed(q);
 }
 
+// Cells of the grid as ghost_prim_c reads them: solid flag and raw state of
+// in-grid cell (i, j). GlobalCells reads the planes in global memory; the
+// stage kernels read the tile they staged in shared memory (rn_step.cu).
+struct GlobalCells {
+  const Grid& g;
+  const float4* __restrict__ A;
+  const float4* __restrict__ B;
+  RN_DEV bool solid(int i, int j) const { return g.mask[j * g.Nx + i] != 0; }
+  RN_DEV float4 a(int i, int j) const { return A[j * g.Nx + i]; }
+  RN_DEV float4 b(int i, int j) const { return B[j * g.Nx + i]; }
+};
+
 // Padded primitive cell (i, j), i in [-2, Nx+1], j in [-2, Nr+1] (FS_PRIM,
 // solver.js:56-126). Wall cells come back as W = (-1, 0, 0, 1), Wb = 0.
 // t is the time the inlet ramp reads (t_old in stage 1, t_new in stage 2).
-RN_DEV void ghost_prim(const Grid& g, const float4* __restrict__ A, const float4* __restrict__ B, int i, int j,
-                       float t, const rn_params& P, float4& W, float4& Wb) {
-  const int Nx = g.Nx, Nr = g.Nr;
+// Every cell it reads lies within 2 cells of (i, j), inside the grid.
+template <class C>
+RN_DEV void ghost_prim_c(int Nx, int Nr, const C& cells, int i, int j, float t, const rn_params& P, float4& W,
+                         float4& Wb) {
   bool mir = j < 0;
   if (mir) j = -j - 1;
   Prim q;
@@ -110,14 +123,14 @@ RN_DEV void ghost_prim(const Grid& g, const float4* __restrict__ A, const float4
   q.s = make_float4(0.0f, 0.0f, P.inlet[3], 0.0f);
   bool wall = false;
   if (i < 0) {
-    if (j < Nr && solid_at(g, 0, j)) wall = true;
+    if (j < Nr && cells.solid(0, j)) wall = true;
     else if (float(j) + 0.5f < P.RcCells && P.inj) wall = true;
     else if (float(j) + 0.5f < P.RcCells) {
       float f = P.ramp > 0.0f ? smoothstepf(0.0f, P.ramp, t) : 1.0f;
       float P0 = mixf(P.pStart, P.res[0], f);
       float T0 = P.res[1], R = P.res[2], G = P.inlet[2], gg = 1.0f + 1.0f / G;
-      float4 a = A[j * Nx];
-      float ubar = fmaxf(B[j * Nx].w, 0.0f);
+      float4 a = cells.a(0, j);
+      float ubar = fmaxf(cells.b(0, j).w, 0.0f);
       float c0 = sqrtf(gg * R * T0);
       float ui = clampf(a.y / fmaxf(a.x, RHO_MIN), 0.0f, 0.5f * c0);
       float ut = ubar * smoothstepf(1.0f, 2.0f, P0 / fmaxf(P.pStart, 1e-6f));
@@ -129,16 +142,16 @@ RN_DEV void ghost_prim(const Grid& g, const float4* __restrict__ A, const float4
     }
   } else if (j >= Nr) {
     int ci = min(i, Nx - 1), cj = Nr - 1;
-    if (!solid_at(g, ci, cj)) {
-      Prim tq = to_prim(A[cj * Nx + ci], B[cj * Nx + ci]);
+    if (!cells.solid(ci, cj)) {
+      Prim tq = to_prim(cells.a(ci, cj), cells.b(ci, cj));
       float cs = sound_speed(tq);
       if (tq.w.z >= cs) q = tq;
       else if (tq.w.z > 0.0f) { q = tq; q.w.w = P.amb[3]; }
     }
   } else if (i >= Nx) {
     int ci = Nx - 1, cj = j;
-    if (!solid_at(g, ci, cj)) {
-      Prim tq = to_prim(A[cj * Nx + ci], B[cj * Nx + ci]);
+    if (!cells.solid(ci, cj)) {
+      Prim tq = to_prim(cells.a(ci, cj), cells.b(ci, cj));
       float cs = sound_speed(tq);
       if (tq.w.y >= cs) q = tq;
       else if (tq.w.y > 0.0f) { q = tq; q.w.w = P.amb[3]; }
@@ -146,9 +159,8 @@ RN_DEV void ghost_prim(const Grid& g, const float4* __restrict__ A, const float4
     }
   } else {
     // the state is loaded with the mask (not after it), so the two loads overlap
-    const int k = j * Nx + i;
-    const float4 a = A[k], b = B[k];
-    if (g.mask[k] != 0) wall = true;
+    const float4 a = cells.a(i, j), b = cells.b(i, j);
+    if (cells.solid(i, j)) wall = true;
     else q = to_prim(a, b);
   }
   if (wall) {
@@ -159,6 +171,10 @@ RN_DEV void ghost_prim(const Grid& g, const float4* __restrict__ A, const float4
   if (mir) q.w.z = -q.w.z;
   W = q.w;
   Wb = q.s;
+}
+RN_DEV void ghost_prim(const Grid& g, const float4* __restrict__ A, const float4* __restrict__ B, int i, int j,
+                       float t, const rn_params& P, float4& W, float4& Wb) {
+  ghost_prim_c(g.Nx, g.Nr, GlobalCells{g, A, B}, i, j, t, P, W, Wb);
 }
 
 // Interior cell as the padded texture holds it (wall flag or toPrim).
@@ -203,17 +219,18 @@ RN_DEV float4 step4(float4 w, float h, float4 d) {
 }
 RN_DEV float jump_ratio(float a, float b) { return fdiv(fabsf(a - b), fminf(a, b)); }
 
-// DIR_R selects the r-direction (normal velocity in .z); one instance of the
-// code serves both directions.
-RN_DEV Flux face_flux(bool DIR_R, float area, float4 w0, float4 b0, float4 w1, float4 b1, float4 w2, float4 b2,
-                      float4 w3, float4 b3, float4 sa1, float4 sb1, float4 sa2, float4 sb2, const rn_params& P) {
+// DIR_R selects the r-direction (normal velocity in .z), fixed at compile
+// time: the tile kernels run the x-faces and the r-faces in loops of their own.
+template <bool DIR_R>
+RN_DEV Flux face_flux(float area, float4 w0, float4 b0, float4 w1, float4 b1, float4 w2, float4 b2, float4 w3,
+                      float4 b3, float4 sa1, float4 sb1, float4 sa2, float4 sb2, const rn_params& P) {
   Flux out;
   out.F = make_float4(0.f, 0.f, 0.f, 0.f);
   out.Y = out.F;
   out.O = 0.0f;
   bool s0 = w0.x < 0.0f, s1 = w1.x < 0.0f, s2 = w2.x < 0.0f, s3 = w3.x < 0.0f;
   if (s1 && s2) return out;
-  if (DIR_R) {   // face-normal frame: normal velocity in .y
+  if constexpr (DIR_R) {   // face-normal frame: normal velocity in .y
     float t;
     t = w0.y; w0.y = w0.z; w0.z = t;
     t = w1.y; w1.y = w1.z; w1.z = t;
@@ -319,7 +336,7 @@ RN_DEV Flux face_flux(bool DIR_R, float area, float4 w0, float4 b0, float4 w1, f
     uf = uK + SK * (fdiv(SK - uK, SK - Ss) - 1.0f);
     Gf = left ? GL : GR;
   }
-  if (DIR_R) { float t = F1; F1 = F2; F2 = t; }    // rotate momentum back to (x, r)
+  if constexpr (DIR_R) { float t = F1; F1 = F2; F2 = t; }    // rotate momentum back to (x, r)
   out.F = make_float4(F0, F1, F2, F3);
   out.Y = make_float4(Y0, Y1, uf * Gf, uf);
   out.O = Y2;
@@ -379,21 +396,22 @@ RN_DEV void vcell(float4 w0, float4 sc, float4 wE, float4 wW, float4 wN, float4 
   T2 = make_float4(fminf(mu + mut, fdiv(0.08f * rho, fmaxf(dt, 1e-9f))), fdiv((sc.z + 1.0f) * p, rho), Smag, mu);
 }
 
-// makeViscFluxShader (solver.js:499-536) for one face; returns false for a
-// zero flux. (w1, s1, t1, m1) is the cell behind the face, (w2, s2, t2, m2) the
-// cell the face belongs to; j is the face's row.
-RN_DEV void visc_flux(bool DIR_R, float4 w1, float4 s1, float4 t1, float4 m1, float4 w2, float4 s2, float4 t2,
-                      float4 m2, int j, float4& F, float4& FY) {
+// makeViscFluxShader (solver.js:499-536) for one face. (w1, s1, t1, m1) is
+// the cell behind the face, (w2, s2, t2, m2) the cell the face belongs to; j
+// is the face's row. DIR_R (the r-direction) is fixed at compile time.
+template <bool DIR_R>
+RN_DEV void visc_flux(float4 w1, float4 s1, float4 t1, float4 m1, float4 w2, float4 s2, float4 t2, float4 m2, int j,
+                      float4& F, float4& FY) {
   float mu = 0.5f * (m1.x + m2.x);
   float uf = 0.5f * (w1.y + w2.y), vf = 0.5f * (w1.z + w2.z);
   float ttx = 0.5f * (t1.x + t2.x), tty = 0.5f * (t1.y + t2.y), ttz = 0.5f * (t1.z + t2.z), ttw = 0.5f * (t1.w + t2.w);
   float r, ux, vx, ur, vr;
-  if (DIR_R) { r = fmaxf(float(j), 0.5f); ux = ttx; vx = ttz; ur = w2.y - w1.y; vr = w2.z - w1.z; }
+  if constexpr (DIR_R) { r = fmaxf(float(j), 0.5f); ux = ttx; vx = ttz; ur = w2.y - w1.y; vr = w2.z - w1.z; }
   else { r = float(j) + 0.5f; ux = w2.y - w1.y; vx = w2.z - w1.z; ur = tty; vr = ttw; }
   float div = ux + vr + fdiv(vf, r);
   float txr = mu * (ur + vx);
   float k = mu * 1.25f;
-  if (DIR_R) {
+  if constexpr (DIR_R) {
     float trr = mu * (2.0f * vr - 0.6666667f * div);
     F = make_float4(-k * (s2.w - s1.w), -txr, -trr, -(uf * txr + vf * trr) - k * (m2.y - m1.y));
   } else {

@@ -19,8 +19,12 @@
 //             batch and frees its memory, which admits the next arrivals.
 // A solve steps exactly as it would alone: batch membership does not change a
 // cell's arithmetic, so its result is the same in any mix.
+// Failures are isolated: a solve whose own work fails (setup, an allocation,
+// a non-finite residual) is evicted alone; a class batch whose step fails
+// evicts its class; only a broken CUDA context fails everything.
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -50,6 +54,7 @@ struct Request {
   rn_integral_spec spec;
   size_t bytes = 0;
   double tSubmit = 0.0;
+  int inject = 0;            // RN_INJECT_* armed by rn_serve_inject for this request
 };
 
 struct Active {
@@ -97,6 +102,8 @@ struct rn_server_t {
   bool stop = false;
   int failed = 0;
   std::string failMsg;
+  int injectNext = 0;         // armed by rn_serve_inject, taken by the next submit
+  long long evicted = 0;      // solves that failed alone
   // worker-side state (read under mu by rn_serve_stats)
   std::vector<Active> active;
   size_t used = 0;
@@ -118,6 +125,10 @@ int sfail(int code, const std::string& msg) { return rn_record_error(code, msg);
 
 // Creates and uploads the handle of request r and adds it to its class batch.
 int admit(rn_server_t* s, Request& r, Active& a) {
+  if (r.inject == RN_INJECT_ADMIT) {
+    r.inject = 0;
+    return sfail(RN_ERR_NOMEM, "injected allocation failure at admission");
+  }
   rn_handle h = nullptr;
   int rc = rn_create(r.Nx, r.Nr, &h);
   if (rc != RN_OK) return rc;
@@ -178,6 +189,33 @@ void retire(rn_server_t* s, Active& a, int status) {
   s->done[a.req.id] = std::move(d);
 }
 
+// A solve that failed alone: leaves its batch and frees its memory; its
+// result carries RN_SOLVE_FAILED and no state.
+void evict(rn_server_t* s, Active& a) {
+  if (a.h) {
+    rn_batch_t* b = s->batches[a.cls];
+    if (b) rn_batch_remove(b, a.h);
+    rn_destroy(a.h);
+    a.h = nullptr;
+  }
+  Done d;
+  std::memset(&d.res, 0, sizeof(d.res));
+  d.res.status = RN_SOLVE_FAILED;
+  d.res.steps = a.steps;
+  d.res.t = a.t;
+  d.res.residual0 = a.r0;
+  d.res.residual = a.r;
+  d.res.submit_ms = a.req.tSubmit;
+  d.res.admit_ms = a.tAdmit;
+  d.res.done_ms = s->now_ms();
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->used -= a.req.bytes;
+  s->cells -= (long long)a.req.Nx * a.req.Nr;
+  s->retired++;
+  s->evicted++;
+  s->done[a.req.id] = std::move(d);
+}
+
 void fail_all(rn_server_t* s, const std::string& msg) {
   for (Active& a : s->active) {
     if (a.h) {
@@ -213,6 +251,9 @@ void fail_all(rn_server_t* s, const std::string& msg) {
 }
 
 // One tick: check_every steps of every class batch, residuals of the last step.
+// A solve whose own work fails is marked and evicted after the tick, a class
+// whose batch step fails has all its solves evicted; the tick itself returns
+// an error only when the CUDA context no longer works.
 int tick(rn_server_t* s) {
   const int K = std::max(s->opts.check_every, 2);
   const size_t need = s->active.size() * 8;
@@ -223,43 +264,69 @@ int tick(rn_server_t* s) {
     RN_CK(cudaHostAlloc(reinterpret_cast<void**>(&s->pinned), sizeof(double) * need * 2, cudaHostAllocDefault));
     s->pinnedCap = need * 2;
   }
+  std::vector<char> bad(s->active.size(), 0);
+  std::map<int, bool> badClass;
+  bool anyBad = false;
   // every class batch queues its K steps before any is waited for
   for (auto& kv : s->batches) {
     rn_batch_t* b = kv.second;
     int members = 0;
     rn_batch_size(b, &members, nullptr);
     if (!members) continue;
-    int rc = rn_batch_step(b, K - 1);
-    if (rc != RN_OK) return rc;
+    if (rn_batch_step(b, K - 1) != RN_OK) { badClass[kv.first] = anyBad = true; continue; }
     void* st = nullptr;
     rn_batch_stream(b, &st);
     cudaStream_t bs = static_cast<cudaStream_t>(st);
-    for (Active& a : s->active)
-      if (a.cls == kv.first && (rc = rn_residual_mark_on(a.h, bs)) != RN_OK) return rc;
-    if ((rc = rn_batch_step(b, 1)) != RN_OK) return rc;
     for (size_t q = 0; q < s->active.size(); q++) {
       Active& a = s->active[q];
       if (a.cls != kv.first) continue;
-      if ((rc = rn_residual_launch(a.h, bs)) != RN_OK) return rc;
-      RN_CK(cudaMemcpyAsync(s->pinned + 8 * q, a.h->dRes, sizeof(double) * 6, cudaMemcpyDeviceToHost, bs));
-      RN_CK(cudaMemcpyAsync(s->pinned + 8 * q + 6, a.h->stepTex + a.h->stepIdx, sizeof(float4),
-                            cudaMemcpyDeviceToHost, bs));
+      if (a.req.inject == RN_INJECT_TICK) {        // host-side injection: fails as an allocation would
+        a.req.inject = 0;
+        rn_record_error(RN_ERR_NOMEM, "injected allocation failure in a tick");
+        bad[q] = anyBad = true;
+        continue;
+      }
+      if (rn_residual_mark_on(a.h, bs) != RN_OK) bad[q] = anyBad = true;
+    }
+    if (rn_batch_step(b, 1) != RN_OK) { badClass[kv.first] = anyBad = true; continue; }
+    for (size_t q = 0; q < s->active.size(); q++) {
+      Active& a = s->active[q];
+      if (a.cls != kv.first || bad[q]) continue;
+      if (rn_residual_launch(a.h, bs) != RN_OK ||
+          cudaMemcpyAsync(s->pinned + 8 * q, a.h->dRes, sizeof(double) * 6, cudaMemcpyDeviceToHost, bs) !=
+              cudaSuccess ||
+          cudaMemcpyAsync(s->pinned + 8 * q + 6, a.h->stepTex + a.h->stepIdx, sizeof(float4), cudaMemcpyDeviceToHost,
+                          bs) != cudaSuccess)
+        bad[q] = anyBad = true;
     }
   }
-  for (auto& kv : s->batches) {
-    int rc = rn_batch_sync(kv.second);
-    if (rc != RN_OK) return rc;
+  for (auto& kv : s->batches)
+    if (rn_batch_sync(kv.second) != RN_OK) badClass[kv.first] = anyBad = true;
+  if (anyBad) {
+    // a failure that left the context usable is the failing solves' alone
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e != cudaSuccess && cudaDeviceSynchronize() != cudaSuccess)
+      return rn_record_cuda(e, "solve server tick (the CUDA context no longer works)");
   }
   s->ticks++;
-  // retire what has converged, run out of time or steps
+  // retire what has converged, run out of time or steps; evict what failed
   std::vector<Active> keep;
   for (size_t q = 0; q < s->active.size(); q++) {
     Active& a = s->active[q];
+    if (bad[q] || badClass.count(a.cls)) {
+      evict(s, a);
+      continue;
+    }
     a.steps += K;
     const double* res = s->pinned + 8 * q;
     const float* st = reinterpret_cast<const float*>(s->pinned + 8 * q + 6);
     a.r = res[0];
     a.t = double(st[2]);
+    if (!std::isfinite(a.r)) {                      // the solve's state is no longer finite
+      evict(s, a);
+      continue;
+    }
     if (a.r0 < 0.0) a.r0 = a.r;
     int status = -100;
     if (a.req.drop > 0.0 && a.r0 > 0.0 && a.r <= a.req.drop * a.r0 && a.steps > K) status = RN_SOLVE_CONVERGED;
@@ -323,6 +390,7 @@ void work(rn_server_t* s) {
         std::lock_guard<std::mutex> lk(s->mu);
         s->used -= a.req.bytes;
         s->cells -= (long long)a.req.Nx * a.req.Nr;
+        s->evicted++;
         s->done[a.req.id] = std::move(d);
         s->cvDone.notify_all();
         continue;
@@ -442,6 +510,8 @@ int rn_serve_submit(rn_server s, const rn_solve_request* q, long long* id) {
   {
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->failed) return sfail(RN_ERR_STATE, s->failMsg);
+    r.inject = s->injectNext;
+    s->injectNext = 0;
     r.id = s->nextId++;
     r.tSubmit = s->now_ms();
     *id = r.id;
@@ -489,6 +559,15 @@ int rn_serve_stats(rn_server s, rn_serve_status* out) {
   out->ticks = s->ticks.load();
   out->admitted = s->admitted;
   out->failed = s->failed;
+  out->evicted = s->evicted;
+  return RN_OK;
+}
+
+int rn_serve_inject(rn_server s, int where) {
+  if (!s || (where != RN_INJECT_ADMIT && where != RN_INJECT_TICK))
+    return sfail(RN_ERR_ARG, "rn_serve_inject: bad argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  s->injectNext = where;
   return RN_OK;
 }
 

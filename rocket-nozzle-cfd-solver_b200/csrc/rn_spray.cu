@@ -17,11 +17,20 @@
 // Fast variant: the deposits go instead into 64-bit fixed-point sums per cell
 //   (integer atomics, so the sums do not depend on the order the parcels
 //   arrive in: deterministic, with no sort). A component is quantised in
-//   steps of 2^-40 of a bound no deposit reaches (mass: the largest parcel
-//   mass mhat * dtMax / 4; momentum: that times 4 vMax), after the float
-//   product x * 2^40 / bound, so each deposit keeps float precision and the
-//   sums hold up to 2^22 bounds. The exact variant keeps the sort and the
-//   float sum in parcel-index order.
+//   steps of 2^-40 of a bound no deposit reaches, after the float product
+//   x * 2^40 / bound, so each deposit keeps float precision and the sums hold
+//   up to 2^22 bounds. The bounds follow the ring: every parcel step folds the
+//   largest mass and speed of the parcels it writes (and the bounds it read)
+//   into the next step's pair, so a deposit never exceeds its step's bounds:
+//   mass: max(that mass, mhat dtMax / 4), the spawn mass at the largest step;
+//   momentum: the mass bound times 4 max(that speed, vMax). A parcel's deposit
+//   is at most its mass (evaporated or recycled) and its momentum change at
+//   most m (2 |v_old| + |v_new|), with |v_new| <= max(|v_old|, gas speed) and
+//   the gas speed of the stage-1 state it reads at most vMax. A deposit beyond
+//   64 bounds (only a NaN can reach it) is flagged on the device and reported
+//   by rn_spray_stats and rn_sync. The exact variant keeps the sort and the
+//   float sum in parcel-index order (and tracks the bounds too, so a handle
+//   can switch precision between steps).
 #include <cuda_runtime.h>
 #include <cub/device/device_radix_sort.cuh>
 #include "rn_kernels.cuh"
@@ -46,12 +55,17 @@ __device__ __forceinline__ bool wall_at(const Grid& g, const float4* A1, const f
   return g.mask[cy * g.Nx + cx] != 0;          // padded W.x < 0 exactly at solid cells
 }
 
-// Fixed-point scales of the deposit sums (fast variant): 2^40 / bound.
-__device__ __forceinline__ float dep_scale_mass(const rn_params& P) {
-  return ldexpf(1.0f / fmaxf(P.mhat * P.dtMax * 0.25f, 1e-30f), 40);
+// Fixed-point scales of the deposit sums (fast variant): 2^40 / bound, from
+// the step's (mass, speed) bounds b (float bits; 0 for an empty ring).
+__device__ __forceinline__ float dep_bound_mass(const rn_params& P, const unsigned* b) {
+  return fmaxf(P.mhat * P.dtMax * 0.25f, __uint_as_float(b[0]));
 }
-__device__ __forceinline__ float dep_scale_mom(const rn_params& P) {
-  return ldexpf(1.0f / fmaxf(P.mhat * P.dtMax * fmaxf(P.vMax, 1.0f), 1e-30f), 40);
+__device__ __forceinline__ float dep_scale_mass(const rn_params& P, const unsigned* b) {
+  return ldexpf(1.0f / fmaxf(dep_bound_mass(P, b), 1e-30f), 40);
+}
+__device__ __forceinline__ float dep_scale_mom(const rn_params& P, const unsigned* b) {
+  return ldexpf(1.0f / fmaxf(dep_bound_mass(P, b) * 4.0f * fmaxf(fmaxf(P.vMax, __uint_as_float(b[1])), 1.0f), 1e-30f),
+                40);
 }
 // |x * scale| stays below 2^46 (64 bounds) or is clamped there and flagged:
 // 65,536 deposits of that size still sum within the 63 bits.
@@ -162,6 +176,42 @@ __global__ void __launch_bounds__(256) k_parcels(SprayArgs a, rn_params P) {
   a.oPA[idx] = oA;
   a.oPB[idx] = oB;
   a.oPC[idx] = oC;
+  {
+    // the next step's bounds: the largest mass and speed written here (finite
+    // values only), folded per block, and this step's bounds (they never shrink)
+    // (and, for the parcel-steps counter, how many live parcels it writes)
+    __shared__ float bm[8], bv[8];
+    __shared__ unsigned bn[8];
+    float m = oB.y > 0.0f && oB.y < 3.0e38f ? oB.y : 0.0f;
+    float v = oB.y > 0.0f ? len2(oA.z, oA.w) : 0.0f;
+    v = v < 3.0e38f ? v : 0.0f;
+    unsigned n = __popc(__ballot_sync(0xffffffffu, oB.y > 0.0f));
+    for (int o = 16; o > 0; o >>= 1) {
+      m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+      v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    }
+    if ((threadIdx.x & 31) == 0) { bm[threadIdx.x >> 5] = m; bv[threadIdx.x >> 5] = v; bn[threadIdx.x >> 5] = n; }
+    __syncthreads();
+    if (threadIdx.x < 32) {
+      m = threadIdx.x < 8 ? bm[threadIdx.x] : 0.0f;
+      v = threadIdx.x < 8 ? bv[threadIdx.x] : 0.0f;
+      n = threadIdx.x < 8 ? bn[threadIdx.x] : 0u;
+      for (int o = 16; o > 0; o >>= 1) {
+        m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+        v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+        n += __shfl_xor_sync(0xffffffffu, n, o);
+      }
+      if (threadIdx.x == 0) {
+        if (a.liveSteps && n) atomicAdd(a.liveSteps, (unsigned long long)n);
+        if (blockIdx.x == 0) {
+          m = fmaxf(m, __uint_as_float(a.boundIn[0]));
+          v = fmaxf(v, __uint_as_float(a.boundIn[1]));
+        }
+        if (m > 0.0f) atomicMax(a.boundOut, __float_as_uint(m));
+        if (v > 0.0f) atomicMax(a.boundOut + 1, __float_as_uint(v));
+      }
+    }
+  }
   // deposit record (VS_SPRAY_DEP, spray.js:131-141): old position, new source
   const unsigned none = unsigned(g.Nx * g.Nr);
   unsigned key = none;
@@ -178,7 +228,7 @@ __global__ void __launch_bounds__(256) k_parcels(SprayArgs a, rn_params P) {
   }
 #ifdef RN_FAST
   if (key != none) {
-    const float sm = dep_scale_mass(P), sp = dep_scale_mom(P);
+    const float sm = dep_scale_mass(P, a.boundIn), sp = dep_scale_mom(P, a.boundIn);
     unsigned long long* c = a.acc + 4 * size_t(key);
     bool over = false;
     atomicAdd(c + 0, to_fixed(dep.x, sm, over));
@@ -252,7 +302,7 @@ __global__ void __launch_bounds__(256) k_apply(ApplyArgs a, rn_params P) {
 #ifdef RN_FAST
       const ulonglong2* c = reinterpret_cast<const ulonglong2*>(a.acc) + 2 * size_t(kh);
       const ulonglong2 c01 = c[0], c23 = c[1];
-      const float sm = dep_scale_mass(P), sp = dep_scale_mom(P);
+      const float sm = dep_scale_mass(P, a.boundIn), sp = dep_scale_mom(P, a.boundIn);
       float4 s = make_float4(from_fixed(c01.x, sm), from_fixed(c01.y, sm), from_fixed(c23.x, sp),
                              from_fixed(c23.y, sp));
 #else

@@ -21,6 +21,11 @@
 // stand-in for the symbol. The device address is fetched once per device with
 // cudaGetSymbolAddress (with that device current) by the first call made on
 // it; make that first call before any stream capture begins on the device.
+// The cached address belongs to the module loaded in the device's context: a
+// host that calls cudaDeviceReset must not call rn_integrals_static again in
+// the same process (the module is reloaded and the old address is stale).
+// A call is refused (RN_ERR_ARG) while its stream is being captured, since it
+// ends with a blocking read-back.
 #include <cuda_runtime.h>
 #include <mutex>
 #include <string>
@@ -162,14 +167,27 @@ int rn_integrals_static(const float* A, const float* B, const float* geoA, const
   if (Nr > RN_STATIC_MAX_ROWS)
     return static_fail(RN_ERR_ARG, "rn_integrals_static: " + std::to_string(Nr) + " rows exceed the static scratch (" +
                                        std::to_string(RN_STATIC_MAX_ROWS) + " rows); use rn_integrals");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // The call ends with a blocking read-back, which a capturing stream cannot
+  // take: refuse before anything is queued, so the caller's capture stays valid.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaError_t e = cudaStreamIsCapturing(s, &cap);
+  if (e != cudaSuccess) return static_fail(RN_ERR_CUDA, std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(e));
+  if (cap != cudaStreamCaptureStatusNone)
+    return static_fail(RN_ERR_ARG, "rn_integrals_static: the stream is being captured; call it outside a capture");
+  // An error left by the caller's own earlier work is reported as such, and
+  // nothing is launched after it.
+  e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return static_fail(RN_ERR_CUDA, std::string("rn_integrals_static: earlier CUDA error pending: ") +
+                                        cudaGetErrorString(e));
   double* scratch = nullptr;
   int rc = scratch_for_current_device(&scratch);
   if (rc != RN_OK) return rc;
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   k_integrals_static<<<1, 256, 0, s>>>(scratch, reinterpret_cast<const float4*>(A), reinterpret_cast<const float4*>(B),
                                        reinterpret_cast<const float4*>(geoA), mask, Nx, Nr,
                                        reinterpret_cast<const float4*>(stepinfo), *spec);
-  cudaError_t e = cudaGetLastError();
+  e = cudaGetLastError();
   if (e != cudaSuccess) return static_fail(RN_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
   double r[RESULTS];
   e = cudaMemcpyAsync(r, scratch + TERMS * RN_STATIC_MAX_ROWS, sizeof(r), cudaMemcpyDeviceToHost, s);

@@ -45,30 +45,41 @@ namespace RN_VARIANT {
 // 8 / 24 / 32 / 40 warps): 64 batched instances 2.24 / 3.05 / 3.44 / 3.04,
 // plain 4096x1536 3.33 / 4.55 / 5.52 / 5.65, viscous 512x192 1.71 / 2.24 /
 // 2.18 / 1.89. Results are bit-identical across caps.
-template <int TX_, int TY_, int NT_, int WARPS_>
+template <int TX_, int TY_, int NT_, int WARPS_, int ID_>
 struct TileT {
   static constexpr int TX = TX_, TY = TY_, NT = NT_, NC = TX * TY;   // NT threads, NC cells (NC <= NT)
+  static constexpr int ID = ID_;                                      // index into TILE_* and TileMaps
   static constexpr int MINB = WARPS_ / (NT / 32) > 0 ? WARPS_ / (NT / 32) : 1;
   // Shapes compiled for fewer than 32 warps (more registers per thread) run
   // the fused kernel's stage-2 update and FS_VCELL as one work list, with
   // T1/T2 in shared memory of their own (viscous plume 512x192 with 14x16
-  // tiles: 3.00 -> 3.10-3.18 G cell-updates/s), and load their first
-  // primitives before the member list (prefetch_prims). At 4 blocks per SM
-  // the extra memory, loop body and live registers cost more than they save
-  // (64 batched instances, 16x15: 4.37 -> 4.18 G).
+  // tiles: 3.00 -> 3.10-3.18 G cell-updates/s). At 4 blocks per SM the extra
+  // memory, loop body and live registers cost more than they save (64 batched
+  // instances, 16x15: 4.37 -> 4.18 G).
   static constexpr bool WIDE = WARPS_ < 32;
   static constexpr int PX = TX + 4, PY = TY + 4, NPT = PX * PY;   // primitives with a 2-cell halo
   static constexpr int NXF = TY * (TX + 1), NRF = (TY + 1) * TX;  // x- and r-faces of a tile
   static constexpr int TW = TX + 2, NTT = (TX + 2) * (TY + 2);    // vcell ring (tile + 1)
+  // halo copy: raw A and B planes (NPT float4 each, B at a 128-byte boundary)
+  // and the mask block (PY rows of MW bytes), in float4 slots of shared memory
+  static constexpr int MW = mask_box_width(PX);
+  static constexpr int NPT8 = (NPT + 7) / 8 * 8;
+  static constexpr int MASKF4 = (MW * PY + 127) / 128 * 8;
+  static constexpr unsigned HALO_BYTES = 2u * 16u * NPT + unsigned(MW) * PY;
 };
-using Tile0 = TileT<TILE_TX[0], TILE_TY[0], TILE_NT[0], TILE_WARPS[0]>;
-using Tile1 = TileT<TILE_TX[1], TILE_TY[1], TILE_NT[1], TILE_WARPS[1]>;
-using Tile2 = TileT<TILE_TX[2], TILE_TY[2], TILE_NT[2], TILE_WARPS[2]>;
-using Tile3 = TileT<TILE_TX[3], TILE_TY[3], TILE_NT[3], TILE_WARPS[3]>;
-using Tile4 = TileT<TILE_TX[4], TILE_TY[4], TILE_NT[4], TILE_WARPS[4]>;
+using Tile0 = TileT<TILE_TX[0], TILE_TY[0], TILE_NT[0], TILE_WARPS[0], 0>;
+using Tile1 = TileT<TILE_TX[1], TILE_TY[1], TILE_NT[1], TILE_WARPS[1], 1>;
+using Tile2 = TileT<TILE_TX[2], TILE_TY[2], TILE_NT[2], TILE_WARPS[2], 2>;
+using Tile3 = TileT<TILE_TX[3], TILE_TY[3], TILE_NT[3], TILE_WARPS[3], 3>;
+using Tile4 = TileT<TILE_TX[4], TILE_TY[4], TILE_NT[4], TILE_WARPS[4], 4>;
 static_assert(Tile0::NC <= Tile0::NT && Tile1::NC <= Tile1::NT && Tile2::NC <= Tile2::NT && Tile3::NC <= Tile3::NT &&
                   Tile4::NC <= Tile4::NT,
               "a thread per cell");
+static_assert(4 * Tile3::PX <= 256 && Tile3::MW <= 256 && Tile0::PY <= 256, "copy boxes within 256 elements");
+
+// Polls of the halo copy's mbarrier before a block gives up (each poll waits
+// a short hardware-defined time): far beyond any copy, short of a hang.
+constexpr unsigned HALO_WAIT_POLLS = 1u << 22;
 
 // --------------------------------------------------------------------------
 // block-wide max of non-negative floats -> one atomicMax on the bit pattern
@@ -85,6 +96,12 @@ __device__ __forceinline__ void block_max_to(float w, unsigned* out, float* red)
   }
 }
 
+// The dynamic shared memory rounded up to a 128-byte boundary (the halo
+// copies' destinations are 128-byte aligned; every layout reserves the slack).
+__device__ __forceinline__ float4* aligned_smem(float4* p) {
+  return reinterpret_cast<float4*>((reinterpret_cast<uintptr_t>(p) + 127) & ~uintptr_t(127));
+}
+
 // Shared-memory index of the primitive of cell (mx + dx, my + dy) for listed
 // member e: tile cells live in the PX x PY tile array, listed members'
 // neighbourhoods in 5x5 blocks after it.
@@ -93,75 +110,46 @@ __device__ __forceinline__ int ext_prim(int e, int dx, int dy) {
   return T::NPT + e * 25 + (dy + 2) * 5 + (dx + 2);
 }
 
-// Coordinates of primitive slot k (tile first, then one 5x5 block per member).
-template <class T>
-__device__ __forceinline__ void prim_slot(int k, int x0, int y0, const int* xc, int Nx, int& i, int& j) {
-  if (k < T::NPT) {
-    const int ly = k / T::PX;
-    i = x0 - 2 + (k - ly * T::PX);
-    j = y0 - 2 + ly;
-  } else {
-    const int q = k - T::NPT, e = q / 25, r = q - e * 25, m = xc[e];
-    const int dy = r / 5;
-    i = m % Nx + (r - dy * 5) - 2;
-    j = m / Nx + dy - 2;
-  }
-}
-
-// Stencil of face slot k: the 4 cells along the normal (c0..c3), the 4
-// transverse sensor cells (k1+t, k1-t, ij+t, ij-t) as primitive slots, the
-// face position (i, j), its direction, and whether the reference draws it.
+// Faces of listed member e (slots NXF + NRF + 4e + w, w = W, E, S, N): the
+// face position, its direction, whether the reference draws it, and its
+// stencil as primitive slots (the 4 cells along the normal c0..c3, the 4
+// transverse sensor cells k1+t, k1-t, ij+t, ij-t).
 struct FaceSlot {
   int c[4], s[4];
   int i, j;
   bool dirR, valid;
 };
 template <class T>
-__device__ __forceinline__ FaceSlot face_slot(int k, int x0, int y0, const int* xc, int Nx, int Nr) {
-  constexpr int PX = T::PX, TX = T::TX;
+__device__ __forceinline__ FaceSlot member_face_slot(int q, const int* xc, int Nx) {
   FaceSlot f;
-  if (k < T::NXF) {                                // x-face (i, j): west face of cell (i, j)
-    const int ly = k / (TX + 1), lx = k - ly * (TX + 1), py = ly + 2;
-    f.i = x0 + lx; f.j = y0 + ly; f.dirR = false;
-    f.valid = f.i <= Nx && f.j < Nr;
-    const int b = py * PX + lx;
-    f.c[0] = b; f.c[1] = b + 1; f.c[2] = b + 2; f.c[3] = b + 3;
-    f.s[0] = b + PX + 1; f.s[1] = b - PX + 1; f.s[2] = b + PX + 2; f.s[3] = b - PX + 2;
-  } else if (k < T::NXF + T::NRF) {                // r-face (i, j): south face of cell (i, j)
-    const int kk = k - T::NXF, ly = kk / TX, lx = kk - ly * TX, px = lx + 2;
-    f.i = x0 + lx; f.j = y0 + ly; f.dirR = true;
-    f.valid = f.i < Nx && f.j <= Nr && f.j != 0;
-    const int b = ly * PX + px;
-    f.c[0] = b; f.c[1] = b + PX; f.c[2] = b + 2 * PX; f.c[3] = b + 3 * PX;
-    f.s[0] = b + PX + 1; f.s[1] = b + PX - 1; f.s[2] = b + 2 * PX + 1; f.s[3] = b + 2 * PX - 1;
-  } else {                                         // faces of listed member e: W, E, S, N
-    const int q = k - T::NXF - T::NRF, e = q >> 2, w = q & 3, m = xc[e];
-    const int mx = m % Nx, my = m / Nx;
-    if (w < 2) {
-      const int o = w;                             // face at mx + o
-      f.i = mx + o; f.j = my; f.dirR = false; f.valid = true;
-      f.c[0] = ext_prim<T>(e, o - 2, 0); f.c[1] = ext_prim<T>(e, o - 1, 0);
-      f.c[2] = ext_prim<T>(e, o, 0); f.c[3] = ext_prim<T>(e, o + 1, 0);
-      f.s[0] = ext_prim<T>(e, o - 1, 1); f.s[1] = ext_prim<T>(e, o - 1, -1);
-      f.s[2] = ext_prim<T>(e, o, 1); f.s[3] = ext_prim<T>(e, o, -1);
-    } else {
-      const int o = w - 2;                         // face at my + o
-      f.i = mx; f.j = my + o; f.dirR = true; f.valid = f.j != 0;
-      f.c[0] = ext_prim<T>(e, 0, o - 2); f.c[1] = ext_prim<T>(e, 0, o - 1);
-      f.c[2] = ext_prim<T>(e, 0, o); f.c[3] = ext_prim<T>(e, 0, o + 1);
-      f.s[0] = ext_prim<T>(e, 1, o - 1); f.s[1] = ext_prim<T>(e, -1, o - 1);
-      f.s[2] = ext_prim<T>(e, 1, o); f.s[3] = ext_prim<T>(e, -1, o);
-    }
+  const int e = q >> 2, w = q & 3, m = xc[e];
+  const int mx = m % Nx, my = m / Nx;
+  if (w < 2) {
+    const int o = w;                             // face at mx + o
+    f.i = mx + o; f.j = my; f.dirR = false; f.valid = true;
+    f.c[0] = ext_prim<T>(e, o - 2, 0); f.c[1] = ext_prim<T>(e, o - 1, 0);
+    f.c[2] = ext_prim<T>(e, o, 0); f.c[3] = ext_prim<T>(e, o + 1, 0);
+    f.s[0] = ext_prim<T>(e, o - 1, 1); f.s[1] = ext_prim<T>(e, o - 1, -1);
+    f.s[2] = ext_prim<T>(e, o, 1); f.s[3] = ext_prim<T>(e, o, -1);
+  } else {
+    const int o = w - 2;                         // face at my + o
+    f.i = mx; f.j = my + o; f.dirR = true; f.valid = f.j != 0;
+    f.c[0] = ext_prim<T>(e, 0, o - 2); f.c[1] = ext_prim<T>(e, 0, o - 1);
+    f.c[2] = ext_prim<T>(e, 0, o); f.c[3] = ext_prim<T>(e, 0, o + 1);
+    f.s[0] = ext_prim<T>(e, 1, o - 1); f.s[1] = ext_prim<T>(e, -1, o - 1);
+    f.s[2] = ext_prim<T>(e, 1, o); f.s[3] = ext_prim<T>(e, -1, o);
   }
   return f;
 }
 
-// The four face slots (W, E, S, N) of group member (cx, cy).
+// The four face slots (W, E, S, N) of group member (cx, cy): tile faces for a
+// tile cell (x-face ly*(TX+1)+lx, r-face NXF + ly*TX + lx), else the faces of
+// its entry in the tile's member list.
 template <class T>
 __device__ __forceinline__ void member_faces(int cx, int cy, int x0, int y0, const int* xc, int xn, int Nx,
                                              int& fw, int& fe, int& fs, int& fn) {
   const int mx = cx - x0, my = cy - y0;
-  if (mx >= 0 && mx < T::TX && my >= 0 && my < T::TY) {
+  if (unsigned(mx) < unsigned(T::TX) && unsigned(my) < unsigned(T::TY)) {
     fw = my * (T::TX + 1) + mx;
     fe = fw + 1;
     fs = T::NXF + my * T::TX + mx;
@@ -177,130 +165,252 @@ __device__ __forceinline__ void member_faces(int cx, int cy, int x0, int y0, con
   }
 }
 
-// Dynamic shared memory of one block for a largest member list of maxX cells.
+// Dynamic shared memory (float4 slots) of the stage kernel for a member list
+// of xn cells: 128-byte alignment slack, the mask block, the region that holds
+// the raw halo copy and then the face fluxes F, Y, O, the face areas and the
+// primitives W, Wb.
+template <class T>
+__host__ __device__ constexpr int stage_region_t(int xn) {
+  return 2 * T::NPT8 > 2 * (T::NXF + T::NRF + 4 * xn) + (T::NXF + T::NRF + 4 * xn + 3) / 4
+             ? 2 * T::NPT8
+             : 2 * (T::NXF + T::NRF + 4 * xn) + (T::NXF + T::NRF + 4 * xn + 3) / 4;
+}
 template <class T>
 __host__ __device__ constexpr size_t stage_smem_t(int maxX) {
-  return sizeof(float4) * (2 * (T::NPT + 25 * maxX) + 2 * (T::NXF + T::NRF + 4 * maxX)) +
-         sizeof(float) * 2 * (T::NXF + T::NRF + 4 * maxX);
+  return sizeof(float4) * (8 + T::MASKF4 + stage_region_t<T>(maxX) + (T::NXF + T::NRF + 4 * maxX + 3) / 4 +
+                           2 * (T::NPT + 25 * maxX));
 }
+
 // --------------------------------------------------------------------------
 // Phases shared by the stage, physics and fused kernels. Each loops its slots
 // over the block's threads; the caller puts the barriers between phases.
 
-// Open area of face slot k as the reference reads it from geoA (0 where the
-// face is not drawn).
+// Open area of tile x-face k (west face of cell (x0 + lx, y0 + ly)) and tile
+// r-face k (south face), as the reference reads them from geoA; 0 where the
+// face is not drawn (x: i <= Nx, j < Nr; r: i < Nx, 0 < j <= Nr).
 template <class T>
-__device__ __forceinline__ float face_area(const Grid& g, int k, int x0, int y0, const int* xc) {
-  const FaceSlot s = face_slot<T>(k, x0, y0, xc, g.Nx, g.Nr);
+__device__ __forceinline__ float xface_area(const Grid& g, int k, int x0, int y0) {
+  const int ly = k / (T::TX + 1), lx = k - ly * (T::TX + 1), i = x0 + lx, j = y0 + ly;
+  return (i <= g.Nx && j < g.Nr) ? g.geoA[j * (g.Nx + 1) + i].z : 0.0f;
+}
+template <class T>
+__device__ __forceinline__ float rface_area(const Grid& g, int k, int x0, int y0) {
+  const int ly = k / T::TX, lx = k - ly * T::TX, i = x0 + lx, j = y0 + ly;
+  return (i < g.Nx && j <= g.Nr && j != 0) ? g.geoA[j * (g.Nx + 1) + i].w : 0.0f;
+}
+template <class T>
+__device__ __forceinline__ float member_face_area(const Grid& g, int q, const int* xc) {
+  const FaceSlot s = member_face_slot<T>(q, xc, g.Nx);
   if (!s.valid) return 0.0f;
   const float4* p = g.geoA + (s.j * (g.Nx + 1) + s.i);
   return s.dirR ? p->w : p->z;
 }
 
-// State and mask of a thread's first two primitive slots (tid, tid + NT) where
-// they are tile slots and grid cells: loads that need neither the member list
-// nor the step info, so a block issues them first and they overlap those.
-struct PrimPair {
-  float4 a[2], b[2];
-  uint8_t m[2];
-  bool in[2];
-};
+// Start of a stage kernel's block: thread 0 initialises the halo copy's
+// mbarrier and issues the three tiled copies of the tile + 2-cell halo (raw A
+// into R, raw B into R + NPT8, the mask block into sMask). The mask box starts
+// at the 16-byte boundary at or below the halo's first column.
 template <class T>
-__device__ __forceinline__ PrimPair prefetch_prims(const Grid& g, const float4* __restrict__ A,
-                                                   const float4* __restrict__ B, int x0, int y0) {
-  PrimPair p = {};
-  if constexpr (T::WIDE) {                       // otherwise load_prims loads them itself
-#pragma unroll
-    for (int u = 0; u < 2; u++) {
-      const int k = threadIdx.x + u * T::NT;
-      if (k < T::NPT) {
-        int i, j;
-        prim_slot<T>(k, x0, y0, nullptr, g.Nx, i, j);   // a tile slot: the member list is not read
-        p.in[u] = i >= 0 && i < g.Nx && j >= 0 && j < g.Nr;
-        if (p.in[u]) {
-          const int c = j * g.Nx + i;
-          p.a[u] = A[c];
-          p.b[u] = B[c];
-          p.m[u] = g.mask[c];
-        }
-      }
-    }
+__device__ __forceinline__ void halo_issue(const TileMaps* tm, int slot, int x0, int y0, float4* R, uint8_t* sMask,
+                                           uint64_t* bar) {
+  if (threadIdx.x == 0) {
+    const TileMaps& M = tm[T::ID];
+    mbar_init(bar, 1);
+    mbar_expect_tx(bar, T::HALO_BYTES);
+    tma_load_2d(R, &M.a[slot], 4 * (x0 - 2), y0 - 2, bar);
+    tma_load_2d(R + T::NPT8, &M.b[slot], 4 * (x0 - 2), y0 - 2, bar);
+    tma_load_2d(sMask, &M.mask, (x0 - 2) & ~15, y0 - 2, bar);
   }
-  return p;
+}
+// Every thread waits for the halo copy (after a barrier that published the
+// mbarrier's initialisation). False, in every thread, when any thread gave
+// up; the block then records the error and leaves.
+__device__ __forceinline__ bool halo_wait(uint64_t* bar, unsigned* err) {
+  const bool ok = mbar_wait_bounded(bar, HALO_WAIT_POLLS);
+  if (__syncthreads_and(ok)) return true;
+  if (threadIdx.x == 0 && err) atomicOr(err, 1u);
+  return false;
 }
 
-// FS_PRIM: ghost-cell primitives of the tile + 2-cell halo, then the listed
-// members' 5x5 blocks. The open areas of the NF faces go to sAr on the way:
-// a thread's first two are loaded before its primitives and stored after
-// them, so their latency hides behind the primitive phase.
+// Cells of the staged halo block (raw A, B and mask in shared memory) for
+// ghost_prim_c: every cell a ghost slot reads lies within the block.
+template <class T>
+struct TileCells {
+  const float4* rA;
+  const float4* rB;
+  const uint8_t* m;
+  int x0, y0, mo;
+  __device__ __forceinline__ int slot(int i, int j) const { return (j - y0 + 2) * T::PX + (i - x0 + 2); }
+  __device__ __forceinline__ bool solid(int i, int j) const {
+    return m[(j - y0 + 2) * T::MW + mo + (i - x0 + 2)] != 0;
+  }
+  __device__ __forceinline__ float4 a(int i, int j) const { return rA[slot(i, j)]; }
+  __device__ __forceinline__ float4 b(int i, int j) const { return rB[slot(i, j)]; }
+};
+
+// FS_PRIM: ghost-cell primitives of the tile + 2-cell halo from the staged
+// block, then the listed members' 5x5 blocks from global memory.
 template <class T>
 __device__ __forceinline__ void load_prims(const Grid& g, const float4* __restrict__ A, const float4* __restrict__ B,
                                            float t, const rn_params& P, int x0, int y0, const int* xc, int NP,
-                                           float4* sW, float4* sWb, int NF, float* sAr, const PrimPair& pf) {
+                                           const float4* R, const uint8_t* sMask, float4* sW, float4* sWb) {
   const int Nx = g.Nx, Nr = g.Nr;
-  const int f0 = threadIdx.x, f1 = threadIdx.x + T::NT;
-  const float ar0 = f0 < NF ? face_area<T>(g, f0, x0, y0, xc) : 0.0f;
-  const float ar1 = f1 < NF ? face_area<T>(g, f1, x0, y0, xc) : 0.0f;
-  // Two slots per round: the state and mask of both (where they are grid
-  // cells) are loaded before either is converted, so the two rounds' loads
-  // overlap. Ghost slots outside the grid take ghost_prim's boundary branches.
-  for (int k0 = threadIdx.x; k0 < NP; k0 += 2 * T::NT) {
-    const int k1 = k0 + T::NT;
-    int i0, j0, i1 = -1, j1 = -1;
-    prim_slot<T>(k0, x0, y0, xc, Nx, i0, j0);
-    if (k1 < NP) prim_slot<T>(k1, x0, y0, xc, Nx, i1, j1);
-    const bool in0 = i0 >= 0 && i0 < Nx && j0 >= 0 && j0 < Nr;
-    const bool in1 = k1 < NP && i1 >= 0 && i1 < Nx && j1 >= 0 && j1 < Nr;
-    float4 a0, b0, a1, b1;
-    uint8_t m0 = 0, m1 = 0;
-    const bool first = T::WIDE && k0 == int(threadIdx.x);   // the round prefetch_prims loaded (tile slots)
-    if (first && k0 < T::NPT) { a0 = pf.a[0]; b0 = pf.b[0]; m0 = pf.m[0]; }
-    else if (in0) { const int c = j0 * Nx + i0; a0 = A[c]; b0 = B[c]; m0 = g.mask[c]; }
-    if (first && k1 < T::NPT) { a1 = pf.a[1]; b1 = pf.b[1]; m1 = pf.m[1]; }
-    else if (in1) { const int c = j1 * Nx + i1; a1 = A[c]; b1 = B[c]; m1 = g.mask[c]; }
-#pragma unroll
-    for (int u = 0; u < 2; u++) {
-      const int k = u ? k1 : k0, i = u ? i1 : i0, j = u ? j1 : j0;
-      if (k >= NP) break;
-      float4 W, Wb;
-      if (u ? in1 : in0) {                       // ghost_prim's interior branch
-        if (u ? m1 : m0) {
-          W = make_float4(-1.0f, 0.0f, 0.0f, 1.0f);
-          Wb = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        } else {
-          const Prim q = to_prim(u ? a1 : a0, u ? b1 : b0);
-          W = q.w;
-          Wb = q.s;
-        }
-      } else if (i <= Nx + 1 && j <= Nr + 1) {
-        ghost_prim(g, A, B, i, j, t, P, W, Wb);
+  const TileCells<T> cells{R, R + T::NPT8, sMask, x0, y0, (x0 - 2) - ((x0 - 2) & ~15)};
+  for (int k = threadIdx.x; k < T::NPT; k += T::NT) {
+    const int ly = k / T::PX, lx = k - ly * T::PX;
+    const int i = x0 - 2 + lx, j = y0 - 2 + ly;
+    float4 W, Wb;
+    if (i >= 0 && i < Nx && j >= 0 && j < Nr) {     // ghost_prim's interior branch
+      if (sMask[ly * T::MW + cells.mo + lx]) {
+        W = make_float4(-1.0f, 0.0f, 0.0f, 1.0f);
+        Wb = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
       } else {
-        W = make_float4(-1.f, 0.f, 0.f, 1.f); Wb = make_float4(0.f, 0.f, 0.f, 0.f);
+        const Prim q = to_prim(cells.rA[k], cells.rB[k]);
+        W = q.w;
+        Wb = q.s;
       }
-      sW[k] = W;
-      sWb[k] = Wb;
+    } else if (i <= Nx + 1 && j <= Nr + 1) {
+      ghost_prim_c(Nx, Nr, cells, i, j, t, P, W, Wb);
+    } else {
+      W = make_float4(-1.f, 0.f, 0.f, 1.f); Wb = make_float4(0.f, 0.f, 0.f, 0.f);
     }
+    sW[k] = W;
+    sWb[k] = Wb;
   }
-  if (f0 < NF) sAr[f0] = ar0;
-  if (f1 < NF) sAr[f1] = ar1;
-  for (int k = f1 + T::NT; k < NF; k += T::NT) sAr[k] = face_area<T>(g, k, x0, y0, xc);
+  // listed members' 5x5 blocks (slivers merged across the tile edge)
+  for (int k = T::NPT + threadIdx.x; k < NP; k += T::NT) {
+    const int q = k - T::NPT, e = q / 25, r = q - e * 25, m = xc[e];
+    const int dy = r / 5;
+    const int i = m % Nx + (r - dy * 5) - 2, j = m / Nx + dy - 2;
+    float4 W, Wb;
+    if (i >= 0 && i < Nx && j >= 0 && j < Nr) {
+      const int c = j * Nx + i;
+      const float4 a = A[c], b = B[c];
+      if (g.mask[c]) {
+        W = make_float4(-1.0f, 0.0f, 0.0f, 1.0f);
+        Wb = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      } else {
+        const Prim p = to_prim(a, b);
+        W = p.w;
+        Wb = p.s;
+      }
+    } else if (i <= Nx + 1 && j <= Nr + 1) {
+      ghost_prim(g, A, B, i, j, t, P, W, Wb);
+    } else {
+      W = make_float4(-1.f, 0.f, 0.f, 1.f); Wb = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    sW[k] = W;
+    sWb[k] = Wb;
+  }
+}
+
+// Face areas into sAr: a thread's first x- and r-face (loaded at block start,
+// their latency hidden behind the halo copy), the rest of the tile's faces
+// (shapes with more faces than threads), then the listed members' faces.
+struct FirstAreas {
+  float x, r;
+};
+template <class T>
+__device__ __forceinline__ FirstAreas first_areas(const Grid& g, int x0, int y0) {
+  FirstAreas f;
+  const int tid = threadIdx.x;
+  f.x = tid < T::NXF ? xface_area<T>(g, tid, x0, y0) : 0.0f;
+  f.r = tid < T::NRF ? rface_area<T>(g, tid, x0, y0) : 0.0f;
+  return f;
+}
+template <class T>
+__device__ __forceinline__ void store_areas(const Grid& g, int x0, int y0, const int* xc, int xn, FirstAreas f,
+                                            float* sAr) {
+  const int tid = threadIdx.x;
+  if (tid < T::NXF) sAr[tid] = f.x;
+  if (tid < T::NRF) sAr[T::NXF + tid] = f.r;
+  if constexpr (T::NXF > T::NT)
+    for (int k = tid + T::NT; k < T::NXF; k += T::NT) sAr[k] = xface_area<T>(g, k, x0, y0);
+  if constexpr (T::NRF > T::NT)
+    for (int k = tid + T::NT; k < T::NRF; k += T::NT) sAr[T::NXF + k] = rface_area<T>(g, k, x0, y0);
+  for (int q = tid; q < 4 * xn; q += T::NT) sAr[T::NXF + T::NRF + q] = member_face_area<T>(g, q, xc);
+}
+
+// One tile face of direction DIR_R whose first normal cell is primitive slot
+// b: the normal cells b + n*d and the sensor cells (k1 +- t, ij +- t) of
+// makeFluxShader (solver.js:133-259) sit at fixed offsets from b.
+template <class T, bool DIR_R>
+__device__ __forceinline__ void tile_face(const rn_params& P, int b, float area, const float4* sW, const float4* sWb,
+                                          float4* sF, float4* sY, float* sO, int out) {
+  constexpr int d = DIR_R ? T::PX : 1, t = DIR_R ? 1 : T::PX;
+  Flux f;
+  f.F = make_float4(0.f, 0.f, 0.f, 0.f); f.Y = f.F; f.O = 0.f;
+  if (area != 0.0f)
+    f = face_flux<DIR_R>(area, sW[b], sWb[b], sW[b + d], sWb[b + d], sW[b + 2 * d], sWb[b + 2 * d], sW[b + 3 * d],
+                         sWb[b + 3 * d], sW[b + d + t], sW[b + d - t], sW[b + 2 * d + t], sW[b + 2 * d - t], P);
+  sF[out] = f.F; sY[out] = f.Y; sO[out] = f.O;
+}
+// A listed member's face (direction known only at run time; rare): kept out
+// of line so that the tile face loops hold the only inlined flux code.
+template <class T>
+__device__ __noinline__ void member_face(const rn_params& P, int q, const int* xc, int Nx, float area,
+                                         const float4* sW, const float4* sWb, float4* sF, float4* sY, float* sO) {
+  const FaceSlot s = member_face_slot<T>(q, xc, Nx);
+  Flux f;
+  f.F = make_float4(0.f, 0.f, 0.f, 0.f); f.Y = f.F; f.O = 0.f;
+  if (area != 0.0f) {
+    if (s.dirR)
+      f = face_flux<true>(area, sW[s.c[0]], sWb[s.c[0]], sW[s.c[1]], sWb[s.c[1]], sW[s.c[2]], sWb[s.c[2]],
+                          sW[s.c[3]], sWb[s.c[3]], sW[s.s[0]], sW[s.s[1]], sW[s.s[2]], sW[s.s[3]], P);
+    else
+      f = face_flux<false>(area, sW[s.c[0]], sWb[s.c[0]], sW[s.c[1]], sWb[s.c[1]], sW[s.c[2]], sWb[s.c[2]],
+                           sW[s.c[3]], sWb[s.c[3]], sW[s.s[0]], sW[s.s[1]], sW[s.s[2]], sW[s.s[3]], P);
+  }
+  const int k = T::NXF + T::NRF + q;
+  sF[k] = f.F; sY[k] = f.Y; sO[k] = f.O;
 }
 
 // FS_FLUX_X/R: tile x-faces, tile r-faces, members' faces.
 template <class T>
-__device__ __forceinline__ void inviscid_faces(const Grid& g, const rn_params& P, int x0, int y0, const int* xc,
-                                               int NF, const float4* sW, const float4* sWb, float4* sF, float4* sY,
+__device__ __forceinline__ void inviscid_faces(const Grid& g, const rn_params& P, const int* xc, int xn,
+                                               const float4* sW, const float4* sWb, float4* sF, float4* sY,
                                                float* sO, const float* sAr) {
-  const int Nx = g.Nx, Nr = g.Nr;
-  for (int k = threadIdx.x; k < NF; k += T::NT) {
-    const FaceSlot s = face_slot<T>(k, x0, y0, xc, Nx, Nr);
-    Flux f;
-    f.F = make_float4(0.f, 0.f, 0.f, 0.f); f.Y = f.F; f.O = 0.f;
-    const float area = sAr[k];   // the face's open area, 0 where it is not drawn (load_prims)
-    if (area != 0.0f)
-      f = face_flux(s.dirR, area, sW[s.c[0]], sWb[s.c[0]], sW[s.c[1]], sWb[s.c[1]], sW[s.c[2]], sWb[s.c[2]],
-                    sW[s.c[3]], sWb[s.c[3]], sW[s.s[0]], sW[s.s[1]], sW[s.s[2]], sW[s.s[3]], P);
-    sF[k] = f.F; sY[k] = f.Y; sO[k] = f.O;
+  for (int k = threadIdx.x; k < T::NXF; k += T::NT) {
+    const int ly = k / (T::TX + 1), lx = k - ly * (T::TX + 1);
+    tile_face<T, false>(P, (ly + 2) * T::PX + lx, sAr[k], sW, sWb, sF, sY, sO, k);
+  }
+  for (int k = threadIdx.x; k < T::NRF; k += T::NT) {
+    const int ly = k / T::TX, lx = k - ly * T::TX;
+    tile_face<T, true>(P, ly * T::PX + lx + 2, sAr[T::NXF + k], sW, sWb, sF, sY, sO, T::NXF + k);
+  }
+  for (int q = threadIdx.x; q < 4 * xn; q += T::NT)
+    member_face<T>(P, q, xc, g.Nx, sAr[T::NXF + T::NRF + q], sW, sWb, sF, sY, sO);
+}
+
+// memberFlux (solver.js:287-299) of group member (cx, cy): its four faces'
+// fluxes weighted by their open areas (0 on the axis face, whose flux is 0 too).
+template <class T, bool WITH_O>
+__device__ __forceinline__ void add_member(int cx, int cy, int x0, int y0, const int* xc, int xn, int Nx,
+                                           const float4* sF, const float4* sY, const float* sO, const float* sAr,
+                                           float4& L, float4& LY, float& LO) {
+  int fw, fe, fs, fn;
+  member_faces<T>(cx, cy, x0, y0, xc, xn, Nx, fw, fe, fs, fn);
+  const float aw = fabsf(sAr[fw]), ae = fabsf(sAr[fe]), as_ = fabsf(sAr[fs]), an = fabsf(sAr[fn]);
+  sub4(L, ae, sF[fe], aw, sF[fw]);
+  sub4(L, an, sF[fn], as_, sF[fs]);
+  sub4(LY, ae, sY[fe], aw, sY[fw]);
+  sub4(LY, an, sY[fn], as_, sY[fs]);
+  if constexpr (WITH_O) {
+    LO -= ae * sO[fe] - aw * sO[fw];
+    LO -= an * sO[fn] - as_ * sO[fs];
+  }
+}
+// The group of host (Hx, Hy) with slave mask sm_: the host, then its slaves in
+// the reference's member order (slave bits 1, 2, 4, 8 = W, E, S, N).
+template <class T, bool WITH_O>
+__device__ __forceinline__ void group_flux(int Hx, int Hy, int sm_, int x0, int y0, const int* xc, int xn, int Nx,
+                                           const float4* sF, const float4* sY, const float* sO, const float* sAr,
+                                           float4& L, float4& LY, float& LO) {
+  add_member<T, WITH_O>(Hx, Hy, x0, y0, xc, xn, Nx, sF, sY, sO, sAr, L, LY, LO);
+  for (int s = sm_ & 15; s != 0; s &= s - 1) {
+    const int bit = __ffs(s) - 1;
+    const int cx = Hx + (bit == 0 ? -1 : bit == 1 ? 1 : 0), cy = Hy + (bit == 2 ? -1 : bit == 3 ? 1 : 0);
+    add_member<T, WITH_O>(cx, cy, x0, y0, xc, xn, Nx, sF, sY, sO, sAr, L, LY, LO);
   }
 }
 
@@ -335,26 +445,8 @@ __device__ __forceinline__ bool update_cell(const StageArgs& a, const rn_params&
   float4 L = make_float4(0.f, 0.f, 0.f, 0.f), LY = L;
   float LO = 0.0f;
   const int sm_ = iround(ghz);
-  for (int m = 0; m < 5; m++) {
-    int cx = Hx, cy = Hy;
-    if (m == 1) { if (!(sm_ & 1)) continue; cx -= 1; }
-    else if (m == 2) { if (!(sm_ & 2)) continue; cx += 1; }
-    else if (m == 3) { if (!(sm_ & 4)) continue; cy -= 1; }
-    else if (m == 4) { if (!(sm_ & 8)) continue; cy += 1; }
-    // the member's four faces; their open areas are the ones the face phase
-    // read from geoA (0 on the axis face, whose flux is 0 too)
-    int fw, fe, fs, fn;
-    member_faces<T>(cx, cy, x0, y0, xc, xn, Nx, fw, fe, fs, fn);
-    const float aw = fabsf(sAr[fw]), ae = fabsf(sAr[fe]), as_ = fabsf(sAr[fs]), an = fabsf(sAr[fn]);
-    sub4(L, ae, sF[fe], aw, sF[fw]);
-    sub4(L, an, sF[fn], as_, sF[fs]);
-    sub4(LY, ae, sY[fe], aw, sY[fw]);
-    sub4(LY, an, sY[fn], as_, sY[fs]);
-    if (P.inj) {
-      LO -= ae * sO[fe] - aw * sO[fw];
-      LO -= an * sO[fn] - as_ * sO[fs];
-    }
-  }
+  if (P.inj) group_flux<T, true>(Hx, Hy, sm_, x0, y0, xc, xn, Nx, sF, sY, sO, sAr, L, LY, LO);
+  else group_flux<T, false>(Hx, Hy, sm_, x0, y0, xc, xn, Nx, sF, sY, sO, sAr, L, LY, LO);
   // embedded wall: pressure force along the r-weighted wall vector
   float wl = len2(gg.z, gg.w);
   if (wl > 1e-6f) {
@@ -407,21 +499,25 @@ __device__ __forceinline__ bool update_cell(const StageArgs& a, const rn_params&
 // One RK stage on tile (bx, by) = tile index tileId of the instance in `a`.
 template <class T, int STAGE>
 __device__ __forceinline__ void stage_body(const StageArgs& a, const rn_params& P, int bx, int by, int tileId,
-                                           float4* sm, float* red, int* xc) {
+                                           float4* smRaw, float* red, int* xc, uint64_t* bar) {
   constexpr int TX = T::TX, NT = T::NT;
   const Grid& g = a.g;
   const int Nx = g.Nx, Nr = g.Nr;
   const int tid = threadIdx.x;
   const int x0 = bx * TX, y0 = by * T::TY;
-  const PrimPair pf = prefetch_prims<T>(g, a.A, a.B, x0, y0);
+  float4* sm = aligned_smem(smRaw);
+  uint8_t* sMask = reinterpret_cast<uint8_t*>(sm);
+  float4* R = sm + T::MASKF4;
+  halo_issue<T>(a.tm, a.slotIn, x0, y0, R, sMask, bar);
+  const FirstAreas fa = first_areas<T>(g, x0, y0);
   const int xb = a.xoff[tileId], xn = a.xoff[tileId + 1] - xb;
   const int NP = T::NPT + 25 * xn, NF = T::NXF + T::NRF + 4 * xn;
-  float4* sW = sm;
-  float4* sWb = sW + NP;
-  float4* sF = sWb + NP;
+  float4* sF = R;
   float4* sY = sF + NF;
   float* sO = reinterpret_cast<float*>(sY + NF);
-  float* sAr = sO + NF;
+  float* sAr = reinterpret_cast<float*>(R + stage_region_t<T>(xn));
+  float4* sW = reinterpret_cast<float4*>(sAr) + (NF + 3) / 4;
+  float4* sWb = sW + NP;
   for (int q = tid; q < xn; q += NT) xc[q] = a.xcell[xb + q];
 
   float dt, t;
@@ -441,9 +537,11 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const rn_params& 
     t = st.z;                                     // inlet ramp at t_new
   }
   __syncthreads();
-  load_prims<T>(g, a.A, a.B, t, P, x0, y0, xc, NP, sW, sWb, NF, sAr, pf);
+  if (!halo_wait(bar, a.err)) return;
+  load_prims<T>(g, a.A, a.B, t, P, x0, y0, xc, NP, R, sMask, sW, sWb);
+  store_areas<T>(g, x0, y0, xc, xn, fa, sAr);
   __syncthreads();
-  inviscid_faces<T>(g, P, x0, y0, xc, NF, sW, sWb, sF, sY, sO, sAr);
+  inviscid_faces<T>(g, P, xc, xn, sW, sWb, sF, sY, sO, sAr);
   __syncthreads();
 
   const int i = x0 + tid % TX, j = y0 + tid / TX;
@@ -460,83 +558,86 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const rn_params& 
 }
 
 // --------------------------------------------------------------------------
-// vcell slot k: the tile + 1 ring first, then 5 cells per listed member
-// (itself, W, E, S, N). Returns the cell and the primitive slots of the cell
-// and its E, W, N, S neighbours.
+// FS_VCELL of vcell slot k of the tile + 1 ring (k < NTT) or, after it, of a
+// listed member's cell or one of its 4 neighbours (itself, W, E, S, N).
 template <class T>
-__device__ __forceinline__ void vcell_slot(int k, int x0, int y0, const int* xc, int Nx, int& i, int& j, int& c,
-                                           int& e_, int& w_, int& n_, int& s_) {
+__device__ __forceinline__ void vcell_at(const Grid& g, const rn_params& P, float dt, int x0, int y0, const int* xc,
+                                         int k, const float4* sW, const float4* sWb, float4* sT1, float4* sT2) {
+  const int Nx = g.Nx, Nr = g.Nr;
+  int i, j, c, rs;
   if (k < T::NTT) {
     const int ly = k / T::TW, lx = k - ly * T::TW;
     i = x0 - 1 + lx; j = y0 - 1 + ly;
     c = (ly + 1) * T::PX + lx + 1;
-    e_ = c + 1; w_ = c - 1; n_ = c + T::PX; s_ = c - T::PX;
+    rs = T::PX;
   } else {
     const int q = k - T::NTT, e = q / 5, r = q - e * 5, m = xc[e];
     const int dx = r == 1 ? -1 : r == 2 ? 1 : 0, dy = r == 3 ? -1 : r == 4 ? 1 : 0;
     i = m % Nx + dx; j = m / Nx + dy;
     c = ext_prim<T>(e, dx, dy);
-    e_ = c + 1; w_ = c - 1; n_ = c + 5; s_ = c - 5;
+    rs = 5;
   }
-}
-
-// FS_VCELL of vcell slot k (the tile + 1 ring, then the members' cells).
-template <class T>
-__device__ __forceinline__ void vcell_at(const Grid& g, const rn_params& P, float dt, int x0, int y0, const int* xc,
-                                         int k, const float4* sW, const float4* sWb, float4* sT1, float4* sT2) {
-  const int Nx = g.Nx, Nr = g.Nr;
-  int i, j, c, e_, w_, n_, s_;
-  vcell_slot<T>(k, x0, y0, xc, Nx, i, j, c, e_, w_, n_, s_);
   float4 T1 = make_float4(0.f, 0.f, 0.f, 0.f), T2 = T1;
   if (i >= 0 && i < Nx && j >= 0 && j < Nr)
-    vcell(sW[c], sWb[c], sW[e_], sW[w_], sW[n_], sW[s_], i, j, g.geoM[j * Nx + i].w, dt, P, T1, T2);
+    vcell(sW[c], sWb[c], sW[c + 1], sW[c - 1], sW[c + rs], sW[c - rs], i, j, g.geoM[j * Nx + i].w, dt, P, T1, T2);
   sT1[k] = T1;
   sT2[k] = T2;
 }
 
+// One viscous face: primitive slots p1 (behind) and p2 (the face's cell),
+// vcell slots v1 and v2; zero flux where it is not drawn or a side is a wall.
+template <bool DIR_R>
+__device__ __forceinline__ void visc_face(bool ok, float area, int j, int p1, int p2, int v1, int v2,
+                                          const float4* sW, const float4* sWb, const float4* sT1, const float4* sT2,
+                                          float4& F, float4& FY) {
+  F = make_float4(0.f, 0.f, 0.f, 0.f);
+  FY = F;
+  if (ok) {
+    const float4 w1 = sW[p1], w2 = sW[p2];
+    if (area != 0.0f && !(w1.x < 0.0f || w2.x < 0.0f))
+      visc_flux<DIR_R>(w1, sWb[p1], sT1[v1], sT2[v1], w2, sWb[p2], sT1[v2], sT2[v2], j, F, FY);
+  }
+}
+template <class T>
+__device__ __noinline__ void visc_member_face(const Grid& g, int q, const int* xc, const float4* sW, const float4* sWb,
+                                              const float4* sT1, const float4* sT2, const float* sAr, float4* sF,
+                                              float4* sY) {
+  const int Nx = g.Nx, Nr = g.Nr;
+  const int e = q >> 2, w = q & 3, m = xc[e];
+  const int mx = m % Nx, my = m / Nx, vb = T::NTT + 5 * e;
+  const float area = sAr[T::NXF + T::NRF + q];
+  float4 F, FY;
+  if (w == 0) visc_face<false>(mx > 0 && mx < Nx && my < Nr, area, my, ext_prim<T>(e, -1, 0), ext_prim<T>(e, 0, 0),
+                               vb + 1, vb, sW, sWb, sT1, sT2, F, FY);
+  else if (w == 1) visc_face<false>(mx + 1 > 0 && mx + 1 < Nx && my < Nr, area, my, ext_prim<T>(e, 0, 0),
+                                    ext_prim<T>(e, 1, 0), vb, vb + 2, sW, sWb, sT1, sT2, F, FY);
+  else if (w == 2) visc_face<true>(mx < Nx && my > 0 && my < Nr, area, my, ext_prim<T>(e, 0, -1), ext_prim<T>(e, 0, 0),
+                                   vb + 3, vb, sW, sWb, sT1, sT2, F, FY);
+  else visc_face<true>(mx < Nx && my + 1 > 0 && my + 1 < Nr, area, my + 1, ext_prim<T>(e, 0, 0), ext_prim<T>(e, 0, 1),
+                       vb, vb + 4, sW, sWb, sT1, sT2, F, FY);
+  sF[T::NXF + T::NRF + q] = F;
+  sY[T::NXF + T::NRF + q] = FY;
+}
+
 // FS_VFLUX_X/R: viscous faces of the tile and of the members.
 template <class T>
-__device__ __forceinline__ void viscous_faces(const Grid& g, int x0, int y0, const int* xc, int NF, const float4* sW,
+__device__ __forceinline__ void viscous_faces(const Grid& g, int x0, int y0, const int* xc, int xn, const float4* sW,
                                               const float4* sWb, const float4* sT1, const float4* sT2,
                                               const float* sAr, float4* sF, float4* sY) {
   constexpr int TX = T::TX, PX = T::PX, TW = T::TW;
   const int Nx = g.Nx, Nr = g.Nr;
-  for (int k = threadIdx.x; k < NF; k += T::NT) {
-    float4 F = make_float4(0.f, 0.f, 0.f, 0.f), FY = F;
-    bool dirR, ok;
-    int i, j, p1, p2, v1, v2;          // primitive and vcell slots of the cells behind (1) and at (2) the face
-    if (k < T::NXF) {
-      const int ly = k / (TX + 1), lx = k - ly * (TX + 1);
-      i = x0 + lx; j = y0 + ly; dirR = false;
-      ok = i > 0 && i < Nx && j < Nr;
-      p2 = (ly + 2) * PX + lx + 2; p1 = p2 - 1;
-      v2 = (ly + 1) * TW + lx + 1; v1 = v2 - 1;
-    } else if (k < T::NXF + T::NRF) {
-      const int kk = k - T::NXF, ly = kk / TX, lx = kk - ly * TX;
-      i = x0 + lx; j = y0 + ly; dirR = true;
-      ok = i < Nx && j > 0 && j < Nr;
-      p2 = (ly + 2) * PX + lx + 2; p1 = p2 - PX;
-      v2 = (ly + 1) * TW + lx + 1; v1 = v2 - TW;
-    } else {
-      const int q = k - T::NXF - T::NRF, e = q >> 2, w = q & 3, m = xc[e];
-      const int mx = m % Nx, my = m / Nx, vb = T::NTT + 5 * e;
-      if (w == 0) { i = mx; j = my; dirR = false; p1 = ext_prim<T>(e, -1, 0); p2 = ext_prim<T>(e, 0, 0); v1 = vb + 1; v2 = vb; }
-      else if (w == 1) { i = mx + 1; j = my; dirR = false; p1 = ext_prim<T>(e, 0, 0); p2 = ext_prim<T>(e, 1, 0); v1 = vb; v2 = vb + 2; }
-      else if (w == 2) { i = mx; j = my; dirR = true; p1 = ext_prim<T>(e, 0, -1); p2 = ext_prim<T>(e, 0, 0); v1 = vb + 3; v2 = vb; }
-      else { i = mx; j = my + 1; dirR = true; p1 = ext_prim<T>(e, 0, 0); p2 = ext_prim<T>(e, 0, 1); v1 = vb; v2 = vb + 4; }
-      ok = dirR ? (i < Nx && j > 0 && j < Nr) : (i > 0 && i < Nx && j < Nr);
-    }
-    if (ok) {
-      // face k is face k of the inviscid phase, whose open area sAr[k] holds
-      // (every face drawn here was drawn there)
-      float area = sAr[k];
-      float4 w1 = sW[p1], w2 = sW[p2];
-      if (area != 0.0f && !(w1.x < 0.0f || w2.x < 0.0f))
-        visc_flux(dirR, w1, sWb[p1], sT1[v1], sT2[v1], w2, sWb[p2], sT1[v2], sT2[v2], j, F, FY);
-    }
-    sF[k] = F;
-    sY[k] = FY;
+  for (int k = threadIdx.x; k < T::NXF; k += T::NT) {
+    const int ly = k / (TX + 1), lx = k - ly * (TX + 1), i = x0 + lx, j = y0 + ly;
+    const int p2 = (ly + 2) * PX + lx + 2, v2 = (ly + 1) * TW + lx + 1;
+    visc_face<false>(i > 0 && i < Nx && j < Nr, sAr[k], j, p2 - 1, p2, v2 - 1, v2, sW, sWb, sT1, sT2, sF[k], sY[k]);
   }
+  for (int k = threadIdx.x; k < T::NRF; k += T::NT) {
+    const int ly = k / TX, lx = k - ly * TX, i = x0 + lx, j = y0 + ly;
+    const int p2 = (ly + 2) * PX + lx + 2, v2 = (ly + 1) * TW + lx + 1;
+    visc_face<true>(i < Nx && j > 0 && j < Nr, sAr[T::NXF + k], j, p2 - PX, p2, v2 - TW, v2, sW, sWb, sT1, sT2,
+                    sF[T::NXF + k], sY[T::NXF + k]);
+  }
+  for (int q = threadIdx.x; q < 4 * xn; q += T::NT) visc_member_face<T>(g, q, xc, sW, sWb, sT1, sT2, sAr, sF, sY);
 }
 
 // FS_SOURCE of cell (i, j) inside the grid. A, B = the stage-2 state of the
@@ -570,20 +671,8 @@ __device__ __forceinline__ bool source_cell(const Grid& g, const float4* __restr
   float4 T1h = sT1[vh], T2h = sT2[vh];
   if (P.visc) {
     const int sm_ = iround(kh == k ? gmij.z : g.geoM[kh].z);
-    for (int m = 0; m < 5; m++) {
-      int cx = Hx, cy = Hy;
-      if (m == 1) { if (!(sm_ & 1)) continue; cx -= 1; }
-      else if (m == 2) { if (!(sm_ & 2)) continue; cx += 1; }
-      else if (m == 3) { if (!(sm_ & 4)) continue; cy -= 1; }
-      else if (m == 4) { if (!(sm_ & 8)) continue; cy += 1; }
-      int fw, fe, fs, fn;
-      member_faces<T>(cx, cy, x0, y0, xc, xn, Nx, fw, fe, fs, fn);
-      const float aw = fabsf(sAr[fw]), ae = fabsf(sAr[fe]), as_ = fabsf(sAr[fs]), an = fabsf(sAr[fn]);
-      sub4(L, ae, sF[fe], aw, sF[fw]);
-      sub4(L, an, sF[fn], as_, sF[fs]);
-      sub4(LY, ae, sY[fe], aw, sY[fw]);
-      sub4(LY, an, sY[fn], as_, sY[fs]);
-    }
+    float LO = 0.0f;
+    group_flux<T, false>(Hx, Hy, sm_, x0, y0, xc, xn, Nx, sF, sY, nullptr, sAr, L, LY, LO);
     // axisymmetric hoop stress
     float r = fdiv(V, fmaxf(gg.y, 1e-6f)), vor = fdiv(vely, r);
     L.z -= T2h.x * (2.0f * vor - 0.6666667f * (T1h.x + T1h.w + vor)) * gg.y;
@@ -676,53 +765,63 @@ __device__ __forceinline__ bool source_cell(const Grid& g, const float4* __restr
 // the tile's cells and of its listed members (every out-of-tile group host a
 // tile cell can have) stay in shared memory and feed FS_SOURCE directly.
 template <class T>
-__host__ __device__ constexpr size_t fused_region_t(int maxX) {
-  // float4 slots of the region that holds first the inviscid faces' F, Y and
-  // O, then (T::WIDE) the viscous faces' F and Y, which need less, or the
-  // vcell ring's T1/T2 and the viscous faces
+__host__ __device__ constexpr int fused_region_t(int maxX) {
+  // float4 slots of the region that holds first the raw halo copy, then the
+  // inviscid faces' F, Y and O, then (T::WIDE) the viscous faces' F and Y,
+  // which need less, or the vcell ring's T1/T2 and the viscous faces
   return T::WIDE || (2 * (T::NXF + T::NRF + 4 * maxX) + ((T::NXF + T::NRF + 4 * maxX) + 3) / 4) >
                           (2 * (T::NTT + 5 * maxX) + 2 * (T::NXF + T::NRF + 4 * maxX))
              ? (2 * (T::NXF + T::NRF + 4 * maxX) + ((T::NXF + T::NRF + 4 * maxX) + 3) / 4)
              : (2 * (T::NTT + 5 * maxX) + 2 * (T::NXF + T::NRF + 4 * maxX));
 }
 template <class T>
+__host__ __device__ constexpr int fused_region8_t(int maxX) {
+  return (fused_region_t<T>(maxX) > 2 * T::NPT8 ? fused_region_t<T>(maxX) : 2 * T::NPT8);
+}
+template <class T>
 __host__ __device__ constexpr size_t fused_smem_t(int maxX) {
-  // primitives, face region, vcell T1/T2 (T::WIDE), stage-2 results, face areas
-  return sizeof(float4) * (2 * (T::NPT + 25 * maxX) + fused_region_t<T>(maxX) +
-                           (T::WIDE ? 2 * (T::NTT + 5 * maxX) : 0) + 2 * (T::NT + maxX)) +
-         sizeof(float) * (T::NXF + T::NRF + 4 * maxX);
+  // alignment slack, mask block, face region, vcell T1/T2 (T::WIDE), stage-2
+  // results, face areas, primitives
+  return sizeof(float4) * (8 + T::MASKF4 + fused_region8_t<T>(maxX) + (T::WIDE ? 2 * (T::NTT + 5 * maxX) : 0) +
+                           2 * (T::NC + maxX) + (T::NXF + T::NRF + 4 * maxX + 3) / 4 + 2 * (T::NPT + 25 * maxX));
 }
 template <class T>
 __device__ __forceinline__ void stage2_physics_body(const StageArgs& a, const PhysArgs& p, const rn_params& P, int bx,
-                                                    int by, int tileId, float4* sm, float* red, int* xc) {
+                                                    int by, int tileId, float4* smRaw, float* red, int* xc,
+                                                    uint64_t* bar) {
   constexpr int TX = T::TX, NT = T::NT;
   const Grid& g = a.g;
   const int Nx = g.Nx, Nr = g.Nr;
   const int tid = threadIdx.x;
   const int x0 = bx * TX, y0 = by * T::TY;
-  const PrimPair pf = prefetch_prims<T>(g, a.A, a.B, x0, y0);
+  float4* sm = aligned_smem(smRaw);
+  uint8_t* sMask = reinterpret_cast<uint8_t*>(sm);
+  float4* R = sm + T::MASKF4;
+  halo_issue<T>(a.tm, a.slotIn, x0, y0, R, sMask, bar);
+  const FirstAreas fa = first_areas<T>(g, x0, y0);
   const int xb = a.xoff[tileId], xn = a.xoff[tileId + 1] - xb, xnP = P.visc ? xn : 0;
   const int NP = T::NPT + 25 * xn, NF = T::NXF + T::NRF + 4 * xn;
-  const int NV = T::NTT + 5 * xnP, NFV = T::NXF + T::NRF + 4 * xnP;
-  float4* sW = sm;
-  float4* sWb = sW + NP;
-  float4* R = sWb + NP;
-  float4* sT1 = T::WIDE ? R + fused_region_t<T>(xn) : R;
+  const int NV = T::NTT + 5 * xnP;
+  float4* sT1 = T::WIDE ? R + fused_region8_t<T>(xn) : R;
   float4* sT2 = sT1 + (T::WIDE ? T::NTT + 5 * xn : NV);
-  float4* sA2 = T::WIDE ? sT2 + (T::NTT + 5 * xn) : R + fused_region_t<T>(xn);
-  float4* sB2 = sA2 + NT + xn;
-  float* sAr = reinterpret_cast<float*>(sB2 + NT + xn);   // face areas, kept for FS_SOURCE
+  float4* sA2 = T::WIDE ? sT2 + (T::NTT + 5 * xn) : R + fused_region8_t<T>(xn);
+  float4* sB2 = sA2 + T::NC + xn;
+  float* sAr = reinterpret_cast<float*>(sB2 + T::NC + xn);   // face areas, kept for FS_SOURCE
+  float4* sW = reinterpret_cast<float4*>(sAr) + (NF + 3) / 4;
+  float4* sWb = sW + NP;
   for (int q = tid; q < xn; q += NT) xc[q] = a.xcell[xb + q];
   const float4 st = *a.stNew;
   const float dt = st.x, t = st.z;
   __syncthreads();
-  load_prims<T>(g, a.A, a.B, t, P, x0, y0, xc, NP, sW, sWb, NF, sAr, pf);
+  if (!halo_wait(bar, a.err)) return;
+  load_prims<T>(g, a.A, a.B, t, P, x0, y0, xc, NP, R, sMask, sW, sWb);
+  store_areas<T>(g, x0, y0, xc, xn, fa, sAr);
   __syncthreads();
   {
     float4* sF = R;
     float4* sY = sF + NF;
     float* sO = reinterpret_cast<float*>(sY + NF);
-    inviscid_faces<T>(g, P, x0, y0, xc, NF, sW, sWb, sF, sY, sO, sAr);
+    inviscid_faces<T>(g, P, xc, xn, sW, sWb, sF, sY, sO, sAr);
     __syncthreads();
     // One flat list (T::WIDE): the stage-2 update of the tile's cells and of
     // its listed members, then FS_VCELL of the vcell slots. FS_VCELL reads only
@@ -743,21 +842,22 @@ __device__ __forceinline__ void stage2_physics_body(const StageArgs& a, const Ph
         const int e = q - T::NC, m = xc[e];
         float4 oA, oB;
         update_cell<T, 2>(a, P, m % Nx, m / Nx, dt, t, x0, y0, xc, xn, sF, sY, sO, sAr, oA, oB);
-        sA2[NT + e] = oA;
-        sB2[NT + e] = oB;
+        sA2[T::NC + e] = oA;
+        sB2[T::NC + e] = oB;
       } else {
         vcell_at<T>(g, P, dt, x0, y0, xc, q - NU, sW, sWb, sT1, sT2);
       }
     }
   }
   __syncthreads();
+  const int NFV = T::NXF + T::NRF + 4 * xnP;
   float4* sF = T::WIDE ? R : sT2 + NV;
   float4* sY = sF + NFV;
   if (!T::WIDE) {
     for (int k = tid; k < NV; k += NT) vcell_at<T>(g, P, dt, x0, y0, xc, k, sW, sWb, sT1, sT2);
     __syncthreads();
   }
-  if (P.visc) viscous_faces<T>(g, x0, y0, xc, NFV, sW, sWb, sT1, sT2, sAr, sF, sY);
+  if (P.visc) viscous_faces<T>(g, x0, y0, xc, xnP, sW, sWb, sT1, sT2, sAr, sF, sY);
   __syncthreads();
 
   const int i = x0 + tid % TX, j = y0 + tid / TX;
@@ -771,13 +871,13 @@ __device__ __forceinline__ void stage2_physics_body(const StageArgs& a, const Ph
       const int Hx = i + iround(gm.x), Hy = j + iround(gm.y);
       const int hx = Hx - x0, hy = Hy - y0;
       int s;
-      if (hx >= 0 && hx < TX && hy >= 0 && hy < T::TY) {
+      if (unsigned(hx) < unsigned(TX) && unsigned(hy) < unsigned(T::TY)) {
         s = hy * TX + hx;
       } else {
         const int kh = Hy * Nx + Hx;
         int e = 0;
         while (e < xn - 1 && xc[e] != kh) e++;
-        s = NT + e;
+        s = T::NC + e;
       }
       A = sA2[s];
       B = sB2[s];
@@ -799,7 +899,8 @@ __global__ void __launch_bounds__(T::NT, T::MINB) k_stage(StageArgs a, rn_params
   extern __shared__ float4 sm[];
   __shared__ float red[T::NT / 32];
   __shared__ int xc[MAXX];
-  stage_body<T, STAGE>(a, P, blockIdx.x, blockIdx.y, blockIdx.y * gridDim.x + blockIdx.x, sm, red, xc);
+  __shared__ uint64_t bar;
+  stage_body<T, STAGE>(a, P, blockIdx.x, blockIdx.y, blockIdx.y * gridDim.x + blockIdx.x, sm, red, xc, &bar);
 }
 // heavy == nullptr: one block per tile of the grid, skipping tiles that list
 // more than xSmall out-of-tile members (xSmall < 0: none skipped); otherwise
@@ -811,6 +912,7 @@ __global__ void __launch_bounds__(T::NT, T::MINB) k_stage2phys(StageArgs a, Phys
   extern __shared__ float4 sm[];
   __shared__ float red[T::NT / 32];
   __shared__ int xc[MAXX];
+  __shared__ uint64_t bar;
   int bx, by, tile;
   if (heavy) {
     const int tilesX = (a.g.Nx + T::TX - 1) / T::TX;
@@ -823,7 +925,7 @@ __global__ void __launch_bounds__(T::NT, T::MINB) k_stage2phys(StageArgs a, Phys
     tile = by * gridDim.x + bx;
     if (xSmall >= 0 && a.xoff[tile + 1] - a.xoff[tile] > xSmall) return;
   }
-  stage2_physics_body<T>(a, p, P, bx, by, tile, sm, red, xc);
+  stage2_physics_body<T>(a, p, P, bx, by, tile, sm, red, xc, &bar);
 }
 
 // Batch kernels: block b belongs to instance blockInst[b]; its descriptor
@@ -842,6 +944,7 @@ __global__ void __launch_bounds__(T::NT, T::MINB) k_stage_batch(const BatchInst*
   extern __shared__ float4 sm[];
   __shared__ float red[T::NT / 32];
   __shared__ int xc[MAXX];
+  __shared__ uint64_t bar;
   __shared__ BatchInst d;
   load_inst(insts, blockInst[blockIdx.x], d);
   const int s0 = (d.cur0 + ph.shift) % 3, s1 = (s0 + 1) % 3, s2 = (s0 + 2) % 3;
@@ -859,8 +962,11 @@ __global__ void __launch_bounds__(T::NT, T::MINB) k_stage_batch(const BatchInst*
   a.wOut = d.wmax + (1 - ws);
   a.finalCfl = ph.finalCfl;
   a.xoff = d.xoff; a.xcell = d.xcell; a.maxX = ph.maxX;
+  a.slotIn = STAGE == 1 ? s0 : s1;
+  a.tm = d.tm;
+  a.err = d.err;
   const int local = blockIdx.x - d.firstBlock, by = local / d.tilesX, bx = local - by * d.tilesX;
-  stage_body<T, STAGE>(a, d.P, bx, by, local, sm, red, xc);
+  stage_body<T, STAGE>(a, d.P, bx, by, local, sm, red, xc, &bar);
 }
 template <class T>
 __global__ void __launch_bounds__(T::NT, T::MINB) k_stage2phys_batch(const BatchInst* insts, const int* blockInst,
@@ -868,6 +974,7 @@ __global__ void __launch_bounds__(T::NT, T::MINB) k_stage2phys_batch(const Batch
   extern __shared__ float4 sm[];
   __shared__ float red[T::NT / 32];
   __shared__ int xc[MAXX];
+  __shared__ uint64_t bar;
   __shared__ BatchInst d;
   const int2 hv = heavy ? heavy[blockIdx.x] : make_int2(0, 0);   // (member, tile) of a heavy block
   load_inst(insts, heavy ? hv.x : blockInst[blockIdx.x], d);
@@ -882,6 +989,9 @@ __global__ void __launch_bounds__(T::NT, T::MINB) k_stage2phys_batch(const Batch
   a.wOut = d.wmax + (1 - ws);
   a.finalCfl = 0;
   a.xoff = d.xoff; a.xcell = d.xcell; a.maxX = ph.maxX;
+  a.slotIn = s1;
+  a.tm = d.tm;
+  a.err = d.err;
   PhysArgs p;
   p.g = d.g;
   p.A1 = d.SA[s1]; p.B1 = d.SB[s1]; p.A2 = d.SA[s2]; p.B2 = d.SB[s2]; p.oA = d.SA[s2]; p.oB = d.SB[s2];
@@ -891,7 +1001,7 @@ __global__ void __launch_bounds__(T::NT, T::MINB) k_stage2phys_batch(const Batch
   p.xoff = d.xoff; p.xcell = d.xcell; p.maxX = ph.maxX;
   const int local = heavy ? hv.y : blockIdx.x - d.firstBlock, by = local / d.tilesX, bx = local - by * d.tilesX;
   if (!heavy && xSmall >= 0 && d.xoff[local + 1] - d.xoff[local] > xSmall) return;   // in the heavy launch
-  stage2_physics_body<T>(a, p, d.P, bx, by, local, sm, red, xc);
+  stage2_physics_body<T>(a, p, d.P, bx, by, local, sm, red, xc, &bar);
 }
 
 // --------------------------------------------------------------------------

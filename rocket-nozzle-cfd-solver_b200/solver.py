@@ -36,7 +36,7 @@ EXPORTS = ("rn_create", "rn_destroy", "rn_resize", "rn_set_mask", "rn_set_geomet
            "rn_server_create", "rn_server_destroy", "rn_serve_submit", "rn_serve_poll", "rn_serve_wait",
            "rn_serve_stats", "rn_solve_bytes", "rn_set_wall_profile", "rn_wall_separation", "rn_derived",
            "rn_derived_buffer", "rn_build_geometry", "rn_get_geometry", "rn_spray_build_injector",
-           "rn_spray_set_parcels",
+           "rn_spray_set_parcels", "rn_serve_inject", "rn_spray_parcel_steps",
            "rn_last_error")
 PRECISION = {"fast": 0, "exact": 1}
 TILES = {"16x16": 0, "16x8": 1, "16x15": 2, "32x15": 3, "14x16": 4}
@@ -107,7 +107,7 @@ class RnSolveResult(ctypes.Structure):
 
 class RnServeStatus(ctypes.Structure):
     _fields_ = [(n, ctypes.c_longlong) for n in ("queued", "active", "finished", "bytes_used", "bytes_budget",
-                                                  "ticks", "admitted", "failed")]
+                                                  "ticks", "admitted", "failed", "evicted")]
 
 
 class RnSeparationSpec(ctypes.Structure):
@@ -279,6 +279,8 @@ def lib():
                                 ctypes.c_void_p]
     L.rn_serve_stats.argtypes = [H, ctypes.POINTER(RnServeStatus)]
     L.rn_solve_bytes.argtypes = [i, i, ctypes.POINTER(ctypes.c_longlong)]
+    L.rn_serve_inject.argtypes = [H, i]
+    L.rn_spray_parcel_steps.argtypes = [H, ctypes.POINTER(ctypes.c_longlong)]
     dp = ctypes.POINTER(ctypes.c_double)
     L.rn_set_wall_profile.argtypes = [H, dp, dp, dp]
     L.rn_wall_separation.argtypes = [H, ctypes.POINTER(RnSeparationSpec), ctypes.POINTER(RnSeparationOut)]
@@ -671,6 +673,13 @@ class GPUSpray:
         _check(lib().rn_spray_stats(self.s.h, out))
         return {"fuel": out[0], "ox": out[1], "parcels": int(out[2]), "meanD": out[3]}
 
+    def parcelSteps(self):
+        """Live parcels summed over every spray step since the ring was last
+        set (counted on the device; waits for the queued steps)."""
+        v = ctypes.c_longlong()
+        _check(lib().rn_spray_parcel_steps(self.s.h, ctypes.byref(v)))
+        return v.value
+
     def readParcels(self):
         """The current parcel textures PA, PB, PC (65,536 x 4 each)."""
         r = self.s._readRect
@@ -850,6 +859,12 @@ class SolveServer:
                                         A.ctypes.data if state else None, B.ctypes.data if state else None),
                     (RN_OK, RN_NOT_READY))
         return None if rc == RN_NOT_READY else self._result(rid, res, A, B, state)
+
+    def inject(self, where):
+        """Host-side fault injection for tests: the next submitted request
+        fails as a device allocation would, at its admission ("admit") or in
+        its first tick ("tick"); the server evicts it alone."""
+        _check(lib().rn_serve_inject(self.s, {"admit": 1, "tick": 2}[where]))
 
     def stats(self):
         st = RnServeStatus()

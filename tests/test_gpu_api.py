@@ -10,7 +10,7 @@ import os
 import numpy as np
 import pytest
 
-from helpers import assert_state_close, field_rel_l2, run_oracle
+from helpers import assert_state_close, field_rel_l2, run_oracle  # noqa: F401
 
 pytestmark = pytest.mark.gpu
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -343,24 +343,64 @@ def test_fast_deposit_sums_are_deterministic(rn):
     assert np.array_equal(out[0]["A"], out[1]["A"]) and np.array_equal(out[0]["B"], out[1]["B"])
 
 
-def test_fast_deposit_out_of_range_is_reported(rn):
-    """A deposit beyond the fixed-point range of the fast deposit sums (here
-    parcels a million times heavier than mhat*dtMax/4) is clamped and reported
-    once by the spray statistics; the next call is clean again."""
+def test_oversize_parcels_match_oracle(rn, oracle):
+    """Parcels ten thousand times heavier than the spawn bound mhat*dtMax/4 and
+    five times faster than vMax, among them the 8 that the spawn recycles in
+    two steps, whose whole masses are deposited (far beyond the 64 bounds a
+    fixed scale could hold): the fast deposit sums scale to the ring's own
+    largest mass and speed (tracked on the device step by step), so the
+    deposits are neither clamped nor flagged, and the state matches the
+    oracle's float sums after the steps (two, before the violent sources'
+    flow can amplify last-bit differences)."""
     from rocket_nozzle_cfd_solver_b200 import configs
     s = rn.build_sim_setup(configs.injector_spray(128, 48)[0])
     PA, PB, head = configs.prepopulated_parcels(s, 1024)
+    PA = np.array(PA, dtype=np.float32).reshape(-1, 4)
     PB = np.array(PB, dtype=np.float32).reshape(-1, 4)
-    live = PB[:, 1] > 0
-    PB[live, 1] = np.float32(1e6 * s.P["spray"]["mhat"] * s.P["dtMax"] / 4)
+    # the 8 slots the spawn recycles in two steps (head 0) deposit their whole
+    # mass; every 32nd other parcel deposits drag and evaporation sources
+    head = 0
+    heavy = np.r_[np.arange(8), np.flatnonzero(PB[:, 1] > 0)[8::32]]
+    PB[heavy, 1] = np.float32(1e4 * s.P["spray"]["mhat"] * s.P["dtMax"] / 4)
+    PA[heavy, 2] = np.float32(5.0 * s.P["vMax"])
+    state = s.initialState()
+    g = rn.GPUSolver(s.Nx, s.Nr)
+    g.setGeometry(s.geo)
+    g.setState(state["A"], state["B"])
+    rn.GPUSpray(g).resize()
+    g.spray.setInjector(s.injector)
+    g.spray.setParcels(PA.ravel(), PB.ravel(), head)
+    g.step(2, s.P)
+    g.spray.stats()                                  # no range error
+    g.sync()
+    o = oracle.OracleSolver(s.Nx, s.Nr)
+    o.setGeometry(s.geo)
+    o.setState(state["A"], state["B"])
+    o.setInjector(s.injector)
+    o.setParcels(PA.ravel(), PB.ravel(), head)
+    o.step(2, s.P)
+    e = assert_state_close(g.readAll(), o.readAll(), TOL)
+    print("oversize parcels, rel-L2 per field:", e)
+    g.close()
+
+
+def test_non_finite_parcel_is_reported(rn):
+    """The one deposit the bounds cannot hold, a parcel whose speed is not a
+    number, is flagged on the device and reported once by the spray
+    statistics (and would be by rn_sync); the next call is clean again."""
+    from rocket_nozzle_cfd_solver_b200 import configs
+    s = rn.build_sim_setup(configs.injector_spray(128, 48)[0])
+    PA, PB, head = configs.prepopulated_parcels(s, 64)
+    PA = np.array(PA, dtype=np.float32).reshape(-1, 4)
+    PA[0, 2] = np.float32("nan")
     g = rn.GPUSolver(s.Nx, s.Nr)
     g.setGeometry(s.geo)
     init = s.initialState()
     g.setState(init["A"], init["B"])
     rn.GPUSpray(g).resize()
     g.spray.setInjector(s.injector)
-    g.spray.setParcels(PA, PB.ravel(), head)
-    g.step(3, s.P)
+    g.spray.setParcels(PA.ravel(), PB, head)
+    g.step(1, s.P)
     with pytest.raises(rn.RnError, match="fixed-point range"):
         g.spray.stats()
     g.spray.stats()                                  # reported once

@@ -153,3 +153,44 @@ def test_server_cell_cap(rn):
     for s, r in zip(ss, res):
         out, _ = alone(rn, s, 100)
         assert np.array_equal(r["A"], out["A"])
+
+
+def test_server_isolates_failing_requests(rn):
+    """A request whose setup fails (a geometry the library rejects), one whose
+    admission allocation fails and one whose first tick fails (host-side
+    injections of an allocation failure) are each evicted alone with status
+    'failed'; the other solves finish bit-identical to the same solves
+    stepped alone, and the server keeps accepting work."""
+    import copy
+    good = [setup_of(rn, "plain", 96, 36), setup_of(rn, "viscous", 128, 48), setup_of(rn, "plain", 128, 48)]
+    bad_geo = copy.copy(setup_of(rn, "plain", 96, 36))
+    geo = dict(bad_geo.geo)
+    geoM = np.array(geo["geoM"], dtype=np.float32).reshape(-1, 4)
+    k = int(np.flatnonzero(np.asarray(geo["mask"]) == 0)[40])
+    geoM[k, 0] = 2.0                                  # a host two cells away: rn_set_geometry rejects it
+    geo["geoM"] = geoM.ravel()
+    bad_geo["geo"] = geo
+    steps = 80
+    srv = rn.SolveServer(check_every=20, precision="exact")
+    ids = {"g0": srv.submit(good[0], drop=0, t_end_s=0, max_steps=steps)}
+    ids["setup"] = srv.submit(bad_geo, drop=0, t_end_s=0, max_steps=steps)
+    srv.inject("admit")
+    ids["admit"] = srv.submit(good[1], drop=0, t_end_s=0, max_steps=steps)
+    ids["g1"] = srv.submit(good[1], drop=0, t_end_s=0, max_steps=steps)
+    srv.inject("tick")
+    ids["tick"] = srv.submit(good[2], drop=0, t_end_s=0, max_steps=steps)
+    ids["g2"] = srv.submit(good[2], drop=0, t_end_s=0, max_steps=steps)
+    res = {k: srv.wait(v, timeout_s=300, state=True) for k, v in ids.items()}
+    later = srv.submit(good[0], drop=0, t_end_s=0, max_steps=steps)   # still serving
+    r_later = srv.wait(later, timeout_s=300, state=True)
+    st = srv.stats()
+    srv.close()
+    for k in ("setup", "admit", "tick"):
+        assert res[k]["status"] == "failed", (k, res[k]["status"])
+    assert st["failed"] == 0 and st["evicted"] == 3 and st["bytes_used"] == 0
+    for k, s in (("g0", good[0]), ("g1", good[1]), ("g2", good[2]), ("later", good[0])):
+        r = r_later if k == "later" else res[k]
+        assert r["status"] == "max_steps" and r["steps"] == steps, k
+        out, integ = alone(rn, s, steps)
+        assert np.array_equal(r["A"], out["A"]) and np.array_equal(r["B"], out["B"]), k
+        assert r["integrals"] == integ, k
