@@ -219,18 +219,19 @@ RN_DEV float4 step4(float4 w, float h, float4 d) {
 }
 RN_DEV float jump_ratio(float a, float b) { return fdiv(fabsf(a - b), fminf(a, b)); }
 
-// DIR_R selects the r-direction (normal velocity in .z), fixed at compile
-// time: the tile kernels run the x-faces and the r-faces in loops of their own.
-template <bool DIR_R>
-RN_DEV Flux face_flux(float area, float4 w0, float4 b0, float4 w1, float4 b1, float4 w2, float4 b2, float4 w3,
-                      float4 b3, float4 sa1, float4 sb1, float4 sa2, float4 sb2, const rn_params& P) {
+// DIR_R selects the r-direction (normal velocity in .z). One instance of the
+// code serves both directions: the fused kernels are large enough that a
+// second inlined copy costs more in instruction-cache misses than the
+// direction's selects cost in instructions.
+RN_DEV Flux face_flux(bool DIR_R, float area, float4 w0, float4 b0, float4 w1, float4 b1, float4 w2, float4 b2,
+                      float4 w3, float4 b3, float4 sa1, float4 sb1, float4 sa2, float4 sb2, const rn_params& P) {
   Flux out;
   out.F = make_float4(0.f, 0.f, 0.f, 0.f);
   out.Y = out.F;
   out.O = 0.0f;
   bool s0 = w0.x < 0.0f, s1 = w1.x < 0.0f, s2 = w2.x < 0.0f, s3 = w3.x < 0.0f;
   if (s1 && s2) return out;
-  if constexpr (DIR_R) {   // face-normal frame: normal velocity in .y
+  if (DIR_R) {   // face-normal frame: normal velocity in .y
     float t;
     t = w0.y; w0.y = w0.z; w0.z = t;
     t = w1.y; w1.y = w1.z; w1.z = t;
@@ -336,7 +337,7 @@ RN_DEV Flux face_flux(float area, float4 w0, float4 b0, float4 w1, float4 b1, fl
     uf = uK + SK * (fdiv(SK - uK, SK - Ss) - 1.0f);
     Gf = left ? GL : GR;
   }
-  if constexpr (DIR_R) { float t = F1; F1 = F2; F2 = t; }    // rotate momentum back to (x, r)
+  if (DIR_R) { float t = F1; F1 = F2; F2 = t; }    // rotate momentum back to (x, r)
   out.F = make_float4(F0, F1, F2, F3);
   out.Y = make_float4(Y0, Y1, uf * Gf, uf);
   out.O = Y2;
@@ -398,20 +399,19 @@ RN_DEV void vcell(float4 w0, float4 sc, float4 wE, float4 wW, float4 wN, float4 
 
 // makeViscFluxShader (solver.js:499-536) for one face. (w1, s1, t1, m1) is
 // the cell behind the face, (w2, s2, t2, m2) the cell the face belongs to; j
-// is the face's row. DIR_R (the r-direction) is fixed at compile time.
-template <bool DIR_R>
-RN_DEV void visc_flux(float4 w1, float4 s1, float4 t1, float4 m1, float4 w2, float4 s2, float4 t2, float4 m2, int j,
-                      float4& F, float4& FY) {
+// is the face's row; DIR_R selects the r-direction (one instance for both).
+RN_DEV void visc_flux(bool DIR_R, float4 w1, float4 s1, float4 t1, float4 m1, float4 w2, float4 s2, float4 t2,
+                      float4 m2, int j, float4& F, float4& FY) {
   float mu = 0.5f * (m1.x + m2.x);
   float uf = 0.5f * (w1.y + w2.y), vf = 0.5f * (w1.z + w2.z);
   float ttx = 0.5f * (t1.x + t2.x), tty = 0.5f * (t1.y + t2.y), ttz = 0.5f * (t1.z + t2.z), ttw = 0.5f * (t1.w + t2.w);
   float r, ux, vx, ur, vr;
-  if constexpr (DIR_R) { r = fmaxf(float(j), 0.5f); ux = ttx; vx = ttz; ur = w2.y - w1.y; vr = w2.z - w1.z; }
+  if (DIR_R) { r = fmaxf(float(j), 0.5f); ux = ttx; vx = ttz; ur = w2.y - w1.y; vr = w2.z - w1.z; }
   else { r = float(j) + 0.5f; ux = w2.y - w1.y; vx = w2.z - w1.z; ur = tty; vr = ttw; }
   float div = ux + vr + fdiv(vf, r);
   float txr = mu * (ur + vx);
   float k = mu * 1.25f;
-  if constexpr (DIR_R) {
+  if (DIR_R) {
     float trr = mu * (2.0f * vr - 0.6666667f * div);
     F = make_float4(-k * (s2.w - s1.w), -txr, -trr, -(uf * txr + vf * trr) - k * (m2.y - m1.y));
   } else {

@@ -232,70 +232,59 @@ __device__ __forceinline__ bool halo_wait(uint64_t* bar, unsigned* err) {
   return false;
 }
 
-// Cells of the staged halo block (raw A, B and mask in shared memory) for
-// ghost_prim_c: every cell a ghost slot reads lies within the block.
+// Cells for ghost_prim_c and the interior slots: from the staged halo block
+// (raw A, B and mask in shared memory) where the cell lies in it, else from
+// global memory (a listed member's neighbourhood outside the block).
 template <class T>
-struct TileCells {
+struct HaloCells {
+  const Grid& g;
+  const float4* __restrict__ A;
+  const float4* __restrict__ B;
   const float4* rA;
   const float4* rB;
   const uint8_t* m;
   int x0, y0, mo;
+  __device__ __forceinline__ bool staged(int i, int j) const {
+    return unsigned(i - x0 + 2) < unsigned(T::PX) && unsigned(j - y0 + 2) < unsigned(T::PY);
+  }
   __device__ __forceinline__ int slot(int i, int j) const { return (j - y0 + 2) * T::PX + (i - x0 + 2); }
   __device__ __forceinline__ bool solid(int i, int j) const {
-    return m[(j - y0 + 2) * T::MW + mo + (i - x0 + 2)] != 0;
+    return staged(i, j) ? m[(j - y0 + 2) * T::MW + mo + (i - x0 + 2)] != 0 : g.mask[j * g.Nx + i] != 0;
   }
-  __device__ __forceinline__ float4 a(int i, int j) const { return rA[slot(i, j)]; }
-  __device__ __forceinline__ float4 b(int i, int j) const { return rB[slot(i, j)]; }
+  __device__ __forceinline__ float4 a(int i, int j) const { return staged(i, j) ? rA[slot(i, j)] : A[j * g.Nx + i]; }
+  __device__ __forceinline__ float4 b(int i, int j) const { return staged(i, j) ? rB[slot(i, j)] : B[j * g.Nx + i]; }
 };
 
-// FS_PRIM: ghost-cell primitives of the tile + 2-cell halo from the staged
-// block, then the listed members' 5x5 blocks from global memory.
+// FS_PRIM: ghost-cell primitives of the tile + 2-cell halo, then of the listed
+// members' 5x5 blocks, in one loop through one instance of the ghost code.
 template <class T>
 __device__ __forceinline__ void load_prims(const Grid& g, const float4* __restrict__ A, const float4* __restrict__ B,
                                            float t, const rn_params& P, int x0, int y0, const int* xc, int NP,
                                            const float4* R, const uint8_t* sMask, float4* sW, float4* sWb) {
   const int Nx = g.Nx, Nr = g.Nr;
-  const TileCells<T> cells{R, R + T::NPT8, sMask, x0, y0, (x0 - 2) - ((x0 - 2) & ~15)};
-  for (int k = threadIdx.x; k < T::NPT; k += T::NT) {
-    const int ly = k / T::PX, lx = k - ly * T::PX;
-    const int i = x0 - 2 + lx, j = y0 - 2 + ly;
+  const HaloCells<T> cells{g, A, B, R, R + T::NPT8, sMask, x0, y0, (x0 - 2) - ((x0 - 2) & ~15)};
+  for (int k = threadIdx.x; k < NP; k += T::NT) {
+    int i, j;
+    if (k < T::NPT) {
+      const int ly = k / T::PX;
+      i = x0 - 2 + (k - ly * T::PX); j = y0 - 2 + ly;
+    } else {                                     // member e's 5x5 block
+      const int q = k - T::NPT, e = q / 25, r = q - e * 25, m = xc[e], dy = r / 5;
+      i = m % Nx + (r - dy * 5) - 2; j = m / Nx + dy - 2;
+    }
     float4 W, Wb;
     if (i >= 0 && i < Nx && j >= 0 && j < Nr) {     // ghost_prim's interior branch
-      if (sMask[ly * T::MW + cells.mo + lx]) {
+      const float4 a = cells.a(i, j), b = cells.b(i, j);
+      if (cells.solid(i, j)) {
         W = make_float4(-1.0f, 0.0f, 0.0f, 1.0f);
         Wb = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
       } else {
-        const Prim q = to_prim(cells.rA[k], cells.rB[k]);
+        const Prim q = to_prim(a, b);
         W = q.w;
         Wb = q.s;
       }
     } else if (i <= Nx + 1 && j <= Nr + 1) {
       ghost_prim_c(Nx, Nr, cells, i, j, t, P, W, Wb);
-    } else {
-      W = make_float4(-1.f, 0.f, 0.f, 1.f); Wb = make_float4(0.f, 0.f, 0.f, 0.f);
-    }
-    sW[k] = W;
-    sWb[k] = Wb;
-  }
-  // listed members' 5x5 blocks (slivers merged across the tile edge)
-  for (int k = T::NPT + threadIdx.x; k < NP; k += T::NT) {
-    const int q = k - T::NPT, e = q / 25, r = q - e * 25, m = xc[e];
-    const int dy = r / 5;
-    const int i = m % Nx + (r - dy * 5) - 2, j = m / Nx + dy - 2;
-    float4 W, Wb;
-    if (i >= 0 && i < Nx && j >= 0 && j < Nr) {
-      const int c = j * Nx + i;
-      const float4 a = A[c], b = B[c];
-      if (g.mask[c]) {
-        W = make_float4(-1.0f, 0.0f, 0.0f, 1.0f);
-        Wb = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-      } else {
-        const Prim p = to_prim(a, b);
-        W = p.w;
-        Wb = p.s;
-      }
-    } else if (i <= Nx + 1 && j <= Nr + 1) {
-      ghost_prim(g, A, B, i, j, t, P, W, Wb);
     } else {
       W = make_float4(-1.f, 0.f, 0.f, 1.f); Wb = make_float4(0.f, 0.f, 0.f, 0.f);
     }
@@ -331,55 +320,42 @@ __device__ __forceinline__ void store_areas(const Grid& g, int x0, int y0, const
   for (int q = tid; q < 4 * xn; q += T::NT) sAr[T::NXF + T::NRF + q] = member_face_area<T>(g, q, xc);
 }
 
-// One tile face of direction DIR_R whose first normal cell is primitive slot
-// b: the normal cells b + n*d and the sensor cells (k1 +- t, ij +- t) of
-// makeFluxShader (solver.js:133-259) sit at fixed offsets from b.
-template <class T, bool DIR_R>
-__device__ __forceinline__ void tile_face(const rn_params& P, int b, float area, const float4* sW, const float4* sWb,
-                                          float4* sF, float4* sY, float* sO, int out) {
-  constexpr int d = DIR_R ? T::PX : 1, t = DIR_R ? 1 : T::PX;
-  Flux f;
-  f.F = make_float4(0.f, 0.f, 0.f, 0.f); f.Y = f.F; f.O = 0.f;
-  if (area != 0.0f)
-    f = face_flux<DIR_R>(area, sW[b], sWb[b], sW[b + d], sWb[b + d], sW[b + 2 * d], sWb[b + 2 * d], sW[b + 3 * d],
-                         sWb[b + 3 * d], sW[b + d + t], sW[b + d - t], sW[b + 2 * d + t], sW[b + 2 * d - t], P);
-  sF[out] = f.F; sY[out] = f.Y; sO[out] = f.O;
-}
-// A listed member's face (direction known only at run time; rare): kept out
-// of line so that the tile face loops hold the only inlined flux code.
-template <class T>
-__device__ __noinline__ void member_face(const rn_params& P, int q, const int* xc, int Nx, float area,
-                                         const float4* sW, const float4* sWb, float4* sF, float4* sY, float* sO) {
-  const FaceSlot s = member_face_slot<T>(q, xc, Nx);
-  Flux f;
-  f.F = make_float4(0.f, 0.f, 0.f, 0.f); f.Y = f.F; f.O = 0.f;
-  if (area != 0.0f) {
-    if (s.dirR)
-      f = face_flux<true>(area, sW[s.c[0]], sWb[s.c[0]], sW[s.c[1]], sWb[s.c[1]], sW[s.c[2]], sWb[s.c[2]],
-                          sW[s.c[3]], sWb[s.c[3]], sW[s.s[0]], sW[s.s[1]], sW[s.s[2]], sW[s.s[3]], P);
-    else
-      f = face_flux<false>(area, sW[s.c[0]], sWb[s.c[0]], sW[s.c[1]], sWb[s.c[1]], sW[s.c[2]], sWb[s.c[2]],
-                           sW[s.c[3]], sWb[s.c[3]], sW[s.s[0]], sW[s.s[1]], sW[s.s[2]], sW[s.s[3]], P);
-  }
-  const int k = T::NXF + T::NRF + q;
-  sF[k] = f.F; sY[k] = f.Y; sO[k] = f.O;
-}
-
-// FS_FLUX_X/R: tile x-faces, tile r-faces, members' faces.
+// FS_FLUX_X/R: every face of the tile (x-faces, then r-faces) and of its
+// listed members in one loop through one instance of the flux code. Face k's
+// 4 cells along the normal are primitive slots b, b + d, b + 2d, b + 3d and its
+// sensor cells (k1 +- t, ij +- t of makeFluxShader, solver.js:133-259)
+// b + d +- t and b + 2d +- t: tile faces have (d, t) = (1, PX) (x) or (PX, 1)
+// (r); a listed member's faces live in its 5x5 block, with 5 in place of PX.
+// One code path for every face also makes the fast precision's contracted
+// multiply-adds round alike in every tile shape.
 template <class T>
 __device__ __forceinline__ void inviscid_faces(const Grid& g, const rn_params& P, const int* xc, int xn,
                                                const float4* sW, const float4* sWb, float4* sF, float4* sY,
                                                float* sO, const float* sAr) {
-  for (int k = threadIdx.x; k < T::NXF; k += T::NT) {
-    const int ly = k / (T::TX + 1), lx = k - ly * (T::TX + 1);
-    tile_face<T, false>(P, (ly + 2) * T::PX + lx, sAr[k], sW, sWb, sF, sY, sO, k);
+  constexpr int NXR = T::NXF + T::NRF;
+  for (int k = threadIdx.x; k < NXR + 4 * xn; k += T::NT) {
+    int b, d, t;
+    bool dirR;
+    if (k < T::NXF) {
+      const int ly = k / (T::TX + 1), lx = k - ly * (T::TX + 1);
+      b = (ly + 2) * T::PX + lx; d = 1; t = T::PX; dirR = false;
+    } else if (k < NXR) {
+      const int kk = k - T::NXF, ly = kk / T::TX, lx = kk - ly * T::TX;
+      b = ly * T::PX + lx + 2; d = T::PX; t = 1; dirR = true;
+    } else {                                     // member e's face w (W, E at mx + o; S, N at my + o)
+      const int q = k - NXR, e = q >> 2, w = q & 3, o = w & 1;
+      dirR = w >= 2;
+      b = dirR ? ext_prim<T>(e, 0, o - 2) : ext_prim<T>(e, o - 2, 0);
+      d = dirR ? 5 : 1; t = dirR ? 1 : 5;
+    }
+    Flux f;
+    f.F = make_float4(0.f, 0.f, 0.f, 0.f); f.Y = f.F; f.O = 0.f;
+    const float area = sAr[k];   // the face's open area, 0 where it is not drawn
+    if (area != 0.0f)
+      f = face_flux(dirR, area, sW[b], sWb[b], sW[b + d], sWb[b + d], sW[b + 2 * d], sWb[b + 2 * d], sW[b + 3 * d],
+                    sWb[b + 3 * d], sW[b + d + t], sW[b + d - t], sW[b + 2 * d + t], sW[b + 2 * d - t], P);
+    sF[k] = f.F; sY[k] = f.Y; sO[k] = f.O;
   }
-  for (int k = threadIdx.x; k < T::NRF; k += T::NT) {
-    const int ly = k / T::TX, lx = k - ly * T::TX;
-    tile_face<T, true>(P, ly * T::PX + lx + 2, sAr[T::NXF + k], sW, sWb, sF, sY, sO, T::NXF + k);
-  }
-  for (int q = threadIdx.x; q < 4 * xn; q += T::NT)
-    member_face<T>(P, q, xc, g.Nx, sAr[T::NXF + T::NRF + q], sW, sWb, sF, sY, sO);
 }
 
 // memberFlux (solver.js:287-299) of group member (cx, cy): its four faces'
@@ -401,15 +377,15 @@ __device__ __forceinline__ void add_member(int cx, int cy, int x0, int y0, const
   }
 }
 // The group of host (Hx, Hy) with slave mask sm_: the host, then its slaves in
-// the reference's member order (slave bits 1, 2, 4, 8 = W, E, S, N).
+// the reference's member order (slave bits 1, 2, 4, 8 = W, E, S, N), all
+// through one call site (bit 0 of the walked mask is the host).
 template <class T, bool WITH_O>
 __device__ __forceinline__ void group_flux(int Hx, int Hy, int sm_, int x0, int y0, const int* xc, int xn, int Nx,
                                            const float4* sF, const float4* sY, const float* sO, const float* sAr,
                                            float4& L, float4& LY, float& LO) {
-  add_member<T, WITH_O>(Hx, Hy, x0, y0, xc, xn, Nx, sF, sY, sO, sAr, L, LY, LO);
-  for (int s = sm_ & 15; s != 0; s &= s - 1) {
+  for (int s = ((sm_ & 15) << 1) | 1; s != 0; s &= s - 1) {
     const int bit = __ffs(s) - 1;
-    const int cx = Hx + (bit == 0 ? -1 : bit == 1 ? 1 : 0), cy = Hy + (bit == 2 ? -1 : bit == 3 ? 1 : 0);
+    const int cx = Hx + (bit == 1 ? -1 : bit == 2 ? 1 : 0), cy = Hy + (bit == 3 ? -1 : bit == 4 ? 1 : 0);
     add_member<T, WITH_O>(cx, cy, x0, y0, xc, xn, Nx, sF, sY, sO, sAr, L, LY, LO);
   }
 }
@@ -584,60 +560,48 @@ __device__ __forceinline__ void vcell_at(const Grid& g, const rn_params& P, floa
   sT2[k] = T2;
 }
 
-// One viscous face: primitive slots p1 (behind) and p2 (the face's cell),
-// vcell slots v1 and v2; zero flux where it is not drawn or a side is a wall.
-template <bool DIR_R>
-__device__ __forceinline__ void visc_face(bool ok, float area, int j, int p1, int p2, int v1, int v2,
-                                          const float4* sW, const float4* sWb, const float4* sT1, const float4* sT2,
-                                          float4& F, float4& FY) {
-  F = make_float4(0.f, 0.f, 0.f, 0.f);
-  FY = F;
-  if (ok) {
-    const float4 w1 = sW[p1], w2 = sW[p2];
-    if (area != 0.0f && !(w1.x < 0.0f || w2.x < 0.0f))
-      visc_flux<DIR_R>(w1, sWb[p1], sT1[v1], sT2[v1], w2, sWb[p2], sT1[v2], sT2[v2], j, F, FY);
-  }
-}
-template <class T>
-__device__ __noinline__ void visc_member_face(const Grid& g, int q, const int* xc, const float4* sW, const float4* sWb,
-                                              const float4* sT1, const float4* sT2, const float* sAr, float4* sF,
-                                              float4* sY) {
-  const int Nx = g.Nx, Nr = g.Nr;
-  const int e = q >> 2, w = q & 3, m = xc[e];
-  const int mx = m % Nx, my = m / Nx, vb = T::NTT + 5 * e;
-  const float area = sAr[T::NXF + T::NRF + q];
-  float4 F, FY;
-  if (w == 0) visc_face<false>(mx > 0 && mx < Nx && my < Nr, area, my, ext_prim<T>(e, -1, 0), ext_prim<T>(e, 0, 0),
-                               vb + 1, vb, sW, sWb, sT1, sT2, F, FY);
-  else if (w == 1) visc_face<false>(mx + 1 > 0 && mx + 1 < Nx && my < Nr, area, my, ext_prim<T>(e, 0, 0),
-                                    ext_prim<T>(e, 1, 0), vb, vb + 2, sW, sWb, sT1, sT2, F, FY);
-  else if (w == 2) visc_face<true>(mx < Nx && my > 0 && my < Nr, area, my, ext_prim<T>(e, 0, -1), ext_prim<T>(e, 0, 0),
-                                   vb + 3, vb, sW, sWb, sT1, sT2, F, FY);
-  else visc_face<true>(mx < Nx && my + 1 > 0 && my + 1 < Nr, area, my + 1, ext_prim<T>(e, 0, 0), ext_prim<T>(e, 0, 1),
-                       vb, vb + 4, sW, sWb, sT1, sT2, F, FY);
-  sF[T::NXF + T::NRF + q] = F;
-  sY[T::NXF + T::NRF + q] = FY;
-}
-
-// FS_VFLUX_X/R: viscous faces of the tile and of the members.
+// FS_VFLUX_X/R: every viscous face of the tile and of its listed members in
+// one loop through one instance of the flux code (as the inviscid faces):
+// primitive slots p1 (behind the face) and p2 (the face's cell), vcell slots
+// v1 and v2; zero flux where it is not drawn or a side is a wall.
 template <class T>
 __device__ __forceinline__ void viscous_faces(const Grid& g, int x0, int y0, const int* xc, int xn, const float4* sW,
                                               const float4* sWb, const float4* sT1, const float4* sT2,
                                               const float* sAr, float4* sF, float4* sY) {
-  constexpr int TX = T::TX, PX = T::PX, TW = T::TW;
+  constexpr int TX = T::TX, PX = T::PX, TW = T::TW, NXR = T::NXF + T::NRF;
   const int Nx = g.Nx, Nr = g.Nr;
-  for (int k = threadIdx.x; k < T::NXF; k += T::NT) {
-    const int ly = k / (TX + 1), lx = k - ly * (TX + 1), i = x0 + lx, j = y0 + ly;
-    const int p2 = (ly + 2) * PX + lx + 2, v2 = (ly + 1) * TW + lx + 1;
-    visc_face<false>(i > 0 && i < Nx && j < Nr, sAr[k], j, p2 - 1, p2, v2 - 1, v2, sW, sWb, sT1, sT2, sF[k], sY[k]);
+  for (int k = threadIdx.x; k < NXR + 4 * xn; k += T::NT) {
+    int i, j, p1, p2, v1, v2;
+    bool dirR;
+    if (k < NXR) {
+      dirR = k >= T::NXF;
+      const int kk = dirR ? k - T::NXF : k, W = dirR ? TX : TX + 1;
+      const int ly = kk / W, lx = kk - ly * W;
+      i = x0 + lx; j = y0 + ly;
+      p2 = (ly + 2) * PX + lx + 2; p1 = p2 - (dirR ? PX : 1);
+      v2 = (ly + 1) * TW + lx + 1; v1 = v2 - (dirR ? TW : 1);
+    } else {                                     // member e's face w (W, E at mx + o; S, N at my + o)
+      const int q = k - NXR, e = q >> 2, w = q & 3, o = w & 1, m = xc[e], vb = T::NTT + 5 * e;
+      dirR = w >= 2;
+      i = m % Nx + (dirR ? 0 : o); j = m / Nx + (dirR ? o : 0);
+      p1 = dirR ? ext_prim<T>(e, 0, o - 1) : ext_prim<T>(e, o - 1, 0);
+      p2 = p1 + (dirR ? 5 : 1);
+      v1 = o ? vb : vb + (dirR ? 3 : 1);
+      v2 = o ? vb + (dirR ? 4 : 2) : vb;
+    }
+    const bool ok = dirR ? (i < Nx && j > 0 && j < Nr) : (i > 0 && i < Nx && j < Nr);
+    float4 F = make_float4(0.f, 0.f, 0.f, 0.f), FY = F;
+    if (ok) {
+      // face k is face k of the inviscid phase, whose open area sAr[k] holds
+      // (every face drawn here was drawn there)
+      const float area = sAr[k];
+      const float4 w1 = sW[p1], w2 = sW[p2];
+      if (area != 0.0f && !(w1.x < 0.0f || w2.x < 0.0f))
+        visc_flux(dirR, w1, sWb[p1], sT1[v1], sT2[v1], w2, sWb[p2], sT1[v2], sT2[v2], j, F, FY);
+    }
+    sF[k] = F;
+    sY[k] = FY;
   }
-  for (int k = threadIdx.x; k < T::NRF; k += T::NT) {
-    const int ly = k / TX, lx = k - ly * TX, i = x0 + lx, j = y0 + ly;
-    const int p2 = (ly + 2) * PX + lx + 2, v2 = (ly + 1) * TW + lx + 1;
-    visc_face<true>(i < Nx && j > 0 && j < Nr, sAr[T::NXF + k], j, p2 - PX, p2, v2 - TW, v2, sW, sWb, sT1, sT2,
-                    sF[T::NXF + k], sY[T::NXF + k]);
-  }
-  for (int q = threadIdx.x; q < 4 * xn; q += T::NT) visc_member_face<T>(g, q, xc, sW, sWb, sT1, sT2, sAr, sF, sY);
 }
 
 // FS_SOURCE of cell (i, j) inside the grid. A, B = the stage-2 state of the
@@ -830,20 +794,16 @@ __device__ __forceinline__ void stage2_physics_body(const StageArgs& a, const Ph
     // in a phase of its own, its T1/T2 taking the faces' place.
     const int NU = T::NC + xn;
     for (int q = tid; q < NU + (T::WIDE ? NV : 0); q += NT) {
-      if (q < T::NC) {                            // q == tid here (NC <= NT)
-        const int i = x0 + q % TX, j = y0 + q / TX;
+      if (q < NU) {                               // a tile cell (q == tid, NC <= NT), then a listed member
+        int i, j;
+        if (q < T::NC) { i = x0 + q % TX; j = y0 + q / TX; }
+        else { const int m = xc[q - T::NC]; i = m % Nx; j = m / Nx; }
         if (i < Nx && j < Nr) {
           float4 oA, oB;
           update_cell<T, 2>(a, P, i, j, dt, t, x0, y0, xc, xn, sF, sY, sO, sAr, oA, oB);
           sA2[q] = oA;
           sB2[q] = oB;
         }
-      } else if (q < NU) {
-        const int e = q - T::NC, m = xc[e];
-        float4 oA, oB;
-        update_cell<T, 2>(a, P, m % Nx, m / Nx, dt, t, x0, y0, xc, xn, sF, sY, sO, sAr, oA, oB);
-        sA2[T::NC + e] = oA;
-        sB2[T::NC + e] = oB;
       } else {
         vcell_at<T>(g, P, dt, x0, y0, xc, q - NU, sW, sWb, sT1, sT2);
       }
@@ -929,7 +889,10 @@ __global__ void __launch_bounds__(T::NT, T::MINB) k_stage2phys(StageArgs a, Phys
 }
 
 // Batch kernels: block b belongs to instance blockInst[b]; its descriptor
-// (buffers, ring position, parameter block) is staged in shared memory.
+// (buffers, ring position, parameter block) is staged in shared memory, and
+// thread 0 derives the step's kernel arguments from it into shared memory too:
+// the body reads each field from there when it needs it, where arguments
+// built in registers would stay live across the whole body (and spill).
 __device__ __forceinline__ void load_inst(const BatchInst* insts, int inst, BatchInst& d) {
   __shared__ int di;
   if (threadIdx.x == 0) di = inst;
@@ -939,19 +902,12 @@ __device__ __forceinline__ void load_inst(const BatchInst* insts, int inst, Batc
   for (int q = threadIdx.x; q < int(sizeof(BatchInst) / sizeof(int)); q += blockDim.x) dst[q] = src[q];
   __syncthreads();
 }
-template <class T, int STAGE>
-__global__ void __launch_bounds__(T::NT, T::MINB) k_stage_batch(const BatchInst* insts, const int* blockInst, BatchPhase ph) {
-  extern __shared__ float4 sm[];
-  __shared__ float red[T::NT / 32];
-  __shared__ int xc[MAXX];
-  __shared__ uint64_t bar;
-  __shared__ BatchInst d;
-  load_inst(insts, blockInst[blockIdx.x], d);
+// The step's stage arguments of instance d (stage 1 or 2 + the split step).
+__device__ __forceinline__ void batch_stage_args(const BatchInst& d, const BatchPhase& ph, int stage, StageArgs& a) {
   const int s0 = (d.cur0 + ph.shift) % 3, s1 = (s0 + 1) % 3, s2 = (s0 + 2) % 3;
   const int si = d.stepIdx0 ^ ph.par, ws = d.wslot0 ^ ph.par;
-  StageArgs a;
   a.g = d.g;
-  if (STAGE == 1) {
+  if (stage == 1) {
     a.A = d.SA[s0]; a.B = d.SB[s0]; a.A0 = d.SA[s0]; a.B0 = d.SB[s0]; a.oA = d.SA[s1]; a.oB = d.SB[s1];
   } else {
     a.A = d.SA[s1]; a.B = d.SB[s1]; a.A0 = d.SA[s0]; a.B0 = d.SB[s0]; a.oA = d.SA[s2]; a.oB = d.SB[s2];
@@ -962,9 +918,21 @@ __global__ void __launch_bounds__(T::NT, T::MINB) k_stage_batch(const BatchInst*
   a.wOut = d.wmax + (1 - ws);
   a.finalCfl = ph.finalCfl;
   a.xoff = d.xoff; a.xcell = d.xcell; a.maxX = ph.maxX;
-  a.slotIn = STAGE == 1 ? s0 : s1;
+  a.slotIn = stage == 1 ? s0 : s1;
   a.tm = d.tm;
   a.err = d.err;
+}
+template <class T, int STAGE>
+__global__ void __launch_bounds__(T::NT, T::MINB) k_stage_batch(const BatchInst* insts, const int* blockInst, BatchPhase ph) {
+  extern __shared__ float4 sm[];
+  __shared__ float red[T::NT / 32];
+  __shared__ int xc[MAXX];
+  __shared__ uint64_t bar;
+  __shared__ BatchInst d;
+  __shared__ StageArgs a;
+  load_inst(insts, blockInst[blockIdx.x], d);
+  if (threadIdx.x == 0) batch_stage_args(d, ph, STAGE, a);
+  __syncthreads();
   const int local = blockIdx.x - d.firstBlock, by = local / d.tilesX, bx = local - by * d.tilesX;
   stage_body<T, STAGE>(a, d.P, bx, by, local, sm, red, xc, &bar);
 }
@@ -976,31 +944,25 @@ __global__ void __launch_bounds__(T::NT, T::MINB) k_stage2phys_batch(const Batch
   __shared__ int xc[MAXX];
   __shared__ uint64_t bar;
   __shared__ BatchInst d;
+  __shared__ StageArgs a;
+  __shared__ PhysArgs p;
   const int2 hv = heavy ? heavy[blockIdx.x] : make_int2(0, 0);   // (member, tile) of a heavy block
   load_inst(insts, heavy ? hv.x : blockInst[blockIdx.x], d);
-  const int s0 = (d.cur0 + ph.shift) % 3, s1 = (s0 + 1) % 3, s2 = (s0 + 2) % 3;
-  const int si = d.stepIdx0 ^ ph.par, ws = d.wslot0 ^ ph.par;
-  StageArgs a;
-  a.g = d.g;
-  a.A = d.SA[s1]; a.B = d.SB[s1]; a.A0 = d.SA[s0]; a.B0 = d.SB[s0]; a.oA = d.SA[s2]; a.oB = d.SB[s2];
-  a.stPrev = d.stepTex + si;
-  a.stNew = d.stepTex + (1 - si);
-  a.wIn = d.wmax + ws;
-  a.wOut = d.wmax + (1 - ws);
-  a.finalCfl = 0;
-  a.xoff = d.xoff; a.xcell = d.xcell; a.maxX = ph.maxX;
-  a.slotIn = s1;
-  a.tm = d.tm;
-  a.err = d.err;
-  PhysArgs p;
-  p.g = d.g;
-  p.A1 = d.SA[s1]; p.B1 = d.SB[s1]; p.A2 = d.SA[s2]; p.B2 = d.SB[s2]; p.oA = d.SA[s2]; p.oB = d.SB[s2];
-  p.st = d.stepTex + (1 - si);
-  p.wOut = d.wmax + (1 - ws);
-  p.finalCfl = ph.finalCfl;
-  p.xoff = d.xoff; p.xcell = d.xcell; p.maxX = ph.maxX;
   const int local = heavy ? hv.y : blockIdx.x - d.firstBlock, by = local / d.tilesX, bx = local - by * d.tilesX;
   if (!heavy && xSmall >= 0 && d.xoff[local + 1] - d.xoff[local] > xSmall) return;   // in the heavy launch
+  if (threadIdx.x == 0) {
+    batch_stage_args(d, ph, 2, a);
+    a.finalCfl = 0;
+    const int s0 = (d.cur0 + ph.shift) % 3, s1 = (s0 + 1) % 3, s2 = (s0 + 2) % 3;
+    const int si = d.stepIdx0 ^ ph.par, ws = d.wslot0 ^ ph.par;
+    p.g = d.g;
+    p.A1 = d.SA[s1]; p.B1 = d.SB[s1]; p.A2 = d.SA[s2]; p.B2 = d.SB[s2]; p.oA = d.SA[s2]; p.oB = d.SB[s2];
+    p.st = d.stepTex + (1 - si);
+    p.wOut = d.wmax + (1 - ws);
+    p.finalCfl = ph.finalCfl;
+    p.xoff = d.xoff; p.xcell = d.xcell; p.maxX = ph.maxX;
+  }
+  __syncthreads();
   stage2_physics_body<T>(a, p, d.P, bx, by, local, sm, red, xc, &bar);
 }
 
