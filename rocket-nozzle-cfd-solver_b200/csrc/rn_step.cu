@@ -98,8 +98,12 @@ __device__ __forceinline__ void block_max_to(float w, unsigned* out, float* red)
 
 // The dynamic shared memory rounded up to a 128-byte boundary (the halo
 // copies' destinations are 128-byte aligned; every layout reserves the slack).
+// The rounding is an element offset from the shared array itself, so the
+// compiler still knows every derived pointer addresses shared memory (a round
+// trip through an integer address would make them generic 64-bit pointers:
+// generic loads and two registers per pointer, which spilled).
 __device__ __forceinline__ float4* aligned_smem(float4* p) {
-  return reinterpret_cast<float4*>((reinterpret_cast<uintptr_t>(p) + 127) & ~uintptr_t(127));
+  return p + (((128u - (smem_addr(p) & 127u)) & 127u) >> 4);
 }
 
 // Shared-memory index of the primitive of cell (mx + dx, my + dy) for listed
@@ -889,10 +893,12 @@ __global__ void __launch_bounds__(T::NT, T::MINB) k_stage2phys(StageArgs a, Phys
 }
 
 // Batch kernels: block b belongs to instance blockInst[b]; its descriptor
-// (buffers, ring position, parameter block) is staged in shared memory, and
-// thread 0 derives the step's kernel arguments from it into shared memory too:
-// the body reads each field from there when it needs it, where arguments
-// built in registers would stay live across the whole body (and spill).
+// (buffers, ring position) is staged in shared memory, and thread 0 derives
+// the step's kernel arguments from it into shared memory too: the body reads
+// each field from there when it needs it, where arguments built in registers
+// would stay live across the whole body (and spill). The parameter block is
+// read in place from the read-only descriptor array, so the compiler can
+// reload a field rather than spill it.
 __device__ __forceinline__ void load_inst(const BatchInst* insts, int inst, BatchInst& d) {
   __shared__ int di;
   if (threadIdx.x == 0) di = inst;
@@ -923,21 +929,22 @@ __device__ __forceinline__ void batch_stage_args(const BatchInst& d, const Batch
   a.err = d.err;
 }
 template <class T, int STAGE>
-__global__ void __launch_bounds__(T::NT, T::MINB) k_stage_batch(const BatchInst* insts, const int* blockInst, BatchPhase ph) {
+__global__ void __launch_bounds__(T::NT, T::MINB) k_stage_batch(const BatchInst* __restrict__ insts, const int* blockInst, BatchPhase ph) {
   extern __shared__ float4 sm[];
   __shared__ float red[T::NT / 32];
   __shared__ int xc[MAXX];
   __shared__ uint64_t bar;
   __shared__ BatchInst d;
   __shared__ StageArgs a;
-  load_inst(insts, blockInst[blockIdx.x], d);
+  const int inst = blockInst[blockIdx.x];
+  load_inst(insts, inst, d);
   if (threadIdx.x == 0) batch_stage_args(d, ph, STAGE, a);
   __syncthreads();
   const int local = blockIdx.x - d.firstBlock, by = local / d.tilesX, bx = local - by * d.tilesX;
-  stage_body<T, STAGE>(a, d.P, bx, by, local, sm, red, xc, &bar);
+  stage_body<T, STAGE>(a, insts[inst].P, bx, by, local, sm, red, xc, &bar);
 }
 template <class T>
-__global__ void __launch_bounds__(T::NT, T::MINB) k_stage2phys_batch(const BatchInst* insts, const int* blockInst,
+__global__ void __launch_bounds__(T::NT, T::MINB) k_stage2phys_batch(const BatchInst* __restrict__ insts, const int* blockInst,
                                                                      BatchPhase ph, const int2* heavy, int xSmall) {
   extern __shared__ float4 sm[];
   __shared__ float red[T::NT / 32];
@@ -947,7 +954,8 @@ __global__ void __launch_bounds__(T::NT, T::MINB) k_stage2phys_batch(const Batch
   __shared__ StageArgs a;
   __shared__ PhysArgs p;
   const int2 hv = heavy ? heavy[blockIdx.x] : make_int2(0, 0);   // (member, tile) of a heavy block
-  load_inst(insts, heavy ? hv.x : blockInst[blockIdx.x], d);
+  const int inst = heavy ? hv.x : blockInst[blockIdx.x];
+  load_inst(insts, inst, d);
   const int local = heavy ? hv.y : blockIdx.x - d.firstBlock, by = local / d.tilesX, bx = local - by * d.tilesX;
   if (!heavy && xSmall >= 0 && d.xoff[local + 1] - d.xoff[local] > xSmall) return;   // in the heavy launch
   if (threadIdx.x == 0) {
@@ -963,7 +971,7 @@ __global__ void __launch_bounds__(T::NT, T::MINB) k_stage2phys_batch(const Batch
     p.xoff = d.xoff; p.xcell = d.xcell; p.maxX = ph.maxX;
   }
   __syncthreads();
-  stage2_physics_body<T>(a, p, d.P, bx, by, local, sm, red, xc, &bar);
+  stage2_physics_body<T>(a, p, insts[inst].P, bx, by, local, sm, red, xc, &bar);
 }
 
 // --------------------------------------------------------------------------
