@@ -230,6 +230,17 @@ int rn_build_tile_maps(rn_solver* h) {
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return fail(RN_ERR_CUDA, "cuTensorMapEncodeTiled (mask) failed: " + std::to_string(r));
+    // the cell geometry planes for shapes that stage them (TILE_WARPS < 32)
+    const cuuint32_t gmbox[2] = {cuuint32_t(4 * (TILE_TX[t] + 2)), cuuint32_t(TILE_TY[t] + 2)};
+    const cuuint32_t ggbox[2] = {cuuint32_t(4 * TILE_TX[t]), cuuint32_t(TILE_TY[t])};
+    r = enc(&maps[t].geoM, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, h->geoM, pdim, pstride, gmbox, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r == CUDA_SUCCESS)
+      r = enc(&maps[t].geoG, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, h->geoG, pdim, pstride, ggbox, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(RN_ERR_CUDA, "cuTensorMapEncodeTiled (geometry) failed: " + std::to_string(r));
   }
   CK(cudaMemcpyAsync(h->dMaps, maps.data(), sizeof(TileMaps) * NTILES, cudaMemcpyHostToDevice, h->stream));
   CK(cudaStreamSynchronize(h->stream));

@@ -66,6 +66,14 @@ struct TileT {
   static constexpr int NPT8 = (NPT + 7) / 8 * 8;
   static constexpr int MASKF4 = (MW * PY + 127) / 128 * 8;
   static constexpr unsigned HALO_BYTES = 2u * 16u * NPT + unsigned(MW) * PY;
+  // WIDE shapes (3 blocks per SM, shared memory to spare) also stage the cell
+  // geometry their update and split step read, geoM with a 1-cell ring (the
+  // vcell ring's turbulence lengths) and geoG, and keep the raw halo block
+  // alive past the face phase: their update reads no global memory for tile
+  // cells. STAGED_F4 = the float4 slots these add to the layout.
+  static constexpr int NGM = (TX + 2) * (TY + 2), NGM8 = (NGM + 7) / 8 * 8, NGG8 = (NC + 7) / 8 * 8;
+  static constexpr unsigned GEO_BYTES = 16u * (NGM + NC);
+  static constexpr int STAGED_F4 = WIDE ? 2 * NPT8 + NGM8 + NGG8 : 0;
 };
 using Tile0 = TileT<TILE_TX[0], TILE_TY[0], TILE_NT[0], TILE_WARPS[0], 0>;
 using Tile1 = TileT<TILE_TX[1], TILE_TY[1], TILE_NT[1], TILE_WARPS[1], 1>;
@@ -181,8 +189,8 @@ __host__ __device__ constexpr int stage_region_t(int xn) {
 }
 template <class T>
 __host__ __device__ constexpr size_t stage_smem_t(int maxX) {
-  return sizeof(float4) * (8 + T::MASKF4 + stage_region_t<T>(maxX) + (T::NXF + T::NRF + 4 * maxX + 3) / 4 +
-                           2 * (T::NPT + 25 * maxX));
+  return sizeof(float4) * (8 + T::MASKF4 + T::STAGED_F4 + stage_region_t<T>(maxX) +
+                           (T::NXF + T::NRF + 4 * maxX + 3) / 4 + 2 * (T::NPT + 25 * maxX));
 }
 
 // --------------------------------------------------------------------------
@@ -220,12 +228,54 @@ __device__ __forceinline__ void halo_issue(const TileMaps* tm, int slot, int x0,
   if (threadIdx.x == 0) {
     const TileMaps& M = tm[T::ID];
     mbar_init(bar, 1);
-    mbar_expect_tx(bar, T::HALO_BYTES);
+    mbar_expect_tx(bar, T::HALO_BYTES + (T::WIDE ? T::GEO_BYTES : 0u));
     tma_load_2d(R, &M.a[slot], 4 * (x0 - 2), y0 - 2, bar);
     tma_load_2d(R + T::NPT8, &M.b[slot], 4 * (x0 - 2), y0 - 2, bar);
     tma_load_2d(sMask, &M.mask, (x0 - 2) & ~15, y0 - 2, bar);
+    if constexpr (T::WIDE) {                     // geoM ring box, then geoG tile box, after the raw block
+      tma_load_2d(R + 2 * T::NPT8, &M.geoM, 4 * (x0 - 1), y0 - 1, bar);
+      tma_load_2d(R + 2 * T::NPT8 + T::NGM8, &M.geoG, 4 * x0, y0, bar);
+    }
   }
 }
+
+// Per-cell operands of the update, vcell and split-step phases: from the
+// staged boxes where the cell lies in them (WIDE shapes: the raw halo block,
+// mask, geoM ring and geoG tile stay in shared memory), else from global
+// memory (other shapes, whose raw block the face fluxes overwrite, and listed
+// members outside the boxes). The staged values are copies of the same cells.
+template <class T>
+struct CellSrc {
+  const Grid& g;
+  const float4* __restrict__ A;     // the stage's input state (the source of the raw block)
+  const float4* __restrict__ B;
+  const float4* raw;                // raw A at raw[0..NPT), raw B at raw[NPT8..)
+  const uint8_t* m;
+  int x0, y0, mo;
+  __device__ __forceinline__ bool in_halo(int i, int j) const {
+    return T::WIDE && unsigned(i - x0 + 2) < unsigned(T::PX) && unsigned(j - y0 + 2) < unsigned(T::PY);
+  }
+  __device__ __forceinline__ bool in_ring(int i, int j) const {
+    return T::WIDE && unsigned(i - x0 + 1) < unsigned(T::TX + 2) && unsigned(j - y0 + 1) < unsigned(T::TY + 2);
+  }
+  __device__ __forceinline__ bool in_tile(int i, int j) const {
+    return T::WIDE && unsigned(i - x0) < unsigned(T::TX) && unsigned(j - y0) < unsigned(T::TY);
+  }
+  __device__ __forceinline__ int hslot(int i, int j) const { return (j - y0 + 2) * T::PX + (i - x0 + 2); }
+  __device__ __forceinline__ bool solid(int i, int j) const {
+    return in_halo(i, j) ? m[(j - y0 + 2) * T::MW + mo + (i - x0 + 2)] != 0 : g.mask[j * g.Nx + i] != 0;
+  }
+  __device__ __forceinline__ float4 a(int i, int j) const { return in_halo(i, j) ? raw[hslot(i, j)] : A[j * g.Nx + i]; }
+  __device__ __forceinline__ float4 b(int i, int j) const {
+    return in_halo(i, j) ? raw[T::NPT8 + hslot(i, j)] : B[j * g.Nx + i];
+  }
+  __device__ __forceinline__ float4 gm(int i, int j) const {
+    return in_ring(i, j) ? raw[2 * T::NPT8 + (j - y0 + 1) * (T::TX + 2) + (i - x0 + 1)] : g.geoM[j * g.Nx + i];
+  }
+  __device__ __forceinline__ float4 gg(int i, int j) const {
+    return in_tile(i, j) ? raw[2 * T::NPT8 + T::NGM8 + (j - y0) * T::TX + (i - x0)] : g.geoG[j * g.Nx + i];
+  }
+};
 // Every thread waits for the halo copy (after a barrier that published the
 // mbarrier's initialisation). False, in every thread, when any thread gave
 // up; the block then records the error and leaves.
@@ -397,18 +447,18 @@ __device__ __forceinline__ void group_flux(int Hx, int Hy, int sm_, int x0, int 
 // FS_UPDATE of cell (i, j) inside the grid: the RK update of its host's
 // cut-cell group. Returns whether the cell is fluid.
 template <class T, int STAGE>
-__device__ __forceinline__ bool update_cell(const StageArgs& a, const rn_params& P, int i, int j, float dt, float t,
-                                            int x0, int y0, const int* xc, int xn, const float4* sF,
-                                            const float4* sY, const float* sO, const float* sAr, float4& oA,
-                                            float4& oB) {
+__device__ __forceinline__ bool update_cell(const StageArgs& a, const CellSrc<T>& cs, const rn_params& P, int i,
+                                            int j, float dt, float t, int x0, int y0, const int* xc, int xn,
+                                            const float4* sF, const float4* sY, const float* sO, const float* sAr,
+                                            float4& oA, float4& oB) {
   const Grid& g = a.g;
   const int Nx = g.Nx;
   const int k = j * Nx + i;
   // the cell's own operands in one round of loads; a slave cell (host kh != k)
   // then loads its host's
-  const uint8_t solid = g.mask[k];
-  const float4 gm = g.geoM[k], gg = g.geoG[k];
-  float4 A = a.A[k], B = a.B[k], A0 = STAGE == 2 ? a.A0[k] : A, B0 = STAGE == 2 ? a.B0[k] : B;
+  const bool solid = cs.solid(i, j);
+  const float4 gm = cs.gm(i, j), gg = cs.gg(i, j);
+  float4 A = cs.a(i, j), B = cs.b(i, j), A0 = STAGE == 2 ? a.A0[k] : A, B0 = STAGE == 2 ? a.B0[k] : B;
   if (solid) {
     oA = make_float4(P.ambCons[0], P.ambCons[1], P.ambCons[2], P.ambCons[3]);
     oB = make_float4(P.ambB[0], P.ambB[1], P.ambB[2], P.ambB[3]);
@@ -417,9 +467,9 @@ __device__ __forceinline__ bool update_cell(const StageArgs& a, const rn_params&
   const int Hx = i + iround(gm.x), Hy = j + iround(gm.y), kh = Hy * Nx + Hx;
   float ghz = gm.z;
   if (kh != k) {
-    A = a.A[kh]; B = a.B[kh];
+    A = cs.a(Hx, Hy); B = cs.b(Hx, Hy);
     if (STAGE == 2) { A0 = a.A0[kh]; B0 = a.B0[kh]; }
-    ghz = g.geoM[kh].z;
+    ghz = cs.gm(Hx, Hy).z;
   }
   Prim q = to_prim(A, B);
   float4 L = make_float4(0.f, 0.f, 0.f, 0.f), LY = L;
@@ -466,7 +516,7 @@ __device__ __forceinline__ bool update_cell(const StageArgs& a, const rn_params&
     float ubar = 0.0f;
     if (P.inj) ubar = clampf(UY.w, 0.0f, rho);
     else if (i == 0) {
-      float u0 = a.B[k].w;
+      float u0 = cs.b(i, j).w;
       bool on = STAGE == 2 && t > P.bar[2];
       ubar = on ? fminf(u0 + fminf(dt * P.bar[0], 1.0f) * (vx - u0), P.bar[1]) : u0;
     }
@@ -487,9 +537,11 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const rn_params& 
   const int x0 = bx * TX, y0 = by * T::TY;
   float4* sm = aligned_smem(smRaw);
   uint8_t* sMask = reinterpret_cast<uint8_t*>(sm);
-  float4* R = sm + T::MASKF4;
-  halo_issue<T>(a.tm, a.slotIn, x0, y0, R, sMask, bar);
+  float4* RAW = sm + T::MASKF4;                 // raw halo block (+ geometry boxes for WIDE shapes)
+  float4* R = RAW + T::STAGED_F4;               // face fluxes (other shapes: over the raw block)
+  halo_issue<T>(a.tm, a.slotIn, x0, y0, RAW, sMask, bar);
   const FirstAreas fa = first_areas<T>(g, x0, y0);
+  const CellSrc<T> cs{g, a.A, a.B, RAW, sMask, x0, y0, (x0 - 2) - ((x0 - 2) & ~15)};
   const int xb = a.xoff[tileId], xn = a.xoff[tileId + 1] - xb;
   const int NP = T::NPT + 25 * xn, NF = T::NXF + T::NRF + 4 * xn;
   float4* sF = R;
@@ -518,7 +570,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const rn_params& 
   }
   __syncthreads();
   if (!halo_wait(bar, a.err)) return;
-  load_prims<T>(g, a.A, a.B, t, P, x0, y0, xc, NP, R, sMask, sW, sWb);
+  load_prims<T>(g, a.A, a.B, t, P, x0, y0, xc, NP, RAW, sMask, sW, sWb);
   store_areas<T>(g, x0, y0, xc, xn, fa, sAr);
   __syncthreads();
   inviscid_faces<T>(g, P, xc, xn, sW, sWb, sF, sY, sO, sAr);
@@ -528,7 +580,7 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const rn_params& 
   float wcell = 0.0f;
   if (tid < T::NC && i < Nx && j < Nr) {
     float4 oA, oB;
-    const bool fluid = update_cell<T, STAGE>(a, P, i, j, dt, t, x0, y0, xc, xn, sF, sY, sO, sAr, oA, oB);
+    const bool fluid = update_cell<T, STAGE>(a, cs, P, i, j, dt, t, x0, y0, xc, xn, sF, sY, sO, sAr, oA, oB);
     const int k = j * Nx + i;
     a.oA[k] = oA;
     a.oB[k] = oB;
@@ -541,8 +593,9 @@ __device__ __forceinline__ void stage_body(const StageArgs& a, const rn_params& 
 // FS_VCELL of vcell slot k of the tile + 1 ring (k < NTT) or, after it, of a
 // listed member's cell or one of its 4 neighbours (itself, W, E, S, N).
 template <class T>
-__device__ __forceinline__ void vcell_at(const Grid& g, const rn_params& P, float dt, int x0, int y0, const int* xc,
-                                         int k, const float4* sW, const float4* sWb, float4* sT1, float4* sT2) {
+__device__ __forceinline__ void vcell_at(const Grid& g, const CellSrc<T>& cs, const rn_params& P, float dt, int x0,
+                                         int y0, const int* xc, int k, const float4* sW, const float4* sWb,
+                                         float4* sT1, float4* sT2) {
   const int Nx = g.Nx, Nr = g.Nr;
   int i, j, c, rs;
   if (k < T::NTT) {
@@ -559,7 +612,7 @@ __device__ __forceinline__ void vcell_at(const Grid& g, const rn_params& P, floa
   }
   float4 T1 = make_float4(0.f, 0.f, 0.f, 0.f), T2 = T1;
   if (i >= 0 && i < Nx && j >= 0 && j < Nr)
-    vcell(sW[c], sWb[c], sW[c + 1], sW[c - 1], sW[c + rs], sW[c - rs], i, j, g.geoM[j * Nx + i].w, dt, P, T1, T2);
+    vcell(sW[c], sWb[c], sW[c + 1], sW[c - 1], sW[c + rs], sW[c - rs], i, j, cs.gm(i, j).w, dt, P, T1, T2);
   sT1[k] = T1;
   sT2[k] = T2;
 }
@@ -612,7 +665,7 @@ __device__ __forceinline__ void viscous_faces(const Grid& g, int x0, int y0, con
 // cell's group host; Bw = the cell's own stage-2 B.w. A1/B1 (global) feed
 // the separation samples. Returns whether the cell is fluid.
 template <class T>
-__device__ __forceinline__ bool source_cell(const Grid& g, const float4* __restrict__ A1,
+__device__ __forceinline__ bool source_cell(const Grid& g, const CellSrc<T>& cs, const float4* __restrict__ A1,
                                             const float4* __restrict__ B1, const rn_params& P, int i, int j,
                                             float dt, int x0, int y0, const int* xc, int xn, const float4* sF,
                                             const float4* sY, const float* sAr, const float4* sT1,
@@ -621,8 +674,8 @@ __device__ __forceinline__ bool source_cell(const Grid& g, const float4* __restr
   constexpr int TW = T::TW;
   const int Nx = g.Nx, Nr = g.Nr;
   const int k = j * Nx + i;
-  const uint8_t solid = g.mask[k];
-  const float4 gmij = g.geoM[k], gg = g.geoG[k];
+  const bool solid = cs.solid(i, j);
+  const float4 gmij = cs.gm(i, j), gg = cs.gg(i, j);
   if (solid) {
     oA = make_float4(P.ambCons[0], P.ambCons[1], P.ambCons[2], P.ambCons[3]);
     oB = make_float4(P.ambB[0], P.ambB[1], P.ambB[2], P.ambB[3]);
@@ -638,7 +691,7 @@ __device__ __forceinline__ bool source_cell(const Grid& g, const float4* __restr
   const int vh = (Hy - y0 + 1) * TW + (Hx - x0 + 1);
   float4 T1h = sT1[vh], T2h = sT2[vh];
   if (P.visc) {
-    const int sm_ = iround(kh == k ? gmij.z : g.geoM[kh].z);
+    const int sm_ = iround(kh == k ? gmij.z : cs.gm(Hx, Hy).z);
     float LO = 0.0f;
     group_flux<T, false>(Hx, Hy, sm_, x0, y0, xc, xn, Nx, sF, sY, nullptr, sAr, L, LY, LO);
     // axisymmetric hoop stress
@@ -750,8 +803,9 @@ template <class T>
 __host__ __device__ constexpr size_t fused_smem_t(int maxX) {
   // alignment slack, mask block, face region, vcell T1/T2 (T::WIDE), stage-2
   // results, face areas, primitives
-  return sizeof(float4) * (8 + T::MASKF4 + fused_region8_t<T>(maxX) + (T::WIDE ? 2 * (T::NTT + 5 * maxX) : 0) +
-                           2 * (T::NC + maxX) + (T::NXF + T::NRF + 4 * maxX + 3) / 4 + 2 * (T::NPT + 25 * maxX));
+  return sizeof(float4) * (8 + T::MASKF4 + T::STAGED_F4 + fused_region8_t<T>(maxX) +
+                           (T::WIDE ? 2 * (T::NTT + 5 * maxX) : 0) + 2 * (T::NC + maxX) +
+                           (T::NXF + T::NRF + 4 * maxX + 3) / 4 + 2 * (T::NPT + 25 * maxX));
 }
 template <class T>
 __device__ __forceinline__ void stage2_physics_body(const StageArgs& a, const PhysArgs& p, const rn_params& P, int bx,
@@ -764,9 +818,11 @@ __device__ __forceinline__ void stage2_physics_body(const StageArgs& a, const Ph
   const int x0 = bx * TX, y0 = by * T::TY;
   float4* sm = aligned_smem(smRaw);
   uint8_t* sMask = reinterpret_cast<uint8_t*>(sm);
-  float4* R = sm + T::MASKF4;
-  halo_issue<T>(a.tm, a.slotIn, x0, y0, R, sMask, bar);
+  float4* RAW = sm + T::MASKF4;                 // raw halo block (+ geometry boxes for WIDE shapes)
+  float4* R = RAW + T::STAGED_F4;               // face region (other shapes: over the raw block)
+  halo_issue<T>(a.tm, a.slotIn, x0, y0, RAW, sMask, bar);
   const FirstAreas fa = first_areas<T>(g, x0, y0);
+  const CellSrc<T> cs{g, a.A, a.B, RAW, sMask, x0, y0, (x0 - 2) - ((x0 - 2) & ~15)};
   const int xb = a.xoff[tileId], xn = a.xoff[tileId + 1] - xb, xnP = P.visc ? xn : 0;
   const int NP = T::NPT + 25 * xn, NF = T::NXF + T::NRF + 4 * xn;
   const int NV = T::NTT + 5 * xnP;
@@ -782,7 +838,7 @@ __device__ __forceinline__ void stage2_physics_body(const StageArgs& a, const Ph
   const float dt = st.x, t = st.z;
   __syncthreads();
   if (!halo_wait(bar, a.err)) return;
-  load_prims<T>(g, a.A, a.B, t, P, x0, y0, xc, NP, R, sMask, sW, sWb);
+  load_prims<T>(g, a.A, a.B, t, P, x0, y0, xc, NP, RAW, sMask, sW, sWb);
   store_areas<T>(g, x0, y0, xc, xn, fa, sAr);
   __syncthreads();
   {
@@ -804,12 +860,12 @@ __device__ __forceinline__ void stage2_physics_body(const StageArgs& a, const Ph
         else { const int m = xc[q - T::NC]; i = m % Nx; j = m / Nx; }
         if (i < Nx && j < Nr) {
           float4 oA, oB;
-          update_cell<T, 2>(a, P, i, j, dt, t, x0, y0, xc, xn, sF, sY, sO, sAr, oA, oB);
+          update_cell<T, 2>(a, cs, P, i, j, dt, t, x0, y0, xc, xn, sF, sY, sO, sAr, oA, oB);
           sA2[q] = oA;
           sB2[q] = oB;
         }
       } else {
-        vcell_at<T>(g, P, dt, x0, y0, xc, q - NU, sW, sWb, sT1, sT2);
+        vcell_at<T>(g, cs, P, dt, x0, y0, xc, q - NU, sW, sWb, sT1, sT2);
       }
     }
   }
@@ -818,7 +874,7 @@ __device__ __forceinline__ void stage2_physics_body(const StageArgs& a, const Ph
   float4* sF = T::WIDE ? R : sT2 + NV;
   float4* sY = sF + NFV;
   if (!T::WIDE) {
-    for (int k = tid; k < NV; k += NT) vcell_at<T>(g, P, dt, x0, y0, xc, k, sW, sWb, sT1, sT2);
+    for (int k = tid; k < NV; k += NT) vcell_at<T>(g, cs, P, dt, x0, y0, xc, k, sW, sWb, sT1, sT2);
     __syncthreads();
   }
   if (P.visc) viscous_faces<T>(g, x0, y0, xc, xnP, sW, sWb, sT1, sT2, sAr, sF, sY);
@@ -830,8 +886,8 @@ __device__ __forceinline__ void stage2_physics_body(const StageArgs& a, const Ph
     const int k = j * Nx + i;
     float4 oA, oB, A = make_float4(0.f, 0.f, 0.f, 0.f), B = A;
     float Bw = 0.0f;
-    if (!g.mask[k]) {
-      float4 gm = g.geoM[k];
+    if (!cs.solid(i, j)) {
+      float4 gm = cs.gm(i, j);
       const int Hx = i + iround(gm.x), Hy = j + iround(gm.y);
       const int hx = Hx - x0, hy = Hy - y0;
       int s;
@@ -847,7 +903,7 @@ __device__ __forceinline__ void stage2_physics_body(const StageArgs& a, const Ph
       B = sB2[s];
       Bw = sB2[tid].w;
     }
-    const bool fluid = source_cell<T>(g, p.A1, p.B1, P, i, j, dt, x0, y0, xc, xnP, sF, sY, sAr, sT1, sT2, A, B, Bw,
+    const bool fluid = source_cell<T>(g, cs, p.A1, p.B1, P, i, j, dt, x0, y0, xc, xnP, sF, sY, sAr, sT1, sT2, A, B, Bw,
                                       oA, oB);
     p.oA[k] = oA;
     p.oB[k] = oB;

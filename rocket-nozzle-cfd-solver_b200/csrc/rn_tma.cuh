@@ -22,6 +22,8 @@ struct TileMaps {
   CUtensorMap a[3];     // state ring slots, plane A: box (PX x PY) float4 as 4*PX floats
   CUtensorMap b[3];     // plane B
   CUtensorMap mask;     // row-pitched copy of the solid mask: box (MW x PY) bytes
+  CUtensorMap geoM;     // geoM with a 1-cell ring: box (TX+2) x (TY+2) float4 (shapes that stage it)
+  CUtensorMap geoG;     // geoG of the tile: box TX x TY float4
 };
 
 // Width in bytes of the mask box of a tile whose halo row is PX cells wide:

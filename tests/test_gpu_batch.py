@@ -53,6 +53,13 @@ def test_tile_shapes_bit_identical(rn, oracle, kind):
 
 
 def test_fast_tile_shapes_agree(rn):
+    """Fast precision: every shape computes the same operations too, but
+    the compiler contracts multiply-adds per kernel, and the 14x16 shape's
+    kernels (which stage the cell geometry and keep the raw halo block in
+    shared memory) are compiled apart from the others; so shapes agree to a
+    few rounding steps, not bit for bit (exact precision is bit-identical
+    across shapes: test_tile_shapes_bit_identical)."""
+    from helpers import state_rel_l2
     s = setups(rn, "viscous", [(256, 96)])[0]
     outs = []
     for tile in ("16x16", "16x8", "16x15", "32x15", "14x16"):
@@ -60,7 +67,10 @@ def test_fast_tile_shapes_agree(rn):
         g.step(60, s.P)
         outs.append(g.readAll())
         g.close()
-    assert all(identical(outs[0], o) for o in outs[1:])
+    for tile, o in zip(("16x8", "16x15", "32x15", "14x16"), outs[1:]):
+        e = state_rel_l2(o, outs[0])
+        print(tile, "vs 16x16, fast precision:", {k: float(f"{v:.2e}") for k, v in e.items()})
+        assert max(e.values()) <= 1e-5, (tile, e)
 
 
 def test_autotune_restores_state(rn):
