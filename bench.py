@@ -471,12 +471,14 @@ CLASS_COUNTS = {(128, 48): 64, (256, 96): 64, (512, 192): 8, (1024, 384): 4}
 def class_solves(rn, size, count, t_end_s=2e-3, K=60, seed=64, fp64_samples=0):
     """Solves/s of `count` seeded nozzles of one grid class (configs.
     batched_instance: expansion 4-40, p0 10-100 bar, gamma 1.2/1.4, altitude
-    0-30 km, viscous), each run to 2 ms of simulated time (checked every K
-    steps), one at a time (rn_step per solve, in turn) and batched (one
-    SolverBatch; a member leaves the batch when it reaches 2 ms). Host clock
-    around the stepping, setups excluded; final exit thrust and mass flow of
-    every solve; the first `fp64_samples` solves checked against the oracle
-    run in FP64 for the same steps (the FP64-scheme error)."""
+    0-30 km, viscous), each run to 2 ms of simulated time in chunks of K steps
+    (`while t < t_end: step(K)`), one at a time (rn_step per solve, in turn,
+    default tile) and batched (one SolverBatch, tile shape from its autotuner,
+    rn_batch_run: every member stops on the device at its own chunk). Host
+    clock around the stepping, setups and the autotuner excluded. Final exit
+    thrust and mass flow of every solve; the first `fp64_samples` solves of
+    both forms checked against the oracle run in FP64 for the same steps (the
+    FP64-scheme error; also for the FP32 oracle, the scheme's own FP32 error)."""
     import torch
     from rocket_nozzle_cfd_solver_b200 import configs
     rng = np.random.default_rng(seed + size[0])
@@ -494,17 +496,16 @@ def class_solves(rn, size, count, t_end_s=2e-3, K=60, seed=64, fp64_samples=0):
         perf = rn.exit_performance(s, col)
         return {"steps": g.stepCount, "F": perf["F"], "mdot": perf["mdot"], "A": g.readAll()}
 
+    t_end = [t_setups_end(s, t_end_s) for s in setups]
     # one at a time
     hs = [start(s) for s in setups]
     ps = [rn.params_from_P(s.P) for s in setups]
+    single_tile = hs[0].tile
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    single = []
-    for g, s, p in zip(hs, setups, ps):
-        t_end = t_end_s / s.tScale
-        while float(g.readStepInfo()[2]) < t_end:
+    for g, te, p in zip(hs, t_end, ps):
+        while float(g.readStepInfo()[2]) < te:
             g.step(K, p)
-        single.append(g.stepCount)
     t_single = time.perf_counter() - t0
     single_res = [finish(g, s) for g, s in zip(hs, setups)]
     for g in hs:
@@ -514,41 +515,53 @@ def class_solves(rn, size, count, t_end_s=2e-3, K=60, seed=64, fp64_samples=0):
     batch = rn.SolverBatch()
     for g, s in zip(hs, setups):
         batch.add(g, s.P)
+    tile = batch.autotune(steps=12)
+    batch.sync()
     torch.cuda.synchronize()
+    launches0 = batch.kernelLaunches()
     t0 = time.perf_counter()
-    left = list(range(count))
-    while left:
-        batch.step(K)
-        batch.sync()
-        for q in list(left):
-            if float(hs[q].readStepInfo()[2]) >= t_setups_end(setups[q], t_end_s):
-                batch.remove(hs[q])
-                left.remove(q)
+    batch.run(t_end, chunk=K)
     t_batch = time.perf_counter() - t0
+    launches = batch.kernelLaunches() - launches0
     batch.close()
     batch_res = [finish(g, s) for g, s in zip(hs, setups)]
     for g in hs:
         g.close()
-    same = all(a["steps"] == b["steps"] and np.array_equal(a["A"]["A"], b["A"]["A"])
+    same_steps = all(a["steps"] == b["steps"] for a, b in zip(single_res, batch_res))
+    diff = max(float(np.linalg.norm(a["A"]["A"].astype(np.float64) - b["A"]["A"]) /
+                     max(np.linalg.norm(a["A"]["A"].astype(np.float64)), 1e-30))
                for a, b in zip(single_res, batch_res))
+
+    def rel(x, y):
+        return abs(x - y) / max(abs(y), 1e-30)
+
     fp64 = []
     if fp64_samples:
         oracle = ge.load_oracle()
         oracle.set_threads(os.cpu_count() or 1)
-        for s, r in list(zip(setups, batch_res))[:fp64_samples]:
-            o = oracle.OracleSolver(s.Nx, s.Nr, fp64=True)
-            o.setGeometry(s.geo)
-            init = s.initialState()
-            o.setState(init["A"], init["B"])
-            o.step(r["steps"], s.P)
-            op = rn.exit_performance(s, exit_column(o.readAll(), s))
-            o.close()
-            fp64.append({"steps": r["steps"], "thrust_rel_err": abs(r["F"] - op["F"]) / max(abs(op["F"]), 1e-30),
-                         "mdot_rel_err": abs(r["mdot"] - op["mdot"]) / max(abs(op["mdot"]), 1e-30)})
+        for s, r1, rb in list(zip(setups, single_res, batch_res))[:fp64_samples]:
+            ref = {}
+            for dbl in (True, False):
+                o = oracle.OracleSolver(s.Nx, s.Nr, fp64=dbl)
+                o.setGeometry(s.geo)
+                init = s.initialState()
+                o.setState(init["A"], init["B"])
+                o.step(rb["steps"], s.P)
+                ref[dbl] = rn.exit_performance(s, exit_column(o.readAll(), s))
+                o.close()
+            op = ref[True]
+            fp64.append({"steps": rb["steps"],
+                         "batched": {"thrust_rel_err": rel(rb["F"], op["F"]), "mdot_rel_err": rel(rb["mdot"], op["mdot"])},
+                         "one_at_a_time": {"thrust_rel_err": rel(r1["F"], op["F"]),
+                                           "mdot_rel_err": rel(r1["mdot"], op["mdot"])},
+                         "fp32_oracle": {"thrust_rel_err": rel(ref[False]["F"], op["F"]),
+                                         "mdot_rel_err": rel(ref[False]["mdot"], op["mdot"])}})
     steps = [r["steps"] for r in batch_res]
     return {"grid": f"{size[0]}x{size[1]}", "solves": count, "steps_to_2ms": [min(steps), max(steps)],
             "one_at_a_time_solves_per_s": count / t_single, "batched_solves_per_s": count / t_batch,
-            "speedup": t_single / t_batch, "results_identical": same, "fp64_error": fp64}
+            "speedup": t_single / t_batch, "tile": {"one_at_a_time": single_tile, "batched": tile},
+            "batched_launches": launches, "same_steps": same_steps,
+            "state_rel_l2_batched_vs_one_at_a_time": diff, "fp64_error": fp64}
 
 
 def t_setups_end(s, t_end_s):

@@ -231,6 +231,20 @@ int rn_batch_remove(rn_batch b, rn_handle h);
 int rn_batch_set_params(rn_batch b, rn_handle h, const rn_params* P);
 int rn_batch_size(rn_batch b, int* members, long long* cells);
 int rn_batch_step(rn_batch b, int n);
+/* Runs every member to its own stop, in chunks of `chunk` steps: member m
+ * keeps stepping while the simulated time of its current state (step info
+ * t_new, in the solver's time units) is below t_end[m] and, with max_steps >
+ * 0, the run has taken fewer than max_steps steps; both are checked before
+ * each chunk, so each member takes the steps of the host loop
+ * `while (t < t_end) rn_step(h, chunk, P)`. The checks run on the device (one
+ * small kernel and one 4(n+1)-byte read-back per chunk); a stopped member's
+ * blocks return at once and leave the launch (a rebuilt block table and
+ * graph) once the stopped members' blocks number at least one per SM and an
+ * eighth of the launch. steps[m] (may be NULL) receives the steps member m
+ * took.
+ * Returns when every member has stopped. The batch form of the reference's
+ * frame loop (app.js:965 calls step(n, P) until the user stops it). */
+int rn_batch_run(rn_batch b, const double* t_end, int chunk, long long max_steps, long long* steps);
 int rn_batch_sync(rn_batch b);
 /* tile shape of the batch's launches (RN_TILE_*) */
 int rn_batch_set_tile(rn_batch b, int shape);

@@ -83,7 +83,16 @@ struct rn_batch_t {
   const KernelSet* graphK = nullptr;
   int graphBlocks = -1, graphTile = -1, graphMaxX = -1, graphHeavy = -1;
   Flags graphFlags;
+  const int* graphActive = nullptr;
   long long launches = 0;
+  // rn_batch_run: per member, whether it still steps (empty outside a run);
+  // the same flags on the device, read by the kernels and the gate
+  std::vector<char> runActive;
+  int* dActive = nullptr;
+  double* dTEnd = nullptr;
+  int* dGate = nullptr;                 // the gate's output: active count, then the flags
+  int* hGate = nullptr;                 // pinned copy of it
+  size_t runCap = 0;
 };
 
 namespace {
@@ -123,17 +132,19 @@ int refresh(rn_batch_t* b) {
   const int nm = int(b->members.size());
   const int TX = TILE_TX[b->tile], TY = TILE_TY[b->tile];
   // block table: rebuilt when a member's grid size changed
+  // (members stopped in a run have no blocks: grid size 0 x 0 in the table)
   std::vector<int> layout(2 * nm);
   for (int m = 0; m < nm; m++) {
-    layout[2 * m] = b->members[m]->Nx;
-    layout[2 * m + 1] = b->members[m]->Nr;
+    const bool on = b->runActive.empty() || b->runActive[m];
+    layout[2 * m] = on ? b->members[m]->Nx : 0;
+    layout[2 * m + 1] = on ? b->members[m]->Nr : 0;
   }
   std::vector<int> first(nm), tilesX(nm);
   int nb = 0;
   for (int m = 0; m < nm; m++) {
     first[m] = nb;
-    tilesX[m] = (layout[2 * m] + TX - 1) / TX;
-    nb += tilesX[m] * ((layout[2 * m + 1] + TY - 1) / TY);
+    tilesX[m] = (b->members[m]->Nx + TX - 1) / TX;
+    nb += ((layout[2 * m] + TX - 1) / TX) * ((layout[2 * m + 1] + TY - 1) / TY);
   }
   if (layout != b->layout || nb != b->nblocks) {
     std::vector<int> table(std::max(nb, 1), 0);
@@ -179,6 +190,7 @@ int refresh(rn_batch_t* b) {
   // heavy tiles: their own fused launch (see XSMALL)
   std::vector<int2> heavy;
   for (int m = 0; m < nm; m++) {
+    if (!b->runActive.empty() && !b->runActive[m]) continue;
     const std::vector<int>& off = b->members[m]->hostXoff;
     for (size_t t = 0; t + 1 < off.size(); t++)
       if (off[t + 1] - off[t] > XSMALL) heavy.push_back(make_int2(m, int(t)));
@@ -240,6 +252,7 @@ int launch_step(rn_batch_t* b, int c, bool withSpray) {
   ph.shift = (c * delta) % 3;
   ph.par = c & 1;
   ph.maxX = b->maxX;
+  ph.active = b->runActive.empty() ? nullptr : b->dActive;
   const int nb = b->nblocks;
   ph.finalCfl = 0;
   b->K->batchStage1(b->dInst, b->dBlock, nb, ph, b->tile, b->stream);
@@ -257,6 +270,7 @@ int launch_step(rn_batch_t* b, int c, bool withSpray) {
     BCK(cudaEventRecord(b->evSprayFork, b->stream));
     BCK(cudaStreamWaitEvent(b->sprayStream, b->evSprayFork, 0));
     for (size_t m = 0; m < b->members.size(); m++) {
+      if (!b->runActive.empty() && !b->runActive[m]) continue;   // stopped in rn_batch_run
       rn_solver* h = b->members[m];
       const BatchInst& d = b->uploaded[m];
       const int s0 = (d.cur0 + ph.shift) % 3, s1 = (s0 + 1) % 3;
@@ -304,6 +318,7 @@ int launch_step(rn_batch_t* b, int c, bool withSpray) {
   if (f.inj && withSpray) {
     BCK(cudaStreamWaitEvent(b->stream, b->evSprayJoin, 0));   // the parcel steps are done
     for (size_t m = 0; m < b->members.size(); m++) {
+      if (!b->runActive.empty() && !b->runActive[m]) continue;
       rn_solver* h = b->members[m];
       const BatchInst& d = b->uploaded[m];
       const int s0 = (d.cur0 + ph.shift) % 3;
@@ -355,10 +370,139 @@ int build_graph(rn_batch_t* b) {
   b->graphMaxX = b->maxX;
   b->graphHeavy = b->split ? b->nHeavy : 0;
   b->graphFlags = b->flags;
+  b->graphActive = b->runActive.empty() ? nullptr : b->dActive;
   return RN_OK;
 }
 
 int launches_per_step(const rn_batch_t* b) { return 2 + ((b->flags.phys() && b->split) ? 1 : 0); }
+
+// The launches of n batch steps from the batch counter on (descriptors and
+// block table already refreshed): without sprays, up to the start of a period
+// step by step, whole periods from the graph, the rest step by step.
+int issue_steps(rn_batch_t* b, int n) {
+  int done = 0, rc = RN_OK;
+  if (b->flags.inj) {
+    // parcel heads and seeds change every step: launched step by step
+    for (; done < n; done++) {
+      rc = launch_step(b, b->ctr, true);
+      if (rc != RN_OK) return rc;
+      b->ctr = (b->ctr + 1) % PERIOD;
+    }
+    return RN_OK;
+  }
+  while (done < n && b->ctr != 0) {
+    rc = launch_step(b, b->ctr, false);
+    if (rc != RN_OK) return rc;
+    b->ctr = (b->ctr + 1) % PERIOD;
+    done++;
+  }
+  if (n - done >= PERIOD) {
+    const int* active = b->runActive.empty() ? nullptr : b->dActive;
+    if (!b->graph || b->graphK != b->K || b->graphBlocks != b->nblocks || b->graphTile != b->tile ||
+        b->graphMaxX != b->maxX || b->graphHeavy != (b->split ? b->nHeavy : 0) || !(b->graphFlags == b->flags) ||
+        b->graphActive != active) {
+      rc = build_graph(b);
+      if (rc != RN_OK) return rc;
+    }
+    while (n - done >= PERIOD) {
+      BCK(cudaGraphLaunch(b->graph, b->stream));
+      b->launches += PERIOD * launches_per_step(b);
+      done += PERIOD;
+    }
+  }
+  for (; done < n; done++) {
+    rc = launch_step(b, b->ctr, false);
+    if (rc != RN_OK) return rc;
+    b->ctr = (b->ctr + 1) % PERIOD;
+  }
+  return RN_OK;
+}
+
+// A member's host-side bookkeeping after n batch steps, as n calls of rn_step
+// would leave it.
+void advance(rn_solver* h, long long n, const Flags& f) {
+  h->cur = int((h->cur + n * f.delta()) % 3);
+  if (n & 1) {
+    h->stepIdx = 1 - h->stepIdx;
+    h->wslot = 1 - h->wslot;
+  }
+  h->wvalid = true;
+  h->s1last = f.inj ? (h->cur + 1) % 3 : (h->cur + 2) % 3;   // the last step's stage-1 slot
+  h->stepCount += n;
+}
+
+// Checks the members before the batch step stepping at batch counter c and
+// the run's step done (rn_batch_run): a member still stepping stops when its
+// simulated time t_new >= tEnd (the step info of its current state) or the run
+// reached maxSteps (> 0). out[0] = members still stepping, out[1 + m] = flags.
+__global__ void k_batch_gate(const BatchInst* __restrict__ insts, int nm, int par, const double* __restrict__ tEnd,
+                             long long done, long long maxSteps, int* active, int* out) {
+  __shared__ int count;
+  if (threadIdx.x == 0) count = 0;
+  __syncthreads();
+  int mine = 0;
+  for (int m = threadIdx.x; m < nm; m += blockDim.x) {
+    int on = active[m];
+    if (on) {
+      const BatchInst& d = insts[m];
+      const double t = double(d.stepTex[d.stepIdx0 ^ par].z);
+      if (!(t < tEnd[m]) || (maxSteps > 0 && done >= maxSteps)) on = 0;
+      active[m] = on;
+    }
+    out[1 + m] = on;
+    mine += on;
+  }
+  atomicAdd(&count, mine);
+  __syncthreads();
+  if (threadIdx.x == 0) out[0] = count;
+}
+
+// Device buffers of a run over nm members.
+int run_buffers(rn_batch_t* b, size_t nm) {
+  if (nm <= b->runCap) return RN_OK;
+  cudaFree(b->dActive);
+  cudaFree(b->dTEnd);
+  cudaFree(b->dGate);
+  cudaFreeHost(b->hGate);
+  b->dActive = nullptr; b->dTEnd = nullptr; b->dGate = nullptr; b->hGate = nullptr;
+  b->runCap = 0;
+  drop_graph(b);   // a graph may hold the old flags pointer
+  BCK(cudaMalloc(&b->dActive, sizeof(int) * nm));
+  BCK(cudaMalloc(&b->dTEnd, sizeof(double) * nm));
+  BCK(cudaMalloc(&b->dGate, sizeof(int) * (nm + 1)));
+  BCK(cudaHostAlloc(reinterpret_cast<void**>(&b->hGate), sizeof(int) * (nm + 1), cudaHostAllocDefault));
+  b->runCap = nm;
+  return RN_OK;
+}
+
+// Checks the batch's members before a step (rn_batch_step, rn_batch_run) and
+// orders their queued work before the batch's kernels.
+int prepare(rn_batch_t* b) {
+  const KernelSet* K = b->members[0]->K;
+  for (rn_solver* h : b->members) {
+    if (h->K != K) return bfail(RN_ERR_STATE, "rn_batch_step: members have different precisions");
+    if (h->tile != b->tile) return bfail(RN_ERR_STATE, "rn_batch_step: a member's tile shape differs from the batch's");
+    if (!h->SA[0]) return bfail(RN_ERR_STATE, "rn_batch_step: a member has no buffers");
+  }
+  b->K = K;
+  // each member's CFL wave speed of its current state, and its queued work,
+  // before the batch's kernels
+  for (size_t m = 0; m < b->members.size(); m++) {
+    rn_solver* h = b->members[m];
+    int rc = rn_ensure_wave_speed(h);
+    if (rc != RN_OK) return rc;
+    BCK(cudaEventRecord(b->fence[m], h->stream));
+    BCK(cudaStreamWaitEvent(b->stream, b->fence[m], 0));
+  }
+  return RN_OK;
+}
+
+// Later work of each member waits for the batch.
+int release_members(rn_batch_t* b) {
+  BCK(cudaEventRecord(b->done, b->stream));
+  for (rn_solver* h : b->members) BCK(cudaStreamWaitEvent(h->stream, b->done, 0));
+  return RN_OK;
+}
 
 }  // namespace
 
@@ -368,6 +512,87 @@ void rn_batch_detach(rn_solver* h) {
 }
 
 extern "C" {
+
+int rn_batch_step(rn_batch b, int n) {
+  if (!b || n < 0) return bfail(RN_ERR_ARG, "rn_batch_step: bad argument");
+  if (b->members.empty() || n == 0) return RN_OK;
+  int rc = prepare(b);
+  if (rc == RN_OK) rc = refresh(b);
+  if (rc == RN_OK) rc = issue_steps(b, n);
+  if (rc != RN_OK) return rc;
+  BCK(cudaGetLastError());
+  for (rn_solver* h : b->members) advance(h, n, b->flags);
+  return release_members(b);
+}
+
+int rn_batch_run(rn_batch b, const double* t_end, int chunk, long long max_steps, long long* steps) {
+  if (!b || !t_end || chunk < 1 || max_steps < 0) return bfail(RN_ERR_ARG, "rn_batch_run: bad argument");
+  const size_t nm = b->members.size();
+  if (steps)
+    for (size_t m = 0; m < nm; m++) steps[m] = 0;
+  if (nm == 0) return RN_OK;
+  int rc = prepare(b);
+  if (rc == RN_OK) rc = run_buffers(b, nm);
+  if (rc != RN_OK) return rc;
+  std::vector<int> on(nm, 1);
+  BCK(cudaMemcpyAsync(b->dTEnd, t_end, sizeof(double) * nm, cudaMemcpyHostToDevice, b->stream));
+  BCK(cudaMemcpyAsync(b->dActive, on.data(), sizeof(int) * nm, cudaMemcpyHostToDevice, b->stream));
+  b->runActive.assign(nm, 1);
+  auto finish = [&](int code) {
+    // outside a run every member steps again; the next step rebuilds the
+    // table and the descriptors
+    b->runActive.clear();
+    b->layout.clear();
+    b->uploaded.clear();
+    if (code != RN_OK) return code;
+    return release_members(b);
+  };
+  rc = refresh(b);
+  int tableBlocks = b->nblocks;
+  long long done = 0;
+  while (rc == RN_OK) {
+    k_batch_gate<<<1, 256, 0, b->stream>>>(b->dInst, int(nm), b->ctr & 1, b->dTEnd, done, max_steps, b->dActive,
+                                           b->dGate);
+    b->launches++;
+    cudaError_t e = cudaMemcpyAsync(b->hGate, b->dGate, sizeof(int) * (nm + 1), cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) { rc = rn_record_cuda(e, "rn_batch_run: gate"); break; }
+    if (b->hGate[0] == 0) break;
+    int activeBlocks = 0;
+    for (size_t m = 0; m < nm; m++) {
+      b->runActive[m] = char(b->hGate[1 + m] != 0);
+      const rn_solver* h = b->members[m];
+      if (b->runActive[m])
+        activeBlocks += ((h->Nx + TILE_TX[b->tile] - 1) / TILE_TX[b->tile]) *
+                        ((h->Nr + TILE_TY[b->tile] - 1) / TILE_TY[b->tile]);
+    }
+    // the stopped members' blocks leave the table (a new table and graph)
+    // once they number an SM's worth and an eighth of it; until then they
+    // return at once
+    const int stoppedBlocks = tableBlocks - activeBlocks;
+    if (stoppedBlocks >= b->numSMs && 8 * stoppedBlocks >= tableBlocks) {
+      rc = refresh(b);
+      if (rc != RN_OK) break;
+      tableBlocks = b->nblocks;
+    }
+    const long long left = max_steps > 0 ? max_steps - done : chunk;
+    const int n = int(left < chunk ? left : chunk);
+    rc = issue_steps(b, n);
+    if (rc != RN_OK) break;
+    for (size_t m = 0; m < nm; m++)
+      if (b->runActive[m]) {
+        advance(b->members[m], n, b->flags);
+        if (steps) steps[m] += n;
+      }
+    done += n;
+  }
+  if (rc == RN_OK) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) rc = rn_record_cuda(e, "rn_batch_run");
+  }
+  return finish(rc);
+}
+
 
 int rn_batch_create(rn_batch* out) {
   if (!out) return bfail(RN_ERR_ARG, "rn_batch_create: out is NULL");
@@ -404,6 +629,10 @@ int rn_batch_destroy(rn_batch b) {
   cudaFree(b->dInst);
   cudaFree(b->dBlock);
   cudaFree(b->dHeavy);
+  cudaFree(b->dActive);
+  cudaFree(b->dTEnd);
+  cudaFree(b->dGate);
+  cudaFreeHost(b->hGate);
   cudaFreeHost(b->hInst);
   cudaEventDestroy(b->staged);
   cudaEventDestroy(b->done);
@@ -504,79 +733,6 @@ int rn_batch_set_tile(rn_batch b, int shape) {
   b->tile = shape;
   b->layout.clear();   // block table and descriptors are rebuilt by the next step
   b->uploaded.clear();
-  return RN_OK;
-}
-
-int rn_batch_step(rn_batch b, int n) {
-  if (!b || n < 0) return bfail(RN_ERR_ARG, "rn_batch_step: bad argument");
-  if (b->members.empty() || n == 0) return RN_OK;
-  const KernelSet* K = b->members[0]->K;
-  for (rn_solver* h : b->members) {
-    if (h->K != K) return bfail(RN_ERR_STATE, "rn_batch_step: members have different precisions");
-    if (h->tile != b->tile) return bfail(RN_ERR_STATE, "rn_batch_step: a member's tile shape differs from the batch's");
-    if (!h->SA[0]) return bfail(RN_ERR_STATE, "rn_batch_step: a member has no buffers");
-  }
-  b->K = K;
-  // each member's CFL wave speed of its current state, and its queued work,
-  // before the batch's kernels
-  for (size_t m = 0; m < b->members.size(); m++) {
-    rn_solver* h = b->members[m];
-    int rc = rn_ensure_wave_speed(h);
-    if (rc != RN_OK) return rc;
-    BCK(cudaEventRecord(b->fence[m], h->stream));
-    BCK(cudaStreamWaitEvent(b->stream, b->fence[m], 0));
-  }
-  int rc = refresh(b);
-  if (rc != RN_OK) return rc;
-  const Flags f = b->flags;
-  int done = 0;
-  if (f.inj) {
-    // parcel heads and seeds change every step: launched step by step
-    for (; done < n; done++) {
-      rc = launch_step(b, b->ctr, true);
-      if (rc != RN_OK) return rc;
-      b->ctr = (b->ctr + 1) % PERIOD;
-    }
-  } else {
-    // up to the start of a period step by step, whole periods from the graph
-    while (done < n && b->ctr != 0) {
-      launch_step(b, b->ctr, false);
-      b->ctr = (b->ctr + 1) % PERIOD;
-      done++;
-    }
-    if (n - done >= PERIOD) {
-      if (!b->graph || b->graphK != b->K || b->graphBlocks != b->nblocks || b->graphTile != b->tile ||
-          b->graphMaxX != b->maxX || b->graphHeavy != (b->split ? b->nHeavy : 0) || !(b->graphFlags == f)) {
-        rc = build_graph(b);
-        if (rc != RN_OK) return rc;
-      }
-      while (n - done >= PERIOD) {
-        BCK(cudaGraphLaunch(b->graph, b->stream));
-        b->launches += PERIOD * launches_per_step(b);
-        done += PERIOD;
-      }
-    }
-    for (; done < n; done++) {
-      launch_step(b, b->ctr, false);
-      b->ctr = (b->ctr + 1) % PERIOD;
-    }
-  }
-  BCK(cudaGetLastError());
-  // the handles' bookkeeping, as n calls of rn_step would leave it
-  const int delta = f.delta();
-  for (rn_solver* h : b->members) {
-    h->cur = int((h->cur + (long long)n * delta) % 3);
-    if (n & 1) {
-      h->stepIdx = 1 - h->stepIdx;
-      h->wslot = 1 - h->wslot;
-    }
-    h->wvalid = true;
-    h->s1last = f.inj ? (h->cur + 1) % 3 : (h->cur + 2) % 3;   // the last step's stage-1 slot
-    h->stepCount += n;
-  }
-  // later work of each member waits for the batch
-  BCK(cudaEventRecord(b->done, b->stream));
-  for (rn_solver* h : b->members) BCK(cudaStreamWaitEvent(h->stream, b->done, 0));
   return RN_OK;
 }
 

@@ -125,6 +125,7 @@ struct BatchPhase {
   int par;                              // step parity: stepIdx = stepIdx0 ^ par, wslot = wslot0 ^ par
   int finalCfl;                         // the launched kernel writes the step's final state
   int maxX;
+  const int* active;                    // if set: per member, 0 = stopped (its blocks return at once)
 };
 
 // The kernels are compiled twice from the same sources (rn_variant.cu):

@@ -43,6 +43,29 @@ RN_DEV float fdiv(float a, float b) {
   return a / b;
 #endif
 }
+// Several quotients over one divisor b: over(b)(a) == fdiv(a, b). The fast
+// variant forms the reciprocal once and multiplies (fdiv there is a times the
+// hardware reciprocal of b); the exact variant divides each time.
+struct Over {
+  float b, r;
+  RN_DEV float operator()(float a) const {
+#ifdef RN_FAST
+    return a * r;
+#else
+    return a / b;
+#endif
+  }
+};
+RN_DEV Over over(float b) {
+  Over o;
+  o.b = b;
+#ifdef RN_FAST
+  o.r = __fdividef(1.0f, b);
+#else
+  o.r = 0.0f;
+#endif
+  return o;
+}
 
 // Pairs of lanes through Blackwell's packed FP32 instructions (two IEEE
 // round-to-nearest operations per instruction, each lane rounding as the
@@ -80,12 +103,13 @@ RN_DEV bool solid_at(const Grid& g, int i, int j) { return g.mask[j * g.Nx + i] 
 RN_DEV Prim to_prim(float4 a, float4 b) {
   Prim q;
   float rho = fmaxf(a.x, RHO_MIN);
-  float vx = fdiv(a.y, rho), vy = fdiv(a.z, rho);
+  const Over per_rho = over(rho);
+  float vx = per_rho(a.y), vy = per_rho(a.z);
   float G = fmaxf(b.z, 0.5f);
   float p = fmaxf(fdiv(a.w - 0.5f * rho * (vx * vx + vy * vy), G), P_MIN);
   q.w = make_float4(rho, vx, vy, p);
-  q.s = make_float4(clampf(fdiv(b.x, rho), 0.0f, 1.0f), clampf(fdiv(b.y, rho), 0.0f, 1.0f), G,
-                    clampf(fdiv(b.w, rho), 0.0f, 1.0f));
+  q.s = make_float4(clampf(per_rho(b.x), 0.0f, 1.0f), clampf(per_rho(b.y), 0.0f, 1.0f), G,
+                    clampf(per_rho(b.w), 0.0f, 1.0f));
   return q;
 }
 // soundSpeed (solver.js:40)
@@ -205,12 +229,27 @@ RN_DEV float van_leer_of(float ab, float den) {
   return ab > 0.0f ? fdiv(2.0f * ab, den) : copysignf(0.0f, den);
 }
 RN_DEV float van_leer(float a, float b) { return van_leer_of(a * b, a + b); }
+#ifdef RN_FAST
+// Fast variant of a lane pair: ab > 0 means a and b of one sign, so |den| =
+// |a| + |b| >= 2 sqrt(ab) > 1e-30 and the guard never applies; 2 ab / den is
+// 2 ab times the hardware reciprocal of den (what fdiv computes), the pair's
+// products in one packed multiply. Where ab <= 0 the limiter is a zero (its
+// sign, which van_leer_of takes from den, only signs a zero face difference).
+RN_DEV float2 van_leer2(float2 ab, float2 den) {
+  const float2 q = mul2(add2(ab, ab), make_float2(__fdividef(1.0f, den.x), __fdividef(1.0f, den.y)));
+  return make_float2(ab.x > 0.0f ? q.x : 0.0f, ab.y > 0.0f ? q.y : 0.0f);
+}
+#endif
 // Componentwise van_leer(a, b) of two float4 slopes.
 RN_DEV float4 van_leer4(float4 a, float4 b) {
   const float2 ab0 = mul2(lo2(a), lo2(b)), ab1 = mul2(hi2(a), hi2(b));
   const float2 dn0 = add2(lo2(a), lo2(b)), dn1 = add2(hi2(a), hi2(b));
+#ifdef RN_FAST
+  return cat4(van_leer2(ab0, dn0), van_leer2(ab1, dn1));
+#else
   return make_float4(van_leer_of(ab0.x, dn0.x), van_leer_of(ab0.y, dn0.y), van_leer_of(ab1.x, dn1.x),
                      van_leer_of(ab1.y, dn1.y));
+#endif
 }
 // w + h * d per component (h = +-0.5: the MUSCL face values).
 RN_DEV float4 step4(float4 w, float h, float4 d) {
@@ -283,14 +322,16 @@ RN_DEV Flux face_flux(bool DIR_R, float area, float4 w0, float4 b0, float4 w1, f
   float GL = WLs.z, GR = WRs.z;
   float rL = WLw.x, uL = WLw.y, vL = WLw.z, pL = WLw.w;
   float rR = WRw.x, uR = WRw.y, vR = WRw.z, pR = WRw.w;
-  float cL = sqrtf(fdiv((1.0f + fdiv(1.0f, GL)) * pL, rL)), cR = sqrtf(fdiv((1.0f + fdiv(1.0f, GR)) * pR, rR));
+  const Over per_rL = over(rL), per_rR = over(rR);
+  float cL = sqrtf(per_rL((1.0f + fdiv(1.0f, GL)) * pL)), cR = sqrtf(per_rR((1.0f + fdiv(1.0f, GR)) * pR));
   float EL = pL * GL + 0.5f * rL * (uL * uL + vL * vL);
   float ER = pR * GR + 0.5f * rR * (uR * uR + vR * vR);
   float sL = sqrtf(rL), sR = sqrtf(rR);
-  float uT = fdiv(sL * uL + sR * uR, sL + sR);
-  float HT = fdiv(fdiv(sL * (EL + pL), rL) + fdiv(sR * (ER + pR), rR), sL + sR);
-  float vT = fdiv(sL * vL + sR * vR, sL + sR);
-  float GT = fdiv(sL * GL + sR * GR, sL + sR);
+  const Over per_s = over(sL + sR);
+  float uT = per_s(sL * uL + sR * uR);
+  float HT = per_s(per_rL(sL * (EL + pL)) + per_rR(sR * (ER + pR)));
+  float vT = per_s(sL * vL + sR * vR);
+  float GT = per_s(sL * GL + sR * GR);
   float cT = sqrtf(fmaxf(fdiv(HT - 0.5f * (uT * uT + vT * vT), GT), 1e-12f));
   float SL = fminf(uL - cL, uT - cT);
   float SR = fmaxf(uR + cR, uT + cT);
@@ -311,7 +352,8 @@ RN_DEV Flux face_flux(bool DIR_R, float area, float4 w0, float4 b0, float4 w1, f
     float FK0 = left ? FL0 : FR0, FK1 = left ? FL1 : FR1, FK2 = left ? FL2 : FR2, FK3 = left ? FL3 : FR3;
     float FYK0 = left ? YL0 : YR0, FYK1 = left ? YL1 : YR1, FYK2 = left ? YL2 : YR2;
     float UK1 = left ? mL : mR, UK2 = rK * vK;
-    float kk = fdiv(rK * (SK - uK), SK - Ss);
+    const Over per_dS = over(SK - Ss);
+    float kk = per_dS(rK * (SK - uK));
     float Us0 = kk * 1.0f, Us1 = kk * Ss, Us2 = kk * vK, Us3 = kk * (fdiv(EK, rK) + (Ss - uK) * (Ss + fdiv(pK, rK * (SK - uK))));
     float C0 = FK0 + SK * (Us0 - rK), C1 = FK1 + SK * (Us1 - UK1), C2 = FK2 + SK * (Us2 - UK2), C3 = FK3 + SK * (Us3 - EK);
     float CY0 = FYK0 + SK * (kk * YK0 - rK * YK0), CY1 = FYK1 + SK * (kk * YK1 - rK * YK1);
@@ -334,7 +376,7 @@ RN_DEV Flux face_flux(bool DIR_R, float area, float4 w0, float4 b0, float4 w1, f
       F0 = C0; F1 = C1; F2 = C2; F3 = C3;
       Y0 = CY0; Y1 = CY1; Y2 = CY2;
     }
-    uf = uK + SK * (fdiv(SK - uK, SK - Ss) - 1.0f);
+    uf = uK + SK * (per_dS(SK - uK) - 1.0f);
     Gf = left ? GL : GR;
   }
   if (DIR_R) { float t = F1; F1 = F2; F2 = t; }    // rotate momentum back to (x, r)
@@ -378,10 +420,11 @@ RN_DEV void vcell(float4 w0, float4 sc, float4 wE, float4 wW, float4 wN, float4 
   float fE = wE.x < 0.0f ? 0.0f : 1.0f, fW = wW.x < 0.0f ? 0.0f : 1.0f;
   float fN = wN.x < 0.0f ? 0.0f : 1.0f, fS = wS.x < 0.0f ? 0.0f : 1.0f;
   float dxn = fmaxf(fE + fW, 1.0f), drn = fmaxf(fN + fS, 1.0f);
-  float ux = fdiv(fE * (wE.y - w0.y) + fW * (w0.y - wW.y), dxn);
-  float vx = fdiv(fE * (wE.z - w0.z) + fW * (w0.z - wW.z), dxn);
-  float ur = fdiv(fN * (wN.y - w0.y) + fS * (w0.y - wS.y), drn);
-  float vr = fdiv(fN * (wN.z - w0.z) + fS * (w0.z - wS.z), drn);
+  const Over per_dx = over(dxn), per_dr = over(drn);
+  float ux = per_dx(fE * (wE.y - w0.y) + fW * (w0.y - wW.y));
+  float vx = per_dx(fE * (wE.z - w0.z) + fW * (w0.z - wW.z));
+  float ur = per_dr(fN * (wN.y - w0.y) + fS * (w0.y - wS.y));
+  float vr = per_dr(fN * (wN.z - w0.z) + fS * (w0.z - wS.z));
   float r = float(j) + 0.5f, vor = fdiv(w0.z, r);
   float div = ux + vr + vor;
   float S2 = 2.0f * (ux * ux + vr * vr + vor * vor) + (ur + vx) * (ur + vx) - 0.6666667f * div * div;

@@ -480,7 +480,8 @@ __device__ __forceinline__ bool update_cell(const StageArgs& a, const CellSrc<T>
   // embedded wall: pressure force along the r-weighted wall vector
   float wl = len2(gg.z, gg.w);
   if (wl > 1e-6f) {
-    float nx = fdiv(gg.z, wl), nr = fdiv(gg.w, wl);
+    const Over per_wl = over(wl);
+    float nx = per_wl(gg.z), nr = per_wl(gg.w);
     float pw = wall_pressure(q, q.w.y * nx + q.w.z * nr);
     L.y -= gg.z * pw;
     L.z -= gg.w * pw;
@@ -500,8 +501,8 @@ __device__ __forceinline__ bool update_cell(const StageArgs& a, const CellSrc<T>
                      0.5f * (B0.z + B.z + f * LB.z), 0.5f * (B0.w + B.w + f * LB.w));
   }
   float rho = fmaxf(U.x, RHO_MIN);
-  float den = fmaxf(U.x, RHO_MIN);
-  float vx = fdiv(U.y, den), vy = fdiv(U.z, den);
+  const Over per_den = over(fmaxf(U.x, RHO_MIN));
+  float vx = per_den(U.y), vy = per_den(U.z);
   float sp = len2(vx, vy);
   if (sp > P.vMax) { float s = fdiv(P.vMax, sp); vx *= s; vy *= s; }
   if (!(rho < 1e30f) || !(vx < 1e30f && vx > -1e30f)) {   // NaN guard
@@ -700,7 +701,8 @@ __device__ __forceinline__ bool source_cell(const Grid& g, const CellSrc<T>& cs,
     // Werner-Wengle wall shear and Reynolds-analogy heat flux
     float wl = len2(gg.z, gg.w);
     if (wl > 1e-6f) {
-      float nx = fdiv(gg.z, wl), nr = fdiv(gg.w, wl);
+      const Over per_wl = over(wl);
+      float nx = per_wl(gg.z), nr = per_wl(gg.w);
       float dn = velx * nx + vely * nr;
       float utx = velx - dn * nx, uty = vely - dn * nr;
       float up = len2(utx, uty);
@@ -767,7 +769,8 @@ __device__ __forceinline__ bool source_cell(const Grid& g, const CellSrc<T>& cs,
     }
   }
   float rn = fmaxf(U.x, RHO_MIN);
-  float vnx = fdiv(U.y, rn), vny = fdiv(U.z, rn);
+  const Over per_rn = over(rn);
+  float vnx = per_rn(U.y), vny = per_rn(U.z);
   if (!(rn < 1e30f) || !(vnx < 1e30f && vnx > -1e30f)) {
     oA = make_float4(P.ambCons[0], P.ambCons[1], P.ambCons[2], P.ambCons[3]);
     oB = make_float4(P.ambB[0], P.ambB[1], P.ambB[2], P.ambB[3]);
@@ -993,6 +996,7 @@ __global__ void __launch_bounds__(T::NT, T::MINB) k_stage_batch(const BatchInst*
   __shared__ BatchInst d;
   __shared__ StageArgs a;
   const int inst = blockInst[blockIdx.x];
+  if (ph.active && !ph.active[inst]) return;      // a member stopped by rn_batch_run: the whole block
   load_inst(insts, inst, d);
   if (threadIdx.x == 0) batch_stage_args(d, ph, STAGE, a);
   __syncthreads();
@@ -1011,6 +1015,7 @@ __global__ void __launch_bounds__(T::NT, T::MINB) k_stage2phys_batch(const Batch
   __shared__ PhysArgs p;
   const int2 hv = heavy ? heavy[blockIdx.x] : make_int2(0, 0);   // (member, tile) of a heavy block
   const int inst = heavy ? hv.x : blockInst[blockIdx.x];
+  if (ph.active && !ph.active[inst]) return;      // a member stopped by rn_batch_run: the whole block
   load_inst(insts, inst, d);
   const int local = heavy ? hv.y : blockIdx.x - d.firstBlock, by = local / d.tilesX, bx = local - by * d.tilesX;
   if (!heavy && xSmall >= 0 && d.xoff[local + 1] - d.xoff[local] > xSmall) return;   // in the heavy launch

@@ -31,7 +31,7 @@ EXPORTS = ("rn_create", "rn_destroy", "rn_resize", "rn_set_mask", "rn_set_geomet
            "rn_set_precision", "rn_get_precision", "rn_get_stream", "rn_profile", "rn_profile_read",
            "rn_integrals_static", "rn_set_tile", "rn_get_tile", "rn_autotune", "rn_batch_create",
            "rn_batch_destroy", "rn_batch_add", "rn_batch_remove", "rn_batch_set_params", "rn_batch_size",
-           "rn_batch_step", "rn_batch_sync", "rn_batch_set_tile", "rn_batch_autotune", "rn_batch_stream",
+           "rn_batch_step", "rn_batch_run", "rn_batch_sync", "rn_batch_set_tile", "rn_batch_autotune", "rn_batch_stream",
            "rn_batch_kernel_launches", "rn_residual_mark", "rn_residual", "rn_server_default_opts",
            "rn_server_create", "rn_server_destroy", "rn_serve_submit", "rn_serve_poll", "rn_serve_wait",
            "rn_serve_stats", "rn_solve_bytes", "rn_set_wall_profile", "rn_wall_separation", "rn_derived",
@@ -262,6 +262,8 @@ def lib():
     L.rn_batch_set_params.argtypes = [H, H, ctypes.POINTER(RnParams)]
     L.rn_batch_size.argtypes = [H, ctypes.POINTER(i), ctypes.POINTER(ctypes.c_longlong)]
     L.rn_batch_step.argtypes = [H, i]
+    L.rn_batch_run.argtypes = [H, ctypes.POINTER(ctypes.c_double), i, ctypes.c_longlong,
+                               ctypes.POINTER(ctypes.c_longlong)]
     L.rn_batch_sync.argtypes = [H]
     L.rn_batch_set_tile.argtypes = [H, i]
     L.rn_batch_autotune.argtypes = [H, i, ctypes.POINTER(i)]
@@ -724,6 +726,23 @@ class SolverBatch:
         _check(lib().rn_batch_step(self.b, int(n)))
         for s in self.members:
             s.stepCount += int(n)
+
+    def run(self, t_end, chunk=60, max_steps=0):
+        """Steps every member in chunks of `chunk` steps until its simulated
+        time (step info t_new, solver units) reaches its entry of t_end, or
+        the run has taken max_steps (> 0), both checked on the device before
+        each chunk: the steps of `while t < t_end: solver.step(chunk, P)` run
+        for each member alone. Returns the steps each member took."""
+        n = len(self.members)
+        te = (ctypes.c_double * max(n, 1))(*[float(v) for v in t_end])
+        if len(t_end) != n:
+            raise ValueError("t_end needs one entry per member")
+        out = (ctypes.c_longlong * max(n, 1))()
+        _check(lib().rn_batch_run(self.b, te, int(chunk), int(max_steps), out))
+        steps = [int(out[k]) for k in range(n)]
+        for s, k in zip(self.members, steps):
+            s.stepCount += k
+        return steps
 
     def sync(self):
         _check(lib().rn_batch_sync(self.b))

@@ -261,3 +261,64 @@ def test_default_tile_by_grid_size(rn):
         tiles = -(-Nx // 14) * -(-Nr // 16)
         assert g.tile == ("14x16" if tiles <= 3 * sms else "16x15"), (Nx, Nr, g.tile)
         g.close()
+
+
+def loop_to(g, s, t_end, chunk):
+    """The plain form of a run to a stop time: `while t < t_end: step(chunk)`."""
+    steps = 0
+    while float(g.readStepInfo()[2]) < t_end:
+        g.step(chunk, s.P)
+        steps += chunk
+    return steps
+
+
+@pytest.mark.parametrize("kind,sizes,chunk", [
+    ("viscous", [(320, 120), (200, 76), (96, 36)], 7),
+    ("plain", [(320, 120), (160, 60), (128, 48)], 12),
+    ("spray", [(320, 120), (96, 36), (112, 40)], 5),
+])
+def test_batch_run_matches_host_loops(rn, kind, sizes, chunk):
+    """rn_batch_run stops each member on the device before the chunk at which
+    its simulated time reaches its own t_end: every member takes the steps of
+    the host loop run alone and ends bit-identical to it. The first member
+    stops at once (t_end 0): its 160 blocks (16 x 15 tiles) are more than an
+    SM's worth, so they leave the launch at the first chunk; the second stops
+    after 3 chunks, and its blocks then return early until the run ends. A
+    capped run (max_steps) and plain batch steps afterwards continue from the
+    same ring positions."""
+    ss = setups(rn, kind, sizes)
+    # stop times: 0, and the probe's time after 2 chunks + 3 and 5 chunks
+    probe = [make(rn, s) for s in ss]
+    t_end = [0.0]
+    for g, s, n in zip(probe[1:], ss[1:], (2 * chunk + 3, 5 * chunk)):
+        g.step(n, s.P)
+        t_end.append(float(g.readStepInfo()[2]))
+    for g in probe:
+        g.close()
+    batch = rn.SolverBatch()
+    members = [make(rn, s) for s in ss]
+    singles = [make(rn, s) for s in ss]
+    for g, s in zip(members, ss):
+        batch.add(g, s.P)
+    steps = batch.run(t_end, chunk=chunk)
+    want = [loop_to(h, s, te, chunk) for h, s, te in zip(singles, ss, t_end)]
+    assert steps == want and steps[0] == 0 and steps[1] == 3 * chunk and steps[2] >= 5 * chunk, (steps, want)
+    for g, h in zip(members, singles):
+        assert g.stepCount == h.stepCount
+        assert identical(g.readAll(), h.readAll()) and np.array_equal(g.readStepInfo(), h.readStepInfo())
+    # a capped run: every member takes max_steps steps
+    steps = batch.run([1e30] * len(ss), chunk=chunk, max_steps=2 * chunk + 1)
+    assert steps == [2 * chunk + 1] * len(ss)
+    for h, s in zip(singles, ss):
+        h.step(2 * chunk + 1, s.P)
+    batch.step(9)
+    for h, s in zip(singles, ss):
+        h.step(9, s.P)
+    for g, h in zip(members, singles):
+        assert identical(g.readAll(), h.readAll()) and np.array_equal(g.readStepInfo(), h.readStepInfo())
+    if kind == "spray":
+        for g, h in zip(members, singles):
+            assert np.array_equal(g.spray.readParcels()["PA"], h.spray.readParcels()["PA"])
+    batch.close()
+    for g in members + singles:
+        g.close()
