@@ -437,9 +437,16 @@ int rn_serve_inject(rn_server s, int where);
 int rn_get_stream(rn_handle h, void** stream);
 
 /* Per-kernel device time: with profiling on, every kernel the handle launches
- * is bracketed by CUDA events on its stream. rn_profile_read waits for the
- * stream, returns milliseconds and launch counts per kernel kind (indexed by
- * RN_K_*) accumulated since the last read, and clears them. */
+ * is bracketed by CUDA events on its stream. enable = 1: launch by launch
+ * (rn_step does not replay its graph, so the times include the gaps in
+ * which the GPU waits for the host's next launch); enable = 2: steps without
+ * sprays run as replays of a graph of one period that holds an event pair
+ * around each kernel (event-record nodes), read after every replay, so each
+ * kernel is timed as it runs back to back with the others; the steps before
+ * the first whole period, and spray steps, are timed launch by launch. 0
+ * turns it off. rn_profile_read waits for the stream, returns milliseconds
+ * and launch counts per kernel kind (indexed by RN_K_*) accumulated since the
+ * last read, and clears them. */
 #define RN_K_REDUCE 0
 #define RN_K_STAGE1 1
 #define RN_K_STAGE2 2

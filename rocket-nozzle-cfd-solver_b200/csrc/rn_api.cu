@@ -343,15 +343,20 @@ struct ProfScope {
   ProfScope(rn_solver* h_, int kind_) : h(h_), kind(kind_) {
     if (h->prof) {
       e0 = prof_event(h);
-      cudaEventRecord(e0, h->stream);
+      record(e0);
     }
   }
   ~ProfScope() {
     if (h->prof && e0) {
       cudaEvent_t e1 = prof_event(h);
-      cudaEventRecord(e1, h->stream);
-      h->evPending.push_back({kind, {e0, e1}});
+      record(e1);
+      (h->profCapture ? h->profGraphEv : h->evPending).push_back({kind, {e0, e1}});
     }
+  }
+  // while a graph is captured for profiling, as an event-record node of it
+  void record(cudaEvent_t e) {
+    if (h->profCapture) cudaEventRecordWithFlags(e, h->stream, cudaEventRecordExternal);
+    else cudaEventRecord(e, h->stream);
   }
 };
 
@@ -699,6 +704,70 @@ void drop_step_graph(rn_solver* h) {
   if (h->stepGraph) cudaGraphExecDestroy(h->stepGraph);
   h->stepGraph = nullptr;
 }
+
+// Profiling inside graph replays (rn_profile mode 2, steps without sprays):
+// one period of the handle's launches is captured with an event pair around
+// each kernel (event-record nodes of the graph) and replayed period by
+// period, the pairs read after each replay, so each kernel is timed as it
+// runs in the replayed graph (no host launch gaps between the kernels). The
+// steps before the first whole period run one by one, timed launch by launch.
+int prof_graph_steps(rn_solver* h, const rn_params* P, int n, int& done) {
+  while (done < n && !h->wvalid) {
+    int rc = step_once(h, P);
+    if (rc != RN_OK) return rc;
+    done++;
+  }
+  if (n - done < STEP_PERIOD) return RN_OK;
+  if (h->nHeavy > 0 && !h->side) {   // the helper stream exists before the capture
+    CK(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&h->evFork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&h->evJoin, cudaEventDisableTiming));
+  }
+  const int cur = h->cur, stepIdx = h->stepIdx, wslot = h->wslot, s1last = h->s1last;
+  const long long stepCount = h->stepCount, launches = h->launches;
+  cudaGraph_t gr = nullptr;
+  cudaGraphExec_t ex = nullptr;
+  h->profGraphEv.clear();
+  h->profCapture = true;
+  cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+  int rc = RN_OK;
+  for (int k = 0; k < STEP_PERIOD && rc == RN_OK && e == cudaSuccess; k++) rc = step_once(h, P);
+  cudaError_t e2 = e == cudaSuccess ? cudaStreamEndCapture(h->stream, &gr) : e;
+  h->profCapture = false;
+  const long long perPeriod = h->launches - launches;
+  h->cur = cur; h->stepIdx = stepIdx; h->wslot = wslot; h->s1last = s1last;
+  h->stepCount = stepCount; h->launches = launches;
+  auto release = [&]() {
+    for (auto& p : h->profGraphEv) {
+      h->evPool.push_back(p.second.first);
+      h->evPool.push_back(p.second.second);
+    }
+    h->profGraphEv.clear();
+    if (ex) cudaGraphExecDestroy(ex);
+    if (gr) cudaGraphDestroy(gr);
+  };
+  if (rc != RN_OK) { release(); return rc; }
+  if (e2 != cudaSuccess) { release(); return cuda_fail(e2, "rn_step: profiled graph capture"); }
+  e = cudaGraphInstantiate(&ex, gr, 0);
+  if (e != cudaSuccess) { ex = nullptr; release(); return cuda_fail(e, "rn_step: profiled graph instantiate"); }
+  while (n - done >= STEP_PERIOD) {
+    e = cudaGraphLaunch(ex, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    for (auto& p : h->profGraphEv) {
+      float t = 0.0f;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&t, p.second.first, p.second.second);
+      h->profMs[p.first] += t;
+      h->profN[p.first] += 1;
+    }
+    if (e != cudaSuccess) { release(); return cuda_fail(e, "rn_step: profiled graph replay"); }
+    h->s1last = (h->cur + 1 + 2 * (STEP_PERIOD - 1)) % 3;
+    h->stepCount += STEP_PERIOD;
+    h->launches += perPeriod;
+    done += STEP_PERIOD;
+  }
+  release();
+  return RN_OK;
+}
 }  // namespace
 
 extern "C" {
@@ -728,6 +797,10 @@ int rn_step(rn_handle h, int n, const rn_params* P) {
   // own: the launches then go into that graph as they are)
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(h->stream, &cs) != cudaSuccess) cs = cudaStreamCaptureStatusNone;
+  if (h->prof == 2 && !inj && cs == cudaStreamCaptureStatusNone && n >= 2 * period) {
+    int rc = prof_graph_steps(h, P, n, done);
+    if (rc != RN_OK) return rc;
+  }
   if (!h->prof && cs == cudaStreamCaptureStatusNone && n >= 2 * period) {
     while (done < n && (!h->wvalid || (graph_matches(h, P) && !at_start()))) {
       int rc = step_once(h, P);
@@ -1126,8 +1199,8 @@ int rn_autotune(rn_handle h, const rn_params* P, int steps, int* chosen) {
   const bool wvalid = h->wvalid;
   const long long stepCount = h->stepCount, launches = h->launches;
   const uint32_t head = h->head, seed = h->seed;
-  const bool prof = h->prof;
-  h->prof = false;
+  const int prof = h->prof;
+  h->prof = 0;
   cudaError_t e = copy_all(true);
   int best = h->tile, rc = RN_OK;
   float bestMs = 1e30f;
@@ -1182,8 +1255,8 @@ int rn_get_stream(rn_handle h, void** stream) {
 }
 
 int rn_profile(rn_handle h, int enable) {
-  if (!h) return fail(RN_ERR_ARG, "rn_profile: NULL handle");
-  h->prof = enable != 0;
+  if (!h || enable < 0 || enable > 2) return fail(RN_ERR_ARG, "rn_profile: bad argument");
+  h->prof = enable;
   return RN_OK;
 }
 

@@ -53,8 +53,12 @@ struct rn_solver {
   bool asyncBusy = false;
   int asyncTag = 0;
   double* dInt = nullptr;
-  // per-kernel event timing
-  bool prof = false;
+  // per-kernel event timing: prof = 1 launch by launch, 2 inside replays of
+  // the step graph (profCapture while that graph is captured; its event
+  // pairs, read after every replay, in profGraphEv)
+  int prof = 0;
+  bool profCapture = false;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> profGraphEv;
   std::vector<cudaEvent_t> evPool;
   std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> evPending;
   double profMs[RN_NKERNELS] = {0};

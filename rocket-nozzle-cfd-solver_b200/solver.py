@@ -608,9 +608,11 @@ class GPUSolver:
         _check(lib().rn_get_stream(self.h, ctypes.byref(v)))
         return v.value or 0
 
-    def profile(self, enable):
-        """Bracket every kernel with CUDA events on the handle's stream."""
-        _check(lib().rn_profile(self.h, 1 if enable else 0))
+    def profile(self, enable, in_graph=False):
+        """Bracket every kernel with CUDA events on the handle's stream:
+        launch by launch, or (in_graph) inside replays of the step graph,
+        as event-record nodes around each kernel of the replayed period."""
+        _check(lib().rn_profile(self.h, (2 if in_graph else 1) if enable else 0))
 
     def profileRead(self):
         """{kind: (milliseconds, launches)} since the last read."""

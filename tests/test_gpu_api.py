@@ -279,6 +279,30 @@ def test_kernel_launch_accounting(rn):
     g.close()
 
 
+def test_in_graph_profile_times_every_kernel_and_keeps_results(rn):
+    """Profiling inside the replayed step graph (rn_profile mode 2): every
+    kernel of the replayed periods is timed (one event pair per kernel per
+    period), the steps before the first whole period launch by launch, and
+    the results are those of unprofiled stepping, bit for bit."""
+    s, _ = golden_case(rn, "viscous")
+    g, ref = gpu(rn, s), gpu(rn, s)
+    g.profile(True, in_graph=True)
+    g.step(27, s.P)                  # 1 step alone (its CFL reduction first), 4 periods of 6, 2 alone
+    prof = g.profileRead()
+    g.profile(False)
+    assert prof["stage1"][1] == 27 and prof["stage2_physics"][1] == 27 and prof["reduce"][1] == 1, prof
+    assert all(v[0] > 0 for k, v in prof.items() if v[1])
+    ref.step(27, s.P)
+    a, b = g.readAll(), ref.readAll()
+    assert np.array_equal(a["A"], b["A"]) and np.array_equal(a["B"], b["B"])
+    assert np.array_equal(g.readStepInfo(), ref.readStepInfo()) and g.stepCount == ref.stepCount == 27
+    g.step(13, s.P)                  # the handle's own graph afterwards
+    ref.step(13, s.P)
+    assert np.array_equal(g.readAll()["A"], ref.readAll()["A"])
+    g.close()
+    ref.close()
+
+
 @pytest.mark.parametrize("precision", ["fast", "exact"])
 def test_prepopulated_parcel_ring_matches_oracle(rn, oracle, precision):
     """A ring already holding 16,384 seeded parcels (lognormal diameters,
