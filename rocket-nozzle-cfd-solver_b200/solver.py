@@ -736,9 +736,9 @@ class SolverBatch:
         each chunk: the steps of `while t < t_end: solver.step(chunk, P)` run
         for each member alone. Returns the steps each member took."""
         n = len(self.members)
-        te = (ctypes.c_double * max(n, 1))(*[float(v) for v in t_end])
         if len(t_end) != n:
             raise ValueError("t_end needs one entry per member")
+        te = (ctypes.c_double * max(n, 1))(*[float(v) for v in t_end])
         out = (ctypes.c_longlong * max(n, 1))()
         _check(lib().rn_batch_run(self.b, te, int(chunk), int(max_steps), out))
         steps = [int(out[k]) for k in range(n)]

@@ -322,3 +322,23 @@ def test_batch_run_matches_host_loops(rn, kind, sizes, chunk):
     batch.close()
     for g in members + singles:
         g.close()
+
+
+def test_batch_run_rejects_bad_arguments_and_empty_batches(rn):
+    """A chunk below 1 or a negative step cap is refused before anything is
+    queued; an empty batch runs no steps; a t_end list of the wrong length is
+    refused by the host wrapper."""
+    ss = setups(rn, "plain", [(96, 36)])
+    batch = rn.SolverBatch()
+    assert batch.run([], chunk=6) == []
+    g = make(rn, ss[0])
+    batch.add(g, ss[0].P)
+    for kw in ({"chunk": 0}, {"chunk": 6, "max_steps": -1}):
+        with pytest.raises(rn.RnError):
+            batch.run([1.0], **kw)
+    with pytest.raises(ValueError):
+        batch.run([1.0, 2.0], chunk=6)
+    assert g.stepCount == 0
+    assert batch.run([0.0], chunk=6) == [0]                  # already at its stop time
+    batch.close()
+    g.close()
