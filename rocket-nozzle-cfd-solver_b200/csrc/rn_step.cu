@@ -316,20 +316,24 @@ __device__ __forceinline__ void load_prims(const Grid& g, const float4* __restri
                                            float t, const rn_params& P, int x0, int y0, const int* xc, int NP,
                                            const float4* R, const uint8_t* sMask, float4* sW, float4* sWb) {
   const int Nx = g.Nx, Nr = g.Nr;
-  const HaloCells<T> cells{g, A, B, R, R + T::NPT8, sMask, x0, y0, (x0 - 2) - ((x0 - 2) & ~15)};
+  const int mo = (x0 - 2) - ((x0 - 2) & ~15);
+  const HaloCells<T> cells{g, A, B, R, R + T::NPT8, sMask, x0, y0, mo};
   for (int k = threadIdx.x; k < NP; k += T::NT) {
-    int i, j;
+    int i, j, ly = 0, lx = 0;
     if (k < T::NPT) {
-      const int ly = k / T::PX;
-      i = x0 - 2 + (k - ly * T::PX); j = y0 - 2 + ly;
+      ly = k / T::PX; lx = k - ly * T::PX;
+      i = x0 - 2 + lx; j = y0 - 2 + ly;
     } else {                                     // member e's 5x5 block
       const int q = k - T::NPT, e = q / 25, r = q - e * 25, m = xc[e], dy = r / 5;
       i = m % Nx + (r - dy * 5) - 2; j = m / Nx + dy - 2;
     }
     float4 W, Wb;
     if (i >= 0 && i < Nx && j >= 0 && j < Nr) {     // ghost_prim's interior branch
-      const float4 a = cells.a(i, j), b = cells.b(i, j);
-      if (cells.solid(i, j)) {
+      // a slot of the staged block is its own cell k of it (no lookup)
+      const bool own = k < T::NPT;
+      const float4 a = own ? R[k] : cells.a(i, j), b = own ? R[T::NPT8 + k] : cells.b(i, j);
+      const bool solid = own ? sMask[ly * T::MW + mo + lx] != 0 : cells.solid(i, j);
+      if (solid) {
         W = make_float4(-1.0f, 0.0f, 0.0f, 1.0f);
         Wb = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
       } else {
@@ -633,8 +637,10 @@ __device__ __forceinline__ void viscous_faces(const Grid& g, int x0, int y0, con
     bool dirR;
     if (k < NXR) {
       dirR = k >= T::NXF;
-      const int kk = dirR ? k - T::NXF : k, W = dirR ? TX : TX + 1;
-      const int ly = kk / W, lx = kk - ly * W;
+      // x-face k: row k / (TX + 1); r-face k - NXF: row (k - NXF) / TX (both
+      // divisors compile-time constants)
+      const int kx = k / (TX + 1), kr = (k - T::NXF) / TX;
+      const int ly = dirR ? kr : kx, lx = dirR ? k - T::NXF - kr * TX : k - kx * (TX + 1);
       i = x0 + lx; j = y0 + ly;
       p2 = (ly + 2) * PX + lx + 2; p1 = p2 - (dirR ? PX : 1);
       v2 = (ly + 1) * TW + lx + 1; v1 = v2 - (dirR ? TW : 1);
