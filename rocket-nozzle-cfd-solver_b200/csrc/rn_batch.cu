@@ -90,8 +90,9 @@ struct rn_batch_t {
   std::vector<char> runActive;
   int* dActive = nullptr;
   double* dTEnd = nullptr;
-  int* dGate = nullptr;                 // the gate's output: active count, then the flags
-  int* hGate = nullptr;                 // pinned copy of it
+  int* dGate = nullptr;                 // 2 gate outputs: active count, then the flags
+  int* hGate = nullptr;                 // pinned copies of them
+  cudaEvent_t evGate[2] = {nullptr, nullptr};   // each copy's arrival
   size_t runCap = 0;
 };
 
@@ -469,8 +470,10 @@ int run_buffers(rn_batch_t* b, size_t nm) {
   drop_graph(b);   // a graph may hold the old flags pointer
   BCK(cudaMalloc(&b->dActive, sizeof(int) * nm));
   BCK(cudaMalloc(&b->dTEnd, sizeof(double) * nm));
-  BCK(cudaMalloc(&b->dGate, sizeof(int) * (nm + 1)));
-  BCK(cudaHostAlloc(reinterpret_cast<void**>(&b->hGate), sizeof(int) * (nm + 1), cudaHostAllocDefault));
+  BCK(cudaMalloc(&b->dGate, sizeof(int) * 2 * (nm + 1)));
+  BCK(cudaHostAlloc(reinterpret_cast<void**>(&b->hGate), sizeof(int) * 2 * (nm + 1), cudaHostAllocDefault));
+  for (int q = 0; q < 2; q++)
+    if (!b->evGate[q]) BCK(cudaEventCreateWithFlags(&b->evGate[q], cudaEventDisableTiming));
   b->runCap = nm;
   return RN_OK;
 }
@@ -547,44 +550,104 @@ int rn_batch_run(rn_batch b, const double* t_end, int chunk, long long max_steps
     if (code != RN_OK) return code;
     return release_members(b);
   };
-  rc = refresh(b);
-  int tableBlocks = b->nblocks;
+  const size_t G = nm + 1;
   long long done = 0;
-  while (rc == RN_OK) {
-    k_batch_gate<<<1, 256, 0, b->stream>>>(b->dInst, int(nm), b->ctr & 1, b->dTEnd, done, max_steps, b->dActive,
-                                           b->dGate);
+  // the gate for the steps issued so far (`at` of them), its flags read back
+  // into buffer `slot` behind event evGate[slot]
+  auto gate = [&](int slot, long long at) -> int {
+    k_batch_gate<<<1, 256, 0, b->stream>>>(b->dInst, int(nm), b->ctr & 1, b->dTEnd, at, max_steps, b->dActive,
+                                           b->dGate + slot * G);
     b->launches++;
-    cudaError_t e = cudaMemcpyAsync(b->hGate, b->dGate, sizeof(int) * (nm + 1), cudaMemcpyDeviceToHost, b->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
-    if (e != cudaSuccess) { rc = rn_record_cuda(e, "rn_batch_run: gate"); break; }
-    if (b->hGate[0] == 0) break;
+    BCK(cudaMemcpyAsync(b->hGate + slot * G, b->dGate + slot * G, sizeof(int) * G, cudaMemcpyDeviceToHost,
+                        b->stream));
+    BCK(cudaEventRecord(b->evGate[slot], b->stream));
+    return RN_OK;
+  };
+  // waits for gate buffer `slot`; the members still stepping become runActive
+  auto take = [&](int slot, int& count) -> int {
+    BCK(cudaEventSynchronize(b->evGate[slot]));
+    const int* f = b->hGate + slot * G;
+    count = f[0];
+    for (size_t m = 0; m < nm; m++) b->runActive[m] = char(f[1 + m] != 0);
+    return RN_OK;
+  };
+  int tableBlocks = 0;
+  // the stopped members' blocks leave the table (a new table and graph) once
+  // they number an SM's worth and an eighth of it; until then they return at
+  // once
+  auto compact = [&]() -> int {
     int activeBlocks = 0;
     for (size_t m = 0; m < nm; m++) {
-      b->runActive[m] = char(b->hGate[1 + m] != 0);
       const rn_solver* h = b->members[m];
       if (b->runActive[m])
         activeBlocks += ((h->Nx + TILE_TX[b->tile] - 1) / TILE_TX[b->tile]) *
                         ((h->Nr + TILE_TY[b->tile] - 1) / TILE_TY[b->tile]);
     }
-    // the stopped members' blocks leave the table (a new table and graph)
-    // once they number an SM's worth and an eighth of it; until then they
-    // return at once
     const int stoppedBlocks = tableBlocks - activeBlocks;
     if (stoppedBlocks >= b->numSMs && 8 * stoppedBlocks >= tableBlocks) {
-      rc = refresh(b);
-      if (rc != RN_OK) break;
+      int r = refresh(b);
+      if (r != RN_OK) return r;
       tableBlocks = b->nblocks;
     }
-    const long long left = max_steps > 0 ? max_steps - done : chunk;
-    const int n = int(left < chunk ? left : chunk);
-    rc = issue_steps(b, n);
-    if (rc != RN_OK) break;
+    return RN_OK;
+  };
+  auto chunk_at = [&](long long at) -> int {
+    const long long left = max_steps > 0 ? max_steps - at : chunk;
+    return int(left < chunk ? (left > 0 ? left : 0) : chunk);
+  };
+  auto account = [&](int n) {
     for (size_t m = 0; m < nm; m++)
       if (b->runActive[m]) {
         advance(b->members[m], n, b->flags);
         if (steps) steps[m] += n;
       }
-    done += n;
+  };
+  rc = refresh(b);
+  tableBlocks = b->nblocks;
+  int count = 0;
+  if (rc == RN_OK) rc = gate(0, 0);
+  if (rc == RN_OK) rc = take(0, count);
+  if (b->flags.inj) {
+    // with sprays each chunk's per-member parcel launches follow the host's
+    // flags, so every chunk waits for the gate before it
+    while (rc == RN_OK && count > 0) {
+      rc = compact();
+      const int n = chunk_at(done);
+      if (rc == RN_OK) rc = issue_steps(b, n);
+      if (rc != RN_OK) break;
+      account(n);
+      done += n;
+      rc = gate(0, done);
+      if (rc == RN_OK) rc = take(0, count);
+    }
+  } else if (rc == RN_OK && count > 0) {
+    // Without sprays the kernels alone read the flags, so the next chunk is
+    // queued before the gate ahead of it has been read back: gate j's flags
+    // (buffer j & 1) gate chunk j on the device, and the host learns them,
+    // and accounts for chunk j, while chunk j runs. The chunk queued after the
+    // last member stopped is all early returns.
+    rc = compact();
+    int n = chunk_at(done);
+    if (rc == RN_OK) rc = issue_steps(b, n);
+    if (rc == RN_OK) {
+      account(n);
+      done += n;
+      rc = gate(1, done);
+    }
+    for (int j = 1; rc == RN_OK; j++) {
+      n = chunk_at(done);
+      if (n > 0) rc = issue_steps(b, n);             // chunk j, ahead of its gate's read-back
+      if (rc == RN_OK) rc = gate((j + 1) & 1, done + n);
+      if (rc == RN_OK) rc = take(j & 1, count);
+      if (rc != RN_OK || count == 0) break;
+      account(n);
+      done += n;
+      rc = compact();
+    }
+    if (rc == RN_OK) {
+      cudaError_t e = cudaStreamSynchronize(b->stream);
+      if (e != cudaSuccess) rc = rn_record_cuda(e, "rn_batch_run");
+    }
   }
   if (rc == RN_OK) {
     cudaError_t e = cudaGetLastError();
@@ -633,6 +696,8 @@ int rn_batch_destroy(rn_batch b) {
   cudaFree(b->dTEnd);
   cudaFree(b->dGate);
   cudaFreeHost(b->hGate);
+  for (cudaEvent_t e : b->evGate)
+    if (e) cudaEventDestroy(e);
   cudaFreeHost(b->hInst);
   cudaEventDestroy(b->staged);
   cudaEventDestroy(b->done);
