@@ -712,7 +712,7 @@ def exit_column(state, s):
 def run_fp64_check(args):
     """Thrust and exhaust mass flow of the CUDA path (FP32, default precision)
     against an FP64 run of the same scheme (the oracle in double precision),
-    after the same number of steps: config 1 at its full 2000 steps and the
+    after the same number of steps: the plain cold-gas cone 256x96 at its full 2000 steps and the
     viscous plume over a bounded 1000-step sample (its 10k steps take minutes
     in FP64 on the host)."""
     rn = ge.load_package()
@@ -720,7 +720,7 @@ def run_fp64_check(args):
     oracle.set_threads(os.cpu_count() or 1)
     from rocket_nozzle_cfd_solver_b200 import configs
     out = {}
-    for name, cfg, n in (("plain 256x96 (config 1)", configs.plain_small()[0], 2000),
+    for name, cfg, n in (("plain cold-gas cone 256x96, 2000 steps", configs.plain_small()[0], 2000),
                          ("viscous plume 512x192", configs.viscous_plume()[0], 1000)):
         s = rn.build_sim_setup(cfg)
         g = rn.GPUSolver(s.Nx, s.Nr)

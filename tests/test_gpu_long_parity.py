@@ -18,7 +18,7 @@ precision's approximate division and fused multiply-adds, the fixed-point
 spray deposits) grow until the two runs are different realisations of the
 same flow. The per-field relative L2 against the oracle is therefore reported
 at every checkpoint (printed, -s) and bounded only at the first, while the
-mean quantities the solver is run for stay within the bar north_star states:
+mean quantities the solver is run for stay within a 1e-3 bar:
 exit thrust and mass flow within 1e-3 of the FP64 oracle at 10k steps (the
 FP64-scheme error), and the spray chamber's read-outs and parcel mass within
 a few per cent of the oracle's realisation at 2 ms."""
@@ -84,7 +84,7 @@ def test_viscous_plume_10k_steps(rn, long_ref, alt_km):
     fp64 = long_ref[f"plume{alt_km}_fp64_readouts"]
     err64 = np.abs(ro - fp64) / np.abs(fp64)
     print(f"{alt_km} km, 10k steps: thrust / mdot error against the FP64 oracle {err64[:2].tolist()}")
-    # the early checkpoint: the same flow to the north-star bar
+    # the early checkpoint: the same flow, within 1e-3 per field
     assert max(rows[0][1]) <= 1e-3, rows[0]
     # the FP64-scheme error of the mean read-outs at 10k steps
     assert err64[0] <= 1e-3 and err64[1] <= 1e-3, err64

@@ -1,7 +1,7 @@
 """CUDA path against the CPU oracle, through the C-ABI (librn.so), in both
 precision modes.
 
-Tolerance (north-star bar): every conserved field within relative L2 1e-4 of
+Tolerance: every conserved field within relative L2 1e-4 of
 the oracle after N steps, each field measured against the norm of its family
 (helpers.state_rel_l2). Exact mode (IEEE division/sqrt) must be much tighter:
 1e-6, and bit-identical over the first steps of these cases.

@@ -119,7 +119,7 @@ def test_quiescent_state_stays_at_rest(rn, oracle):
 
 
 def test_cold_gas_thrust_near_one_d_theory(rn, oracle):
-    """Config 1 (cold-gas cone, 256 x 96, 2000 steps): the exit-plane read-out
+    """The plain cold-gas cone (256 x 96, 2000 steps): the exit-plane read-out
     of the oracle's state lands near 1-D nozzle theory, as the reference's
     README reports for its own solver (within a few percent)."""
     from rocket_nozzle_cfd_solver_b200 import configs
