@@ -1,6 +1,6 @@
 """CPU oracle: golden fixtures, determinism, FP64 agreement and physical sanity.
 
-The oracle is the checker for the CUDA path; these tests pin it. The
+The CUDA path is checked against the oracle; these tests pin the oracle. The
 reference itself cannot run (WebGL2 only), so the pins are the committed
 fixtures (tests/golden/make_golden.py), the reference's integer hash restated
 independently in Python, and physics known answers.
