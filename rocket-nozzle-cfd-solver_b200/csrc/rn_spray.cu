@@ -287,7 +287,6 @@ __global__ void __launch_bounds__(256) k_apply(ApplyArgs a, rn_params P) {
     a.hsNext[1] = a.hsNext[1] + 1u;
   }
   if (k < N) {
-    const int i = k % g.Nx, j = k / g.Nx;
     float4 oA, oB;
     bool fluid = !g.mask[k];
     // the next step's deposit sums start at zero (both variants keep this up)
@@ -298,7 +297,7 @@ __global__ void __launch_bounds__(256) k_apply(ApplyArgs a, rn_params P) {
       oB = make_float4(P.ambB[0], P.ambB[1], P.ambB[2], P.ambB[3]);
     } else {
       float4 gm = g.geoM[k];
-      const int kh = (j + iround(gm.y)) * g.Nx + (i + iround(gm.x));
+      const int kh = k + iround(gm.y) * g.Nx + iround(gm.x);   // the cell's group host (i + dx, j + dy)
 #ifdef RN_FAST
       const ulonglong2* c = reinterpret_cast<const ulonglong2*>(a.acc) + 2 * size_t(kh);
       const ulonglong2 c01 = c[0], c23 = c[1];
