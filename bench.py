@@ -69,18 +69,23 @@ def profiled_traffic(kind):
 
 
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons while running."""
+    """nvidia-smi samples of SM clock and throttle reasons, every 20 ms while
+    it runs. Started before the warm-up (nvidia-smi takes a while to start);
+    mark() brackets the timed region and summary() keeps the samples taken
+    inside it (the nearest later one if the region was shorter than a
+    sampling interval)."""
 
     def __init__(self, index):
         self.index = index
         self.samples = []
         self.proc = None
+        self.window = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active",
-                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                 "--format=csv,noheader,nounits", "-lms", "20"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
                 text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -93,9 +98,18 @@ class ClockSampler:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) == 3:
                 try:
-                    self.samples.append((float(parts[0]), float(parts[1]), int(parts[2], 16)))
+                    self.samples.append((time.monotonic(), float(parts[0]), float(parts[1]), int(parts[2], 16)))
                 except ValueError:
                     pass
+
+    def wait_first(self, timeout_s=5.0):
+        """Waits (bounded) until nvidia-smi has produced its first sample."""
+        t0 = time.monotonic()
+        while self.proc is not None and not self.samples and time.monotonic() - t0 < timeout_s:
+            time.sleep(0.01)
+
+    def mark(self, t0, t1):
+        self.window = (t0, t1)
 
     def __exit__(self, *exc):
         if self.proc is not None:
@@ -106,16 +120,24 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        if not self.samples:
+        samples = self.samples
+        if self.window is not None:
+            t0, t1 = self.window
+            inside = [q for q in samples if t0 <= q[0] <= t1]
+            if not inside:
+                later = [q for q in samples if q[0] > t1]
+                inside = later[:1]
+            samples = inside
+        if not samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [s[0] for s in self.samples]
+        sm = [q[1] for q in samples]
         reasons = set()
-        for s in self.samples:
+        for q in samples:
             for bit, name in THROTTLE_BITS.items():
-                if s[2] & bit and name != "gpu_idle":
+                if q[3] & bit and name != "gpu_idle":
                     reasons.add(name)
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(s[1] for s in self.samples),
-                "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(q[2] for q in samples),
+                "reasons": sorted(reasons), "samples": len(sm), "interval_ms": 20}
 
 
 GRID = (512, 192)
@@ -213,6 +235,9 @@ def run_ours(args, rank, world, local_rank):
         with torch.cuda.stream(stream):
             flush.fill_(1.0)
 
+    clk = ClockSampler(local_rank)
+    clk.__enter__()                             # sampling from the warm-up on; the timed window is marked below
+    clk.wait_first()
     for _ in range(args.warmup):
         flush_l2()
         g.step(SOLVER_STEPS, params)
@@ -225,16 +250,19 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- timed region: device time per bench step, L2 flushed before each
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    with ClockSampler(local_rank) as clk:
-        for k in range(args.steps):
-            flush_l2()
-            with torch.cuda.stream(stream):
-                evs[k][0].record(stream)
-            g.step(SOLVER_STEPS, params)
-            with torch.cuda.stream(stream):
-                evs[k][1].record(stream)
-        g.sync()
-        torch.cuda.synchronize()
+    t_clk0 = time.monotonic()
+    for k in range(args.steps):
+        flush_l2()
+        with torch.cuda.stream(stream):
+            evs[k][0].record(stream)
+        g.step(SOLVER_STEPS, params)
+        with torch.cuda.stream(stream):
+            evs[k][1].record(stream)
+    g.sync()
+    torch.cuda.synchronize()
+    clk.mark(t_clk0, time.monotonic())
+    time.sleep(0.05)                            # the sample after a region shorter than the interval
+    clk.__exit__(None, None, None)
     launches = g.kernelLaunches() - launches0
     ms = sum(a.elapsed_time(b) for a, b in evs)
     dev = f"cuda:{local_rank}"

@@ -41,3 +41,22 @@ def test_product_arm_fails_without_gpu():
     r = run_bench("--steps", "1", "--warmup", "1", "--no-cpu", timeout=300)
     assert r.returncode != 0
     assert not r.stdout.strip() or "value" not in r.stdout
+
+
+def test_clock_summary_keeps_the_timed_window():
+    """Clock samples are summarised over the marked timed region; a region
+    shorter than the sampling interval takes the next sample after it; a
+    throttle reason seen in the window is reported (idle is not a reason)."""
+    sys.path.insert(0, ROOT)
+    import bench
+    c = bench.ClockSampler(0)
+    c.samples = [(0.0, 1200.0, 1965.0, 0x1), (1.0, 1965.0, 1965.0, 0x0), (1.5, 1965.0, 1965.0, 0x4),
+                 (3.0, 1500.0, 1965.0, 0x20)]
+    c.mark(0.9, 2.0)
+    s = c.summary()
+    assert s["samples"] == 2 and s["sm_mhz"] == 1965.0 and s["reasons"] == ["sw_power_cap"]
+    c.mark(2.1, 2.2)
+    s = c.summary()
+    assert s["samples"] == 1 and s["sm_mhz"] == 1500.0 and s["reasons"] == ["sw_thermal_slowdown"]
+    c.samples = []
+    assert c.summary()["reasons"] == ["unsampled"]
