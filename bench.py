@@ -502,7 +502,7 @@ def run_batched(args, local_rank, rank=0, world=1):
     bpc = BYTES_PER_CELL["stage1"] + BYTES_PER_CELL["stage2_physics"]
     instances = int(replicas.sum_over_ranks(len(setups), dev))
     classes = None
-    if world == 1:
+    if world == 1 and not args.no_classes:
         classes = [class_solves(rn, size, n, fp64_samples=(2 if size[0] <= 256 else 0))
                    for size, n in CLASS_COUNTS.items()]
     return {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "instances": instances,
@@ -878,6 +878,8 @@ def main():
                     help="Poisson arrival rates of the serving leg (1/s), comma-separated")
     ap.add_argument("--serve-max-cells", type=int, default=2000000,
                     help="admission cap on the grid cells the server steps at once (0: memory budget only)")
+    ap.add_argument("--no-classes", action="store_true",
+                    help="skip the batched leg's solves-per-grid-class comparison (for profiling)")
     args = ap.parse_args()
     GRID = tuple(int(v) for v in args.grid.lower().split("x"))
     SOLVER_STEPS = args.solver_steps
